@@ -1,0 +1,315 @@
+"""Benchmark of the PLISCuda simulation step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload schlogl64]
+
+Workload (the configuration the headline metric is quoted on): the Schlogl bistable model on a
+64x64x64 reflective lattice (262,144 subvolumes, 1 species, 4 reactions of order 0-3), plain
+(Cao) tau, reference semantics, binary64 propensities, seeded synthetic initial state
+(X=100 for x<32, 600 above).  One bench "step" is one checkpoint interval of 1.0 simulated time
+units (hundreds of tau-leap steps, as the configuration checkpoints every 1.0), continuing one
+trajectory: W warm-up intervals, then K timed ones.
+
+Metric: events/second (an event is one reaction firing or one molecule jump; a leap firing of k
+counts k), with simulated-time/second alongside.  `value` is device time from CUDA events on the
+library's stream around each interval with the state resident in HBM; L2 is flushed (a 512 MiB
+write) between timed intervals.  `e2e` is the same metric through the C ABI with host buffers:
+every interval uploads the state from pinned host memory (plis_set_state), runs, and reads the
+state back (plis_get_state).
+
+N > 1 (torchrun): each rank simulates its own independent replica (different seed) on its own GPU;
+there is no data-path collective.  value = all ranks' events / the max over ranks of device time.
+
+--impl reference: the reference has no CPU implementation of the step, so its CPU arm is the FP64
+host oracle (oracle/plis_oracle.cpp, OpenMP over subvolumes) on all host threads, on a bounded
+slice of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "events/sec & sim-time/sec on 1 B200 (Schlogl 64^3, plain Cao tau)"
+UNIT = "events/s"
+INTERVAL = 1.0
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _workload(name):
+    from pliscuda_b200 import workloads
+    if name == "schlogl64":
+        return workloads.schlogl(64)
+    if name == "schlogl128":
+        return workloads.schlogl(128)
+    if name == "small_ab":
+        return workloads.small_ab(10)
+    raise SystemExit(f"unknown workload {name}")
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sms, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sms.append(float(p[1]))
+                mx = max(mx, float(p[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sms:
+            return None
+        return {"sm_mhz": statistics.median(sms), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sms)}
+
+
+def run_reference(args):
+    """CPU arm: the FP64 host oracle on all host threads, bounded slice of the workload."""
+    from oracle.oracle import Oracle
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    model, state = _workload(args.workload)
+    threads = os.cpu_count() or 1
+    orc = Oracle.from_model(model, mode=0, precision=0, seed=1, threads=threads)
+    orc.set_state(state)
+    # bounded sample: a slice of simulated time per step, sized so the whole run stays within minutes
+    slice_t = args.ref_slice
+    for _ in range(max(0, args.warmup if args.warmup < 1 else 1)):
+        orc.run(orc.stats().time + slice_t / 4)
+    t0 = time.perf_counter()
+    ev0, st0, tt0 = orc.stats().events, orc.stats().steps, orc.stats().time
+    for _ in range(args.steps):
+        orc.run(orc.stats().time + slice_t)
+    el = time.perf_counter() - t0
+    s = orc.stats()
+    ev = s.events - ev0
+    value = ev / el
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.workload} Schlogl, {model.n_subvolumes} subvolumes, reference semantics",
+                   "step": f"{slice_t} simulated time units per step (bounded CPU sample)"},
+        "sim_time_per_sec": (s.time - tt0) / el,
+        "leap_steps_per_sec": (s.steps - st0) / el,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} x {slice_t} sim-time units of the {args.workload} workload, "
+                                   f"FP64 host oracle (OpenMP, {threads} threads)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+    return 0
+
+
+def cpu_baseline_sample(model, state, threads, budget_s=12.0):
+    """Oracle events/s on a bounded slice (about budget_s of CPU work)."""
+    from oracle.oracle import Oracle
+    orc = Oracle.from_model(model, mode=0, precision=0, seed=1, threads=threads)
+    orc.set_state(state)
+    t0 = time.perf_counter()
+    slice_t = 0.002
+    while True:
+        orc.run(orc.stats().time + slice_t)
+        el = time.perf_counter() - t0
+        if el > budget_s:
+            break
+        slice_t = min(slice_t * 2, 0.05)
+    s = orc.stats()
+    return {"value": s.events / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"first {s.time:.4f} sim-time units ({s.steps} leap steps) of the same workload, FP64 host "
+                      f"oracle, OpenMP {threads} threads, {el:.1f} s"}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="schlogl64")
+    ap.add_argument("--mode", default="reference", choices=["reference", "corrected"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--ref-slice", type=float, default=0.01)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args(argv)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    from pliscuda_b200 import Simulation
+    model, state = _workload(args.workload)
+    seed = 1000 + rank
+    sim = Simulation(model, mode=args.mode, precision=args.precision, seed=seed, device=local)
+    sim.set_state(state)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    t = 0.0
+    for _ in range(args.warmup):
+        t += INTERVAL
+        sim.run(t)
+    torch.cuda.synchronize()
+
+    clocks = Clocks(local)
+    ev_tot, ms_tot, simt_tot, launches = 0, 0.0, 0.0, 0
+    steps_tot = 0
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    for _ in range(args.steps):
+        flush.fill_(1)  # L2 flush between timed intervals (outside the timed interval)
+        torch.cuda.synchronize()
+        a = sim.stats()
+        t += INTERVAL
+        b = sim.run(t)
+        ev_tot += b.events - a.events
+        ms_tot += b.device_ms - a.device_ms
+        simt_tot += b.time - a.time
+        launches += b.kernel_launches - a.kernel_launches
+        steps_tot += b.steps - a.steps
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    if dist:
+        dist.barrier()
+        v = torch.tensor([ms_tot, float(ev_tot), simt_tot], dtype=torch.float64, device=f"cuda:{local}")
+        mx = v.clone()
+        dist.all_reduce(mx[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(v[1:2], op=dist.ReduceOp.SUM)
+        ms_all, ev_all = float(mx[0]), float(v[1])
+    else:
+        ms_all, ev_all = ms_tot, float(ev_tot)
+    value = ev_all / (ms_all / 1e3)
+    sim_time_per_sec = simt_tot / (ms_tot / 1e3)
+
+    # per-kernel roofline from an event-instrumented replay of a slice of the same trajectory
+    cur = sim.get_state()
+    with Simulation(model, mode=args.mode, precision=args.precision, seed=seed, device=local, profile=True) as ps:
+        ps.set_state(cur)
+        ps.run(INTERVAL / 4)
+        per = ps.kernel_profile()
+    dom = max(per, key=lambda k: per[k][0])
+    N, S = model.n_subvolumes, model.n_species
+    algo_bytes = {"leap": 8 * S * N, "classify": 4 * S * N + 9 * N + 4 * S * N, "exact": 0, "apply": 8 * S * N}
+    ms_launch = per[dom][0] / max(1, per[dom][1])
+    achieved = algo_bytes[dom] / (ms_launch / 1e3) / 1e9
+    peak, peak_kind = _peaks()
+    shares = {k: round(v[0] / max(1e-12, sum(x[0] for x in per.values())), 4) for k, v in per.items()}
+
+    # end to end through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        host = torch.from_numpy(cur).pin_memory()
+        hnp = host.numpy()
+        out = torch.empty_like(host).pin_memory()
+        onp = out.numpy()
+        e_ev, e_s = 0, 0.0
+        for i in range(args.steps):
+            torch.cuda.synchronize()
+            w0 = time.perf_counter()
+            sim.set_state(hnp)
+            st = sim.run(INTERVAL)
+            sim.get_state(onp)
+            e_s += time.perf_counter() - w0
+            e_ev += st.events
+            hnp[:] = onp
+        e2e = {"value": e_ev / e_s, "unit": UNIT, "h2d_bytes_per_step": int(hnp.nbytes),
+               "d2h_bytes_per_step": int(onp.nbytes), "sim_time_per_sec": args.steps * INTERVAL / e_s}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(model, state, os.cpu_count() or 1)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_all / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32",
+            "data": "synthetic",
+            "config": {"workload": f"{args.workload}: Schlogl bistable model, {model.n_subvolumes} subvolumes "
+                                   f"(64^3 reflective lattice), 1 species, 4 reactions, {args.mode} semantics",
+                       "step": f"one checkpoint interval of {INTERVAL} simulated time units",
+                       "l2": "flushed between timed steps (512 MiB write)", "parallelism": f"replicas x{world}",
+                       "precision": args.precision},
+            "sim_time_per_sec": sim_time_per_sec,
+            "leap_steps_per_sec": steps_tot / (ms_tot / 1e3),
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                         "algorithmic_bytes_per_launch": algo_bytes[dom], "ms_per_launch": ms_launch,
+                         "kernel_share": shares},
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "clocks": ck,
+        }
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

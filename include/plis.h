@@ -1,0 +1,207 @@
+/* plis.h — C ABI of the B200 PLISCuda simulation step (libplis.so).
+ *
+ * The reference exposes one C++ entry point for its whole hot path,
+ *     void PLISCuda::run_simulation(Topology t, State s, Reactions r, float* h_rrc, float* h_drc,
+ *                                   float endTime, int compartments_count, int* subv_constants,
+ *                                   float log_freq);          (PLISCuda/include/cuda/driver.cuh:32-33)
+ * called once from main (PLISCuda/src/main.cpp:53-63).  This header splits that function into a
+ * handle API with plain pointers and sizes, so it can be bound from C, C++ (the drop-in shim in
+ * pliscuda_b200/compat/), Python ctypes, or any FFI.  Every function returns a plis_status
+ * (0 = PLIS_OK); no exception, exit() or abort crosses the ABI.  The message of the last failure
+ * on the calling thread is available from plis_last_error().
+ *
+ * Data layout at the boundary (the same as the reference's host arrays):
+ *   counts      uint32 [S*N] species-major, counts[s*N + i]      (State.hpp:210, driver.cu:55)
+ *   reactants   int32  [S*R] species-major, reactants[s*R + r]  (Reactions.hpp:197)
+ *   products    int32  [S*R] species-major                      (Reactions.hpp:209)
+ *   neighbours  uint32 [6*N] row-major, unused slots hold the subvolume's own index
+ *                                                               (Topology.hpp:176-184)
+ *   reaction_rates  [C*R], diffusion_rates [C*S] compartment-major (Configuration.hpp:123-143)
+ *   compartment int32  [N] compartment of each subvolume       (cpp_utils.hpp:47-56)
+ * Counts must stay below 2^31 (the reference stores them as int, driver.cu:55-59).
+ */
+#ifndef PLIS_H_
+#define PLIS_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PLIS_ABI_VERSION 1
+
+typedef enum plis_status {
+  PLIS_OK = 0,
+  PLIS_ERR_INVALID = 1,    /* bad argument or inconsistent model (reference: std::invalid_argument) */
+  PLIS_ERR_PARSE = 2,      /* malformed input file (reference: std::invalid_argument from the parsers) */
+  PLIS_ERR_IO = 3,         /* file missing or unreadable (Configuration.hpp:53-55 "file ... not found") */
+  PLIS_ERR_OOM = 4,        /* host or device allocation failed */
+  PLIS_ERR_CUDA = 5,       /* CUDA runtime error (reference: gpuErrchk -> exit, cpp_utils.hpp:97-105) */
+  PLIS_ERR_TIMEOUT = 6,    /* a bounded device-side wait gave up */
+  PLIS_ERR_STUCK = 7,      /* more than max_rollbacks consecutive rollbacks in one step */
+  PLIS_ERR_OVERFLOW = 8,   /* a count would leave [0, 2^31) for a reason a rollback cannot fix */
+  PLIS_ERR_LIMIT = 9,      /* model exceeds a compiled limit (species, reactions, order, neighbours) */
+  PLIS_ERR_NO_DEVICE = 10, /* no CUDA device (main.cpp:19-24) */
+  PLIS_ERR_UNSUPPORTED = 11
+} plis_status;
+
+/* Semantics of the step (plis_options.mode). */
+#define PLIS_MODE_REFERENCE 0 /* the reference's rules, deterministic quirks included */
+#define PLIS_MODE_CORRECTED 1 /* Cao-consistent criticality, diffusion terms and exact events */
+
+/* Arithmetic of propensities, Cao tau and Poisson means (plis_options.precision).  Simulated
+ * time, the tau array, the min-tau reduction and exponential next-event times are binary64 in both. */
+#define PLIS_PREC_FP64 0
+#define PLIS_PREC_FP32 1
+
+/* Per-subvolume operation flags (the reference's enum op, constants.cuh:53-58). */
+#define PLIS_LEAP_CR 0
+#define PLIS_LEAP_NOCR 1
+#define PLIS_SSA 2
+#define PLIS_SSA_FF 3
+
+/* Why plis_run / plis_step returned. */
+#define PLIS_STOP_NONE 0
+#define PLIS_STOP_TIME 1      /* simulated time reached t_end */
+#define PLIS_STOP_STEPS 2     /* the requested number of steps was taken */
+#define PLIS_STOP_NO_EVENT 3  /* min tau was +inf or negative: nothing can fire (driver.cu:269-272) */
+#define PLIS_STOP_ERROR 4
+
+typedef struct plis_model_desc {
+  uint32_t n_subvolumes;  /* N */
+  uint32_t n_species;     /* S */
+  uint32_t n_reactions;   /* R */
+  uint32_t n_compartments;/* C >= 1 */
+  /* Topology: either an explicit table (neighbours != NULL) or an implicit reflective 6-neighbour
+   * lattice lattice_x * lattice_y * lattice_z == N, linearised i = x + X*(y + Y*z)
+   * (genTopology.py:30-37).  An explicit table that is such a lattice is recognised and run as one. */
+  const uint32_t* neighbours;
+  uint32_t lattice_x, lattice_y, lattice_z;
+  const int32_t* reactants;
+  const int32_t* products;
+  const double* reaction_rates;
+  const double* diffusion_rates;
+  const int32_t* compartment; /* NULL: every subvolume in compartment 0 */
+} plis_model_desc;
+
+typedef struct plis_options {
+  uint32_t size;              /* sizeof(plis_options), filled by plis_options_init */
+  int32_t mode;               /* PLIS_MODE_REFERENCE (default) or PLIS_MODE_CORRECTED */
+  int32_t precision;          /* PLIS_PREC_FP64 (default) or PLIS_PREC_FP32 */
+  int32_t critical_threshold; /* NC, default 10 (driver.cu:36) */
+  double epsilon;             /* Cao epsilon, default 0.05 (driver.cu:37) */
+  uint64_t seed;              /* key of the Philox4x32-10 stream, default 1 */
+  uint32_t replica;           /* replica id folded into the key (independent streams) */
+  int32_t device;             /* CUDA device ordinal, default 0 */
+  int32_t max_rollbacks;      /* per step before PLIS_ERR_STUCK, default 64 */
+  int32_t steps_per_launch;   /* steps captured per CUDA-graph launch, 0 = auto */
+  int32_t tile[3];            /* lattice brick per CTA (x, y, z), 0 = auto */
+  int32_t persistent;         /* 1 = one cooperative persistent launch per run call, 0 = graph of phase kernels, -1 = auto */
+  int32_t profile;            /* 1 = launch phase kernels one by one with CUDA events around each (plis_get_profile) */
+} plis_options;
+
+/* Per-kernel device time accumulated while plis_options.profile is set (CUDA events recorded on the
+ * handle's stream around every launch). */
+#define PLIS_KERNEL_LEAP 0
+#define PLIS_KERNEL_EXACT 1
+#define PLIS_KERNEL_APPLY 2
+#define PLIS_KERNEL_CLASSIFY 3
+#define PLIS_KERNEL_COUNT 4
+typedef struct plis_profile {
+  double ms[PLIS_KERNEL_COUNT];
+  uint64_t launches[PLIS_KERNEL_COUNT];
+} plis_profile;
+
+typedef struct plis_stats {
+  double time;            /* simulated time */
+  uint64_t steps;         /* accepted steps */
+  uint64_t rollbacks;     /* rejected attempts */
+  uint64_t events;        /* reaction firings + molecule jumps (a leap firing of k counts k) */
+  uint64_t exact_events;  /* single-event firings (critical and SSA) among them */
+  int32_t stop_reason;    /* PLIS_STOP_* of the last run/step call */
+  int32_t status;         /* sticky error status of the handle (PLIS_OK if none) */
+  double last_tau;        /* arg-min tau of the last accepted step */
+  int64_t last_argmin;    /* its subvolume */
+  double device_ms;       /* device time spent in run/step calls (CUDA events) */
+  uint64_t kernel_launches; /* kernels launched by the library so far */
+} plis_stats;
+
+typedef struct plis_handle plis_handle;
+
+/* Library */
+int plis_abi_version(void);
+const char* plis_last_error(void);         /* thread-local message of the last failed call */
+const char* plis_status_string(int status);
+void plis_options_init(plis_options* opts);
+
+/* Lifecycle.  Replaces the set-up half of run_simulation (driver.cu:15-239): the model is copied
+ * (the caller keeps ownership of every input array), device memory is allocated once, and the
+ * state starts at zero counts until plis_set_state. */
+int plis_create(const plis_model_desc* model, const plis_options* opts, plis_handle** out);
+int plis_destroy(plis_handle* h);
+
+/* State.  plis_set_state copies counts to the device, resets time/steps/statistics and computes
+ * the initial rates, taus and flags (driver.cu:221-234).  plis_get_state copies them back
+ * (driver.cu:366, :391). */
+int plis_set_state(plis_handle* h, const uint32_t* counts);
+int plis_get_state(plis_handle* h, uint32_t* counts);
+int plis_set_time(plis_handle* h, double time);
+
+/* The step loop (driver.cu:259-376).  plis_run advances until simulated time >= t_end (reference
+ * mode: the step that crosses t_end is taken, as the reference loop does; corrected mode: the last
+ * step is shortened to land on t_end exactly).  plis_step takes at most n_steps accepted steps.
+ * Both stop early on PLIS_STOP_NO_EVENT. */
+int plis_run(plis_handle* h, double t_end);
+int plis_step(plis_handle* h, uint64_t n_steps);
+int plis_get_stats(plis_handle* h, plis_stats* out);
+
+/* Per-kernel timing of profiled run/step calls (plis_options.profile = 1); reset by plis_set_state. */
+int plis_get_profile(plis_handle* h, plis_profile* out);
+
+/* Inspection: per-subvolume tau (binary64) and operation flags of the current state. */
+int plis_get_taus(plis_handle* h, double* tau, uint8_t* flags);
+
+/* Topology helpers (host only, no device needed).
+ * plis_canonical_neighbours rewrites a 6-wide table so that each row lists its distinct non-self
+ * neighbours first (lattice rows in the order -x,+x,-y,+y,-z,+z) followed by self padding; this is
+ * the slot order the engine's random stream is keyed on.  lattice_out receives (X,Y,Z) when the
+ * table is a reflective lattice, else zeros.  table may be NULL when lattice_in is given. */
+int plis_canonical_neighbours(uint32_t n, const uint32_t* table, const uint32_t lattice_in[3],
+                              uint32_t* canonical, uint32_t lattice_out[3]);
+
+/* ---------------------------------------------------------------------------------------------
+ * Input files in the reference's formats, read unchanged (Configuration.hpp:27-144,
+ * Topology.hpp:98-191, State.hpp:112-217, Reactions.hpp:132-223, cpp_utils.hpp:29-56).
+ * ------------------------------------------------------------------------------------------- */
+typedef struct plis_config plis_config;
+
+typedef struct plis_config_view {
+  plis_model_desc model;     /* points into the config; valid until plis_config_free */
+  const uint32_t* initial_state; /* [S*N] */
+  double end_time;           /* endTime (Configuration.hpp:73-77) */
+  double log_freq;           /* logFreq (Configuration.hpp:80-85) */
+} plis_config_view;
+
+/* Parse conf.txt and the files it names (paths relative to the conf file's directory, falling
+ * back to the current directory as the reference does).  Errors carry the reference's messages. */
+int plis_config_load(const char* conf_path, plis_config** out);
+int plis_config_view_get(const plis_config* cfg, plis_config_view* view);
+void plis_config_free(plis_config* cfg);
+
+/* Single-file parsers (the reference's operator>> overloads).  Arrays are allocated with malloc
+ * and owned by the caller (free with plis_free). */
+int plis_parse_topology(const char* path, uint32_t* n_out, uint32_t** neighbours_out);
+int plis_parse_state(const char* path, uint32_t* n_out, uint32_t* s_out, uint32_t** counts_out);
+int plis_parse_reactions(const char* path, uint32_t* r_out, uint32_t* s_out, int32_t** reactants_out,
+                         int32_t** products_out);
+void plis_free(void* p);
+
+/* Snapshot in the reference's .dat format (print_state_snapshot, driver.cu:435-447). */
+int plis_write_snapshot(const char* path, const uint32_t* counts, uint32_t n, uint32_t s, double time);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PLIS_H_ */

@@ -1,0 +1,76 @@
+"""TEST INFRASTRUCTURE: compile pieces of the reference from its own sources into oracle/_ref/.
+
+    python oracle/ref_build.py [--reference /root/reference] [--cuda]
+
+* refdump       the reference's header-only input parsers (PLISCuda/include/cpp/*.hpp) driven by
+                oracle/ref/refdump.cpp: g++ on the reference headers where they lie.
+* pliscuda_test the reference's CUDA step (PLISCuda/src/*.cu + main.cpp) built with nvcc for sm_100a
+  pliscuda      with -DTEST (fixed per-subvolume seeds, PLISCuda/src/init.cu:9-11) and without.
+                The reference makefile cannot be used as shipped (its -arch=sm_30 is gone from nvcc
+                12.9 and CCCL needs C++17); the flags below are the four changes recorded in DESIGN.md.
+Outputs go only to oracle/_ref/ (git-ignored; it travels with the tree to the GPU box).
+Nothing from the reference is copied into the repository.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT = os.path.join(HERE, "_ref")
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+
+
+def build_refdump(ref: str) -> str:
+    os.makedirs(OUT, exist_ok=True)
+    out = os.path.join(OUT, "refdump")
+    inc = os.path.join(ref, "PLISCuda", "include", "cpp")
+    _run(["g++", "-std=c++17", "-O1", "-I", inc, "-I/usr/local/cuda/include",
+          os.path.join(HERE, "ref", "refdump.cpp"), "-o", out])
+    return out
+
+
+def build_cuda(ref: str, test: bool) -> str:
+    os.makedirs(OUT, exist_ok=True)
+    src = os.path.join(ref, "PLISCuda", "src")
+    name = "pliscuda_test" if test else "pliscuda"
+    out = os.path.join(OUT, name)
+    obj_dir = os.path.join(OUT, "obj_" + name)
+    os.makedirs(obj_dir, exist_ok=True)
+    flags = ["-std=c++17", "-O3", "-rdc=true", "-arch=sm_100a"] + (["-DTEST"] if test else [])
+    objs = []
+    for f in ["driver.cu", "init.cu", "leap.cu", "log.cu", "rates.cu", "ssa.cu", "tau.cu"]:
+        o = os.path.join(obj_dir, f + ".o")
+        _run(["nvcc"] + flags + ["-c", os.path.join(src, f), "-o", o])
+        objs.append(o)
+    o = os.path.join(obj_dir, "main.o")
+    _run(["nvcc"] + flags + ["-x", "cu", "-c", os.path.join(src, "main.cpp"), "-o", o])
+    objs.append(o)
+    _run(["nvcc", "-arch=sm_100a", "-rdc=true"] + objs + ["-o", out])
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--cuda", action="store_true", help="also build the reference CUDA binaries")
+    a = ap.parse_args(argv)
+    if not os.path.isdir(a.reference):
+        print("reference tree not present; nothing to build")
+        return 0
+    print(build_refdump(a.reference))
+    if a.cuda:
+        print(build_cuda(a.reference, True))
+        print(build_cuda(a.reference, False))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

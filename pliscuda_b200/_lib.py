@@ -1,0 +1,122 @@
+"""ctypes binding of libplis.so (include/plis.h).  Importing this module loads the in-tree library
+and raises immediately if it is missing: there is no Python fallback for the step."""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libplis.so")
+
+u32 = ctypes.c_uint32
+i32 = ctypes.c_int32
+u64 = ctypes.c_uint64
+i64 = ctypes.c_int64
+f64 = ctypes.c_double
+vp = ctypes.c_void_p
+
+PLIS_OK = 0
+STATUS_NAMES = {
+    0: "PLIS_OK", 1: "PLIS_ERR_INVALID", 2: "PLIS_ERR_PARSE", 3: "PLIS_ERR_IO", 4: "PLIS_ERR_OOM",
+    5: "PLIS_ERR_CUDA", 6: "PLIS_ERR_TIMEOUT", 7: "PLIS_ERR_STUCK", 8: "PLIS_ERR_OVERFLOW",
+    9: "PLIS_ERR_LIMIT", 10: "PLIS_ERR_NO_DEVICE", 11: "PLIS_ERR_UNSUPPORTED",
+}
+MODE_REFERENCE, MODE_CORRECTED = 0, 1
+PREC_FP64, PREC_FP32 = 0, 1
+LEAP_CR, LEAP_NOCR, SSA, SSA_FF = 0, 1, 2, 3
+STOP_NONE, STOP_TIME, STOP_STEPS, STOP_NO_EVENT, STOP_ERROR = 0, 1, 2, 3, 4
+
+
+class ModelDesc(ctypes.Structure):
+    _fields_ = [("n_subvolumes", u32), ("n_species", u32), ("n_reactions", u32), ("n_compartments", u32),
+                ("neighbours", vp), ("lattice_x", u32), ("lattice_y", u32), ("lattice_z", u32),
+                ("reactants", vp), ("products", vp), ("reaction_rates", vp), ("diffusion_rates", vp),
+                ("compartment", vp)]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("size", u32), ("mode", i32), ("precision", i32), ("critical_threshold", i32),
+                ("epsilon", f64), ("seed", u64), ("replica", u32), ("device", i32), ("max_rollbacks", i32),
+                ("steps_per_launch", i32), ("tile", i32 * 3), ("persistent", i32), ("profile", i32)]
+
+
+class Profile(ctypes.Structure):
+    _fields_ = [("ms", f64 * 4), ("launches", u64 * 4)]
+
+
+KERNEL_NAMES = ("leap", "exact", "apply", "classify")
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("time", f64), ("steps", u64), ("rollbacks", u64), ("events", u64), ("exact_events", u64),
+                ("stop_reason", i32), ("status", i32), ("last_tau", f64), ("last_argmin", i64),
+                ("device_ms", f64), ("kernel_launches", u64)]
+
+
+class ConfigView(ctypes.Structure):
+    _fields_ = [("model", ModelDesc), ("initial_state", vp), ("end_time", f64), ("log_freq", f64)]
+
+
+class PlisError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        self.status = status
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+
+
+def _load() -> ctypes.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python pliscuda_b200/build.py`")
+    lib = ctypes.CDLL(LIB_PATH)
+    P = ctypes.POINTER
+    sig = {
+        "plis_abi_version": (i32, []),
+        "plis_last_error": (ctypes.c_char_p, []),
+        "plis_status_string": (ctypes.c_char_p, [i32]),
+        "plis_options_init": (None, [P(Options)]),
+        "plis_create": (i32, [P(ModelDesc), P(Options), P(vp)]),
+        "plis_destroy": (i32, [vp]),
+        "plis_set_state": (i32, [vp, vp]),
+        "plis_get_state": (i32, [vp, vp]),
+        "plis_set_time": (i32, [vp, f64]),
+        "plis_run": (i32, [vp, f64]),
+        "plis_step": (i32, [vp, u64]),
+        "plis_get_stats": (i32, [vp, P(Stats)]),
+        "plis_get_taus": (i32, [vp, vp, vp]),
+        "plis_get_profile": (i32, [vp, P(Profile)]),
+        "plis_canonical_neighbours": (i32, [u32, vp, vp, vp, vp]),
+        "plis_config_load": (i32, [ctypes.c_char_p, P(vp)]),
+        "plis_config_view_get": (i32, [vp, P(ConfigView)]),
+        "plis_config_free": (None, [vp]),
+        "plis_parse_topology": (i32, [ctypes.c_char_p, P(u32), P(vp)]),
+        "plis_parse_state": (i32, [ctypes.c_char_p, P(u32), P(u32), P(vp)]),
+        "plis_parse_reactions": (i32, [ctypes.c_char_p, P(u32), P(u32), P(vp), P(vp)]),
+        "plis_free": (None, [vp]),
+        "plis_write_snapshot": (i32, [ctypes.c_char_p, vp, u32, u32, f64]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if lib.plis_abi_version() != 1:
+        raise ImportError("libplis.so ABI version mismatch")
+    return lib
+
+
+lib = _load()
+
+
+def check(status: int) -> None:
+    if status != PLIS_OK:
+        raise PlisError(status, (lib.plis_last_error() or b"").decode(errors="replace"))
+
+
+def default_options(**kw) -> Options:
+    o = Options()
+    lib.plis_options_init(ctypes.byref(o))
+    for k, v in kw.items():
+        if k == "tile":
+            for i in range(3):
+                o.tile[i] = int(v[i])
+        else:
+            setattr(o, k, v)
+    return o

@@ -1,0 +1,199 @@
+// capi.cpp — the C ABI of libplis.so (include/plis.h).  No exception crosses this boundary.
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/plis.h"
+#include "engine.h"
+#include "plis_model.h"
+
+namespace {
+thread_local std::string g_err;
+}
+
+namespace plis {
+void set_error(const std::string& msg) { g_err = msg; }
+}  // namespace plis
+
+struct plis_handle {
+  plis::Engine eng;
+};
+
+#define PLIS_GUARD_BEGIN try {
+#define PLIS_GUARD_END                                  \
+  }                                                     \
+  catch (const std::bad_alloc&) {                       \
+    g_err = "out of host memory";                       \
+    return PLIS_ERR_OOM;                                \
+  }                                                     \
+  catch (const std::exception& e) {                     \
+    g_err = e.what();                                   \
+    return PLIS_ERR_INVALID;                            \
+  }                                                     \
+  catch (...) {                                         \
+    g_err = "unknown failure";                          \
+    return PLIS_ERR_INVALID;                            \
+  }
+
+static int fail(plis_handle* h, int rc) {
+  if (rc != PLIS_OK) g_err = h->eng.error();
+  return rc;
+}
+
+extern "C" {
+
+int plis_abi_version(void) { return PLIS_ABI_VERSION; }
+
+const char* plis_last_error(void) { return g_err.c_str(); }
+
+const char* plis_status_string(int s) {
+  switch (s) {
+    case PLIS_OK: return "ok";
+    case PLIS_ERR_INVALID: return "invalid argument";
+    case PLIS_ERR_PARSE: return "parse error";
+    case PLIS_ERR_IO: return "i/o error";
+    case PLIS_ERR_OOM: return "out of memory";
+    case PLIS_ERR_CUDA: return "CUDA error";
+    case PLIS_ERR_TIMEOUT: return "device wait timed out";
+    case PLIS_ERR_STUCK: return "too many rollbacks";
+    case PLIS_ERR_OVERFLOW: return "count overflow";
+    case PLIS_ERR_LIMIT: return "model exceeds a compiled limit";
+    case PLIS_ERR_NO_DEVICE: return "no CUDA device";
+    case PLIS_ERR_UNSUPPORTED: return "unsupported";
+    default: return "unknown status";
+  }
+}
+
+void plis_options_init(plis_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof *o);
+  o->size = sizeof *o;
+  o->mode = PLIS_MODE_REFERENCE;
+  o->precision = PLIS_PREC_FP64;
+  o->critical_threshold = 10;  // driver.cu:36
+  o->epsilon = 0.05;           // driver.cu:37
+  o->seed = 1;
+  o->device = 0;
+  o->max_rollbacks = 64;
+  o->steps_per_launch = 0;
+  o->persistent = -1;
+}
+
+int plis_create(const plis_model_desc* model, const plis_options* opts, plis_handle** out) {
+  PLIS_GUARD_BEGIN
+  if (!model || !out) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  *out = nullptr;
+  plis_options o;
+  plis_options_init(&o);
+  if (opts) {
+    if (opts->size != sizeof(plis_options)) { g_err = "plis_options.size mismatch (call plis_options_init)"; return PLIS_ERR_INVALID; }
+    o = *opts;
+  }
+  if (o.mode != PLIS_MODE_REFERENCE && o.mode != PLIS_MODE_CORRECTED) { g_err = "unknown mode"; return PLIS_ERR_INVALID; }
+  if (o.precision != PLIS_PREC_FP64 && o.precision != PLIS_PREC_FP32) { g_err = "unknown precision"; return PLIS_ERR_INVALID; }
+  if (o.critical_threshold < 0 || !(o.epsilon > 0.0) || o.max_rollbacks < 0 || o.max_rollbacks > 4000) {
+    g_err = "critical_threshold, epsilon or max_rollbacks out of range";
+    return PLIS_ERR_INVALID;
+  }
+  plis::Model m;
+  std::string err;
+  int rc = plis::build_model(model, &m, &err);
+  if (rc) { g_err = err; return rc; }
+  plis_handle* h = new plis_handle();
+  rc = h->eng.create(m, o);
+  if (rc) {
+    g_err = h->eng.error();
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return PLIS_OK;
+  PLIS_GUARD_END
+}
+
+int plis_destroy(plis_handle* h) {
+  PLIS_GUARD_BEGIN
+  delete h;
+  return PLIS_OK;
+  PLIS_GUARD_END
+}
+
+int plis_set_state(plis_handle* h, const uint32_t* counts) {
+  PLIS_GUARD_BEGIN
+  if (!h || !counts) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return fail(h, h->eng.set_state(counts));
+  PLIS_GUARD_END
+}
+
+int plis_get_state(plis_handle* h, uint32_t* counts) {
+  PLIS_GUARD_BEGIN
+  if (!h || !counts) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return fail(h, h->eng.get_state(counts));
+  PLIS_GUARD_END
+}
+
+int plis_set_time(plis_handle* h, double t) {
+  PLIS_GUARD_BEGIN
+  if (!h) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return fail(h, h->eng.set_time(t));
+  PLIS_GUARD_END
+}
+
+int plis_run(plis_handle* h, double t_end) {
+  PLIS_GUARD_BEGIN
+  if (!h) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return fail(h, h->eng.advance(t_end, ~0ull));
+  PLIS_GUARD_END
+}
+
+int plis_step(plis_handle* h, uint64_t n) {
+  PLIS_GUARD_BEGIN
+  if (!h) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return fail(h, h->eng.advance(__builtin_inf(), n));
+  PLIS_GUARD_END
+}
+
+int plis_get_stats(plis_handle* h, plis_stats* st) {
+  PLIS_GUARD_BEGIN
+  if (!h || !st) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return fail(h, h->eng.stats(st));
+  PLIS_GUARD_END
+}
+
+int plis_get_profile(plis_handle* h, plis_profile* p) {
+  PLIS_GUARD_BEGIN
+  if (!h || !p) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return fail(h, h->eng.profile(p));
+  PLIS_GUARD_END
+}
+
+int plis_get_taus(plis_handle* h, double* tau, uint8_t* flags) {
+  PLIS_GUARD_BEGIN
+  if (!h) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return fail(h, h->eng.get_taus(tau, flags));
+  PLIS_GUARD_END
+}
+
+int plis_canonical_neighbours(uint32_t n, const uint32_t* table, const uint32_t lattice_in[3], uint32_t* canonical,
+                              uint32_t lattice_out[3]) {
+  PLIS_GUARD_BEGIN
+  if (!canonical) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  plis::Topology t;
+  std::string err;
+  int rc = plis::canonicalize(n, table, lattice_in, &t, &err);
+  if (rc) { g_err = err; return rc; }
+  if (lattice_out) std::memcpy(lattice_out, t.lattice, sizeof t.lattice);
+  if (!t.canon.empty()) {
+    std::memcpy(canonical, t.canon.data(), t.canon.size() * sizeof(uint32_t));
+  } else {
+    uint32_t buf[6];
+    for (uint32_t c = 0; c < n; ++c) {
+      int k = plis::lattice_row(t.lattice, c, buf);
+      for (int j = 0; j < 6; ++j) canonical[(size_t)c * 6 + j] = j < k ? buf[j] : c;
+    }
+  }
+  return PLIS_OK;
+  PLIS_GUARD_END
+}
+
+}  // extern "C"

@@ -1,0 +1,400 @@
+// engine.cu — host side of the B200 step: buffers, control block, CUDA-graph batches.
+//
+// The device phases are in engine_kernels.cuh; their template instantiations are compiled in
+// inst_f64.cu / inst_f32.cu so the build parallelises.
+#define PLIS_ENGINE_HOST_TU 1
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "engine_kernels.cuh"
+#include "plis_model.h"
+
+namespace plis {
+
+// ------------------------------------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------------------------------------
+#define PLIS_CU(call)                                                                    \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess) {                                                             \
+      err_ = std::string(#call) + ": " + cudaGetErrorString(e_);                          \
+      return e_ == cudaErrorMemoryAllocation ? PLIS_ERR_OOM : PLIS_ERR_CUDA;             \
+    }                                                                                    \
+  } while (0)
+
+static uint32_t pow2_at_least(uint32_t v) {
+  uint32_t p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+Engine::Engine() {}
+
+Engine::~Engine() { release(); }
+
+void Engine::release() {
+  if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+  graph_exec_ = nullptr;
+  for (void* p : allocs_) cudaFree(p);
+  allocs_.clear();
+  if (h_ctrl_) cudaFreeHost(h_ctrl_);
+  h_ctrl_ = nullptr;
+  for (auto& e : pev_)
+    if (e) { cudaEventDestroy(e); e = nullptr; }
+  if (ev0_) cudaEventDestroy(ev0_);
+  if (ev1_) cudaEventDestroy(ev1_);
+  ev0_ = ev1_ = nullptr;
+  if (stream_) cudaStreamDestroy(stream_);
+  stream_ = nullptr;
+}
+
+int Engine::dmalloc(void** p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+  if (e != cudaSuccess) {
+    err_ = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? PLIS_ERR_OOM : PLIS_ERR_CUDA;
+  }
+  allocs_.push_back(*p);
+  return PLIS_OK;
+}
+
+template <typename T>
+int Engine::upload(const std::vector<T>& v, const T** out) {
+  void* p = nullptr;
+  int rc = dmalloc(&p, v.size() * sizeof(T));
+  if (rc) return rc;
+  if (!v.empty()) PLIS_CU(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  *out = (const T*)p;
+  return PLIS_OK;
+}
+
+int Engine::create(const Model& model, const plis_options& opt) {
+  model_ = model;
+  opt_ = opt;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    err_ = "No CUDA-capable device detected.";
+    return PLIS_ERR_NO_DEVICE;
+  }
+  if (opt.device < 0 || opt.device >= ndev) { err_ = "device ordinal out of range"; return PLIS_ERR_INVALID; }
+  PLIS_CU(cudaSetDevice(opt.device));
+  PLIS_CU(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  PLIS_CU(cudaEventCreate(&ev0_));
+  PLIS_CU(cudaEventCreate(&ev1_));
+  PLIS_CU(cudaMallocHost((void**)&h_ctrl_, sizeof(Ctrl)));
+  std::memset(h_ctrl_, 0, sizeof(Ctrl));
+
+  const Model& M = model_;
+  DevModel& dm = args_.m;
+  std::memset(&dm, 0, sizeof dm);
+  dm.N = M.N; dm.S = M.S; dm.R = M.R; dm.C = M.C;
+  dm.Npad = (M.N + 31u) & ~31u;
+  dm.lattice = M.topo.is_lattice() ? 1u : 0u;
+  dm.X = M.topo.lattice[0]; dm.Y = M.topo.lattice[1]; dm.Z = M.topo.lattice[2];
+  int rc;
+  if (!dm.lattice) {
+    if ((rc = upload(M.topo.canon, &dm.canon))) return rc;
+    if ((rc = upload(M.topo.ncount, &dm.ncount))) return rc;
+  }
+  if (!M.topo.orig.empty()) {
+    if ((rc = upload(M.topo.orig, &dm.orig))) return rc;
+  }
+  if (!M.comp.empty()) {
+    if ((rc = upload(M.comp, &dm.comp))) return rc;
+  }
+  const ReactionTables& t = M.rt;
+  if ((rc = upload(t.n_reac, &dm.n_reac))) return rc;
+  if ((rc = upload(t.n_net, &dm.n_net))) return rc;
+  if ((rc = upload(t.reac_s, &dm.reac_s))) return rc;
+  if ((rc = upload(t.reac_m, &dm.reac_m))) return rc;
+  if ((rc = upload(t.reac_nu, &dm.reac_nu))) return rc;
+  if ((rc = upload(t.net_s, &dm.net_s))) return rc;
+  if ((rc = upload(t.net_nu, &dm.net_nu))) return rc;
+  if ((rc = upload(t.inv_denom, &dm.inv_denom))) return rc;
+  if ((rc = upload(t.hor, &dm.hor))) return rc;
+  if ((rc = upload(t.hmult, &dm.hmult))) return rc;
+  if ((rc = upload(t.sp_off, &dm.sp_off))) return rc;
+  if ((rc = upload(t.sp_r, &dm.sp_r))) return rc;
+  if ((rc = upload(t.sp_nu, &dm.sp_nu))) return rc;
+  if ((rc = upload(t.sr_off, &dm.sr_off))) return rc;
+  if ((rc = upload(t.sr_r, &dm.sr_r))) return rc;
+  if (opt.precision == PLIS_PREC_FP32) {
+    std::vector<float> rr(M.rrate.begin(), M.rrate.end()), dr(M.drate.begin(), M.drate.end());
+    const float* p;
+    if ((rc = upload(rr, &p))) return rc;
+    dm.rr = p;
+    if ((rc = upload(dr, &p))) return rc;
+    dm.dr = p;
+  } else {
+    const double* p;
+    if ((rc = upload(M.rrate, &p))) return rc;
+    dm.rr = p;
+    if ((rc = upload(M.drate, &p))) return rc;
+    dm.dr = p;
+  }
+
+  // geometry
+  Geo& g = args_.g;
+  if (dm.lattice) {
+    uint32_t tx = opt.tile[0] > 0 ? (uint32_t)opt.tile[0] : std::min<uint32_t>(32, pow2_at_least(dm.X));
+    uint32_t ty = opt.tile[1] > 0 ? (uint32_t)opt.tile[1] : std::min<uint32_t>(std::max<uint32_t>(1, 256 / tx), pow2_at_least(dm.Y));
+    uint32_t tz = opt.tile[2] > 0 ? (uint32_t)opt.tile[2] : std::min<uint32_t>(std::max<uint32_t>(1, 256 / (tx * ty)), pow2_at_least(dm.Z));
+    if (tx * ty * tz > 512 || tx * ty * tz == 0) { err_ = "tile has more than 512 subvolumes"; return PLIS_ERR_INVALID; }
+    g.tx = tx; g.ty = ty; g.tz = tz;
+    g.ntx = (dm.X + tx - 1) / tx; g.nty = (dm.Y + ty - 1) / ty; g.ntz = (dm.Z + tz - 1) / tz;
+    g.threads = tx * ty * tz;
+    const uint64_t nb = (uint64_t)g.ntx * g.nty * g.ntz;
+    if (nb > 0x7FFFFFFFull) { err_ = "grid too large"; return PLIS_ERR_LIMIT; }
+    g.nblocks = (uint32_t)nb;
+  } else {
+    g.tx = 256; g.ty = g.tz = 1;
+    g.threads = 256;
+    g.nblocks = (dm.N + 255) / 256;
+    g.ntx = g.nblocks; g.nty = g.ntz = 1;
+  }
+
+  // buffers
+  const size_t cells = (size_t)M.S * dm.Npad;
+  DevBufs& b = args_.b;
+  for (int i = 0; i < 3; ++i)
+    if ((rc = dmalloc((void**)&b.X[i], cells * 4))) return rc;
+  for (int i = 0; i < 2; ++i) {
+    if ((rc = dmalloc((void**)&b.tau[i], (size_t)dm.Npad * 8))) return rc;
+    if ((rc = dmalloc((void**)&b.flag[i], (size_t)dm.Npad))) return rc;
+  }
+  if ((rc = dmalloc((void**)&b.D, cells * 4))) return rc;
+  PLIS_CU(cudaMemset(b.D, 0, cells * 4));
+  if ((rc = dmalloc((void**)&b.slot_tau, (size_t)g.nblocks * 8))) return rc;
+  if ((rc = dmalloc((void**)&b.slot_idx, (size_t)g.nblocks * 8))) return rc;
+  if ((rc = dmalloc((void**)&b.slot_cr, (size_t)g.nblocks * 4))) return rc;
+  if ((rc = dmalloc((void**)&b.slot_bad, (size_t)g.nblocks * 4))) return rc;
+  if ((rc = dmalloc((void**)&b.ctrl, sizeof(Ctrl)))) return rc;
+  PLIS_CU(cudaMemset(b.ctrl, 0, sizeof(Ctrl)));
+
+  DevOpts& o = args_.o;
+  o.mode = opt.mode;
+  o.nc = opt.critical_threshold;
+  o.max_rollbacks = opt.max_rollbacks;
+  o.eps = opt.epsilon;
+  o.seed = opt.seed;
+  o.replica = opt.replica;
+
+  launch_ = (opt.precision == PLIS_PREC_FP32) ? pick_f32(M.S) : pick_f64(M.S);
+  kernels_per_step_ = (opt.mode == PLIS_MODE_REFERENCE) ? 4 : 3;
+  graph_steps_ = opt.steps_per_launch > 0 ? opt.steps_per_launch : 32;
+  PLIS_CU(cudaDeviceSynchronize());
+  return PLIS_OK;
+}
+
+void Engine::enqueue_step() {
+  const dim3 gc(args_.g.nblocks), bc(args_.g.threads);
+  const dim3 gx((args_.m.N + 255) / 256), bx(256);
+  launch_.leap(args_, gc, bc, stream_);
+  launch_.exact(args_, gx, bx, stream_);
+  if (opt_.mode == PLIS_MODE_REFERENCE) k_apply<<<gx, bx, 0, stream_>>>(args_);
+  launch_.classify(args_, gc, bc, stream_);
+}
+
+// Profiled step: the same four launches with CUDA events between them, accumulated per kernel.
+int Engine::enqueue_step_profiled() {
+  const dim3 gc(args_.g.nblocks), bc(args_.g.threads);
+  const dim3 gx((args_.m.N + 255) / 256), bx(256);
+  for (auto& e : pev_)
+    if (!e) PLIS_CU(cudaEventCreate(&e));
+  PLIS_CU(cudaEventRecord(pev_[0], stream_));
+  launch_.leap(args_, gc, bc, stream_);
+  PLIS_CU(cudaEventRecord(pev_[1], stream_));
+  launch_.exact(args_, gx, bx, stream_);
+  PLIS_CU(cudaEventRecord(pev_[2], stream_));
+  if (opt_.mode == PLIS_MODE_REFERENCE) k_apply<<<gx, bx, 0, stream_>>>(args_);
+  PLIS_CU(cudaEventRecord(pev_[3], stream_));
+  launch_.classify(args_, gc, bc, stream_);
+  PLIS_CU(cudaEventRecord(pev_[4], stream_));
+  PLIS_CU(cudaEventSynchronize(pev_[4]));
+  const int kind[4] = {PLIS_KERNEL_LEAP, PLIS_KERNEL_EXACT, PLIS_KERNEL_APPLY, PLIS_KERNEL_CLASSIFY};
+  for (int i = 0; i < 4; ++i) {
+    if (i == 2 && opt_.mode != PLIS_MODE_REFERENCE) continue;
+    float ms = 0.f;
+    PLIS_CU(cudaEventElapsedTime(&ms, pev_[i], pev_[i + 1]));
+    prof_.ms[kind[i]] += ms;
+    prof_.launches[kind[i]] += 1;
+  }
+  return PLIS_OK;
+}
+
+int Engine::profile(plis_profile* p) {
+  *p = prof_;
+  return PLIS_OK;
+}
+
+int Engine::build_graph() {
+  if (graph_exec_) return PLIS_OK;
+  cudaGraph_t graph = nullptr;
+  PLIS_CU(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+  for (int i = 0; i < graph_steps_; ++i) enqueue_step();
+  PLIS_CU(cudaStreamEndCapture(stream_, &graph));
+  cudaError_t e = cudaGraphInstantiate(&graph_exec_, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    err_ = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e);
+    graph_exec_ = nullptr;
+    return PLIS_ERR_CUDA;
+  }
+  return PLIS_OK;
+}
+
+int Engine::read_ctrl() {
+  PLIS_CU(cudaMemcpyAsync(h_ctrl_, args_.b.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, stream_));
+  PLIS_CU(cudaStreamSynchronize(stream_));
+  return PLIS_OK;
+}
+
+int Engine::set_state(const uint32_t* counts) {
+  const DevModel& dm = args_.m;
+  for (size_t i = 0; i < (size_t)dm.S * dm.N; ++i)
+    if (counts[i] >= (1u << 30)) {
+      err_ = "counts must be below 2^30";
+      return PLIS_ERR_OVERFLOW;
+    }
+  const size_t cells = (size_t)dm.S * dm.Npad;
+  PLIS_CU(cudaMemsetAsync(args_.b.X[0], 0, cells * 4, stream_));
+  PLIS_CU(cudaMemcpy2DAsync(args_.b.X[0], (size_t)dm.Npad * 4, counts, (size_t)dm.N * 4, (size_t)dm.N * 4, dm.S,
+                            cudaMemcpyHostToDevice, stream_));
+  PLIS_CU(cudaMemsetAsync(args_.b.X[1], 0, cells * 4, stream_));
+  PLIS_CU(cudaMemsetAsync(args_.b.X[2], 0, cells * 4, stream_));
+  PLIS_CU(cudaMemsetAsync(args_.b.D, 0, cells * 4, stream_));
+  k_fill_tau<<<(dm.Npad + 255) / 256, 256, 0, stream_>>>(args_.b.tau[0], args_.b.flag[0], dm.Npad);
+  k_fill_tau<<<(dm.Npad + 255) / 256, 256, 0, stream_>>>(args_.b.tau[1], args_.b.flag[1], dm.Npad);
+  Ctrl k;
+  std::memset(&k, 0, sizeof k);
+  k.cur = 0; k.tgt = 1; k.spare = 2; k.tf = 0;
+  k.phase = 0;
+  k.done = 0;
+  k.argmin = -1;
+  k.last_argmin = -1;
+  k.t_end = 0.0;
+  *h_ctrl_ = k;
+  PLIS_CU(cudaMemcpyAsync(args_.b.ctrl, h_ctrl_, sizeof(Ctrl), cudaMemcpyHostToDevice, stream_));
+  launch_.classify(args_, dim3(args_.g.nblocks), dim3(args_.g.threads), stream_);
+  launches_ += 3;
+  PLIS_CU(cudaGetLastError());
+  int rc = read_ctrl();
+  if (rc) return rc;
+  device_ms_ = 0.0;
+  std::memset(&prof_, 0, sizeof prof_);
+  return PLIS_OK;
+}
+
+int Engine::set_time(double t) {
+  int rc = read_ctrl();
+  if (rc) return rc;
+  h_ctrl_->t = t;
+  PLIS_CU(cudaMemcpyAsync(&args_.b.ctrl->t, &h_ctrl_->t, sizeof(double), cudaMemcpyHostToDevice, stream_));
+  PLIS_CU(cudaStreamSynchronize(stream_));
+  return PLIS_OK;
+}
+
+int Engine::get_state(uint32_t* counts) {
+  int rc = read_ctrl();
+  if (rc) return rc;
+  const DevModel& dm = args_.m;
+  PLIS_CU(cudaMemcpy2DAsync(counts, (size_t)dm.N * 4, args_.b.X[h_ctrl_->cur], (size_t)dm.Npad * 4, (size_t)dm.N * 4,
+                            dm.S, cudaMemcpyDeviceToHost, stream_));
+  PLIS_CU(cudaStreamSynchronize(stream_));
+  return PLIS_OK;
+}
+
+int Engine::get_taus(double* tau, uint8_t* flags) {
+  int rc = read_ctrl();
+  if (rc) return rc;
+  const uint32_t tf = h_ctrl_->tf;
+  if (tau) PLIS_CU(cudaMemcpyAsync(tau, args_.b.tau[tf], (size_t)args_.m.N * 8, cudaMemcpyDeviceToHost, stream_));
+  if (flags) PLIS_CU(cudaMemcpyAsync(flags, args_.b.flag[tf], args_.m.N, cudaMemcpyDeviceToHost, stream_));
+  PLIS_CU(cudaStreamSynchronize(stream_));
+  return PLIS_OK;
+}
+
+int Engine::advance(double t_end, uint64_t n_steps) {
+  PLIS_CU(cudaEventRecord(ev0_, stream_));
+  k_prepare<<<1, 32, 0, stream_>>>(args_, t_end, (unsigned long long)n_steps);
+  launches_ += 1;
+  PLIS_CU(cudaGetLastError());
+  if (opt_.profile) {  // one step at a time, events around every kernel
+    while (true) {
+      int rc = enqueue_step_profiled();
+      if (rc) return rc;
+      launches_ += kernels_per_step_;
+      PLIS_CU(cudaGetLastError());
+      rc = read_ctrl();
+      if (rc) return rc;
+      if (h_ctrl_->done) break;
+    }
+    PLIS_CU(cudaEventRecord(ev1_, stream_));
+    PLIS_CU(cudaEventSynchronize(ev1_));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev0_, ev1_);
+    device_ms_ += ms;
+    if (h_ctrl_->status != PLIS_OK) { err_ = "device step failed"; return h_ctrl_->status; }
+    return PLIS_OK;
+  }
+  const bool few = n_steps != ~0ull && n_steps < (uint64_t)graph_steps_;
+  if (!few) {
+    int rc = build_graph();
+    if (rc) return rc;
+  }
+  uint64_t budget = few ? n_steps : 0;
+  while (true) {
+    if (few) {
+      for (uint64_t i = 0; i < budget; ++i) enqueue_step();
+      launches_ += budget * kernels_per_step_;
+    } else {
+      PLIS_CU(cudaGraphLaunch(graph_exec_, stream_));
+      launches_ += (uint64_t)graph_steps_ * kernels_per_step_;
+    }
+    PLIS_CU(cudaGetLastError());
+    int rc = read_ctrl();
+    if (rc) return rc;
+    if (h_ctrl_->done) break;
+    if (few) {  // rollbacks used up some of the per-call launches
+      budget = 1;
+    }
+  }
+  PLIS_CU(cudaEventRecord(ev1_, stream_));
+  PLIS_CU(cudaEventSynchronize(ev1_));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ev0_, ev1_);
+  device_ms_ += ms;
+  if (h_ctrl_->status != PLIS_OK) {
+    err_ = h_ctrl_->status == PLIS_ERR_STUCK ? "too many consecutive rollbacks in one step" : "device step failed";
+    return h_ctrl_->status;
+  }
+  return PLIS_OK;
+}
+
+int Engine::stats(plis_stats* st) {
+  int rc = read_ctrl();
+  if (rc) return rc;
+  const Ctrl& k = *h_ctrl_;
+  std::memset(st, 0, sizeof *st);
+  st->time = k.t;
+  st->steps = k.step;
+  st->rollbacks = k.rollbacks;
+  st->events = k.events;
+  st->exact_events = k.exact_events;
+  st->stop_reason = k.stop_reason;
+  st->status = k.status;
+  st->last_tau = k.last_tau;
+  st->last_argmin = k.last_argmin;
+  st->device_ms = device_ms_;
+  st->kernel_launches = launches_;
+  return PLIS_OK;
+}
+
+}  // namespace plis

@@ -1,0 +1,109 @@
+// engine.cuh — device-side data of the B200 step: control block, model view, kernel arguments.
+#ifndef PLIS_ENGINE_CUH_
+#define PLIS_ENGINE_CUH_
+
+#include <stdint.h>
+
+namespace plis {
+
+enum : uint8_t { F_LEAP_CR = 0, F_LEAP_NOCR = 1, F_SSA = 2, F_SSA_FF = 3 };  // constants.cuh:53-58
+
+// Guards keeping every per-step sum inside int32 (identical rules in the host oracle).
+constexpr int64_t kBigDraw = (int64_t)1 << 29;  // |k * nu| of one reaction draw
+constexpr int64_t kBigJump = (int64_t)1 << 27;  // k of one diffusion draw
+constexpr int64_t kBigTile = (int64_t)1 << 30;  // |x + own delta| of one subvolume
+
+// The whole control state of a simulation lives on the device, so a batch of steps (rollbacks
+// included) runs without the host: the reference instead reads the arg-min back and decides on
+// the host every step (driver.cu:267-315).
+struct Ctrl {
+  double t_end;          // stop once t >= t_end
+  uint64_t max_step;     // stop once step >= max_step
+  double t;              // simulated time (binary64)
+  uint64_t step;         // accepted steps
+  double tau_min;        // arg-min of the current taus (first index on ties)
+  int64_t argmin;
+  double tau_step;       // corrected mode: tau_min clamped onto t_end
+  double tau_leap;       // tau used by the leap of the current attempt
+  double dt;             // time increment of the current attempt
+  double last_tau;
+  int64_t last_argmin;
+  uint32_t attempt;      // rollbacks so far in the current step
+  uint32_t exact;        // bit0: critical events in LEAP_CR subvolumes; bit1: arg-min exact event
+  uint32_t n_leap_cr;
+  uint32_t argmin_flag;
+  uint32_t cur, tgt, spare, tf;  // count buffer rotation and tau/flag double-buffer index
+  uint32_t phase;        // 0: initial classification pending, 1: stepping
+  int32_t done, status, stop_reason;
+  uint32_t blocks_done;
+  uint32_t pad_;
+  unsigned long long events, exact_events, rollbacks;
+  unsigned long long ev_attempt, ex_attempt;
+};
+
+struct DevModel {
+  uint32_t N, S, R, C;
+  uint32_t X, Y, Z, lattice;
+  uint32_t Npad;
+  const uint32_t* canon;   // [6N] (table topology)
+  const uint8_t* ncount;   // [N]  (table topology)
+  const uint32_t* orig;    // [6N] table as given (reference quirk of leap.cu:192-193), may be null
+  const int32_t* comp;     // [N] or null
+  const uint8_t* n_reac;
+  const uint8_t* n_net;
+  const uint16_t* reac_s;
+  const uint8_t* reac_m;
+  const int16_t* reac_nu;
+  const uint16_t* net_s;
+  const int16_t* net_nu;
+  const double* inv_denom;
+  const uint8_t* hor;
+  const uint8_t* hmult;
+  const uint16_t* sp_off;
+  const uint16_t* sp_r;
+  const int16_t* sp_nu;
+  const uint16_t* sr_off;
+  const uint16_t* sr_r;
+  const void* rr;   // Real [C][R]
+  const void* dr;   // Real [C][S]
+};
+
+struct DevBufs {
+  int32_t* X[3];
+  double* tau[2];
+  uint8_t* flag[2];
+  int32_t* D;
+  double* slot_tau;
+  long long* slot_idx;
+  uint32_t* slot_cr;
+  uint32_t* slot_bad;
+  Ctrl* ctrl;
+};
+
+struct DevOpts {
+  int32_t mode;
+  int32_t nc;
+  int32_t max_rollbacks;
+  int32_t pad_;
+  double eps;
+  unsigned long long seed;
+  uint32_t replica;
+};
+
+struct Geo {
+  uint32_t tx, ty, tz;     // lattice brick per CTA
+  uint32_t ntx, nty, ntz;  // bricks per dimension
+  uint32_t nblocks;        // CTAs of the cell kernels
+  uint32_t threads;        // threads per CTA
+};
+
+struct KArgs {
+  DevModel m;
+  DevBufs b;
+  DevOpts o;
+  Geo g;
+};
+
+}  // namespace plis
+
+#endif

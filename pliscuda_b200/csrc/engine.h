@@ -1,0 +1,68 @@
+// engine.h — host-side owner of one simulation on one device (one plis_handle).
+#ifndef PLIS_ENGINE_H_
+#define PLIS_ENGINE_H_
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/plis.h"
+#include "engine.cuh"
+#include "plis_model.h"
+
+namespace plis {
+
+// Kernel launchers of one (precision, species-capacity) instantiation.
+struct Launchers {
+  void (*leap)(const KArgs&, dim3, dim3, cudaStream_t);
+  void (*exact)(const KArgs&, dim3, dim3, cudaStream_t);
+  void (*classify)(const KArgs&, dim3, dim3, cudaStream_t);
+};
+
+class Engine {
+ public:
+  Engine();
+  ~Engine();
+  int create(const Model& model, const plis_options& opt);
+  int set_state(const uint32_t* counts);
+  int get_state(uint32_t* counts);
+  int set_time(double t);
+  int get_taus(double* tau, uint8_t* flags);
+  int advance(double t_end, uint64_t n_steps);
+  int stats(plis_stats* st);
+  int profile(plis_profile* p);
+  const std::string& error() const { return err_; }
+  const Model& model() const { return model_; }
+
+ private:
+  void release();
+  int dmalloc(void** p, size_t bytes);
+  template <typename T> int upload(const std::vector<T>& v, const T** out);
+  void enqueue_step();
+  int build_graph();
+  int read_ctrl();
+
+  Model model_;
+  plis_options opt_{};
+  KArgs args_{};
+  Launchers launch_{};
+  cudaStream_t stream_ = nullptr;
+  cudaGraphExec_t graph_exec_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  Ctrl* h_ctrl_ = nullptr;
+  std::vector<void*> allocs_;
+  std::string err_;
+  int graph_steps_ = 32;
+  int kernels_per_step_ = 4;
+  uint64_t launches_ = 0;
+  double device_ms_ = 0.0;
+  plis_profile prof_{};
+  cudaEvent_t pev_[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  int enqueue_step_profiled();
+};
+
+}  // namespace plis
+
+#endif

@@ -1,0 +1,920 @@
+// engine_kernels.cuh — the device phases of the B200 simulation step (sm_100a).
+//
+// One tau-leaping step of the reference (PLISCuda/src/driver.cu:259-376) is four device phases,
+// with every decision taken on the device so that batches of steps replay as one CUDA graph:
+//
+//   k_leap      Poisson firings of non-critical reactions and per-neighbour diffusions of every
+//               LEAP subvolume (leap.cu:3-65).  Each thread owns one subvolume of a lattice brick;
+//               the brick's own values and the molecules it sends are reduced into the zeroed
+//               target buffer with int32 atomics (commutative, so the result is deterministic).
+//   k_exact     the single critical event of every LEAP_CR subvolume (leap.cu:67-199) and the exact
+//               event of the arg-min subvolume (ssa.cu:270-324).  Decisions read the pre-step counts
+//               and the post-leap counts; the reference's race on the latter (leap.cu:131-134) is
+//               gone because the changes are staged in a delta buffer.
+//   k_apply     adds the staged deltas (reference mode with critical events only).
+//   k_classify  negativity check (check_state, leap.cu:203-212), rates, criticality, Cao tau,
+//               tau_cr, flags and fast-forward (rates.cu, tau.cu:197-252) of the post-step state,
+//               a warp-shuffle + CTA min-tau with arg-min, and in the last CTA to finish: the
+//               grid-wide arg-min, rollback-or-accept, the time update and the next step's plan
+//               (driver.cu:267-334).  It also zeroes the buffer the next leap will reduce into.
+//
+// Counts are int32 species-major [S][Npad] in three rotating buffers (current, target, spare), so
+// accepting a step is an index rotation and a rollback discards the target: no device-to-device
+// copies (the reference copies the state twice per step, driver.cu:303, :323).
+#ifndef PLIS_ENGINE_KERNELS_CUH_
+#define PLIS_ENGINE_KERNELS_CUH_
+
+#include <cuda_runtime.h>
+
+#include "../../include/plis.h"
+#include "engine.cuh"
+#include "engine.h"
+#include "plis_stream.h"
+
+namespace plis {
+
+// ------------------------------------------------------------------------------------------------
+// precision traits
+// ------------------------------------------------------------------------------------------------
+template <typename Real> struct RT;
+template <> struct RT<double> {
+  static __device__ __forceinline__ double poisson(plis_stream* s, double lam) { return plis_poisson_d(s, lam); }
+  static __device__ __forceinline__ double uniform(plis_stream* s) { return plis_uniform_d(s); }
+  static __device__ __forceinline__ long long count(double k) { return plis_count_d(k); }
+  static __device__ __forceinline__ double inf() { return PLIS_INF_D; }
+};
+template <> struct RT<float> {
+  static __device__ __forceinline__ float poisson(plis_stream* s, float lam) { return plis_poisson_f(s, lam); }
+  static __device__ __forceinline__ float uniform(plis_stream* s) { return plis_uniform_f(s); }
+  static __device__ __forceinline__ long long count(float k) { return plis_count_f(k); }
+  static __device__ __forceinline__ float inf() { return PLIS_INF_F; }
+};
+
+// Per-thread copy of one subvolume's counts.  Small species counts stay in registers: the
+// selection loops below use compile-time indices only.
+template <int MAXS> struct Counts {
+  int32_t v[MAXS];
+  __device__ __forceinline__ int32_t get(int s) const {
+    if (MAXS <= 8) {
+      int32_t r = 0;
+#pragma unroll
+      for (int i = 0; i < MAXS; ++i)
+        if (i == s) r = v[i];
+      return r;
+    }
+    return v[s];
+  }
+};
+template <int MAXS> struct Deltas {
+  long long v[MAXS];
+  __device__ __forceinline__ void add(int s, long long d) {
+    if (MAXS <= 8) {
+#pragma unroll
+      for (int i = 0; i < MAXS; ++i)
+        if (i == s) v[i] += d;
+      return;
+    }
+    v[s] += d;
+  }
+};
+
+// ------------------------------------------------------------------------------------------------
+// geometry
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ bool cell_of(const KArgs& A, uint32_t& c) {
+  if (A.m.lattice) {
+    const uint32_t b = blockIdx.x, t = threadIdx.x;
+    const uint32_t bx = b % A.g.ntx, br = b / A.g.ntx;
+    const uint32_t by = br % A.g.nty, bz = br / A.g.nty;
+    const uint32_t lx = t % A.g.tx, tr = t / A.g.tx;
+    const uint32_t ly = tr % A.g.ty, lz = tr / A.g.ty;
+    const uint32_t x = bx * A.g.tx + lx, y = by * A.g.ty + ly, z = bz * A.g.tz + lz;
+    if (x >= A.m.X || y >= A.m.Y || z >= A.m.Z) return false;
+    c = x + A.m.X * (y + A.m.Y * z);
+    return true;
+  }
+  c = blockIdx.x * blockDim.x + threadIdx.x;
+  return c < A.m.N;
+}
+
+// canonical neighbours: lattice rows -x,+x,-y,+y,-z,+z (absent ones skipped), else the table
+__device__ __forceinline__ int nbrs(const DevModel& m, uint32_t c, uint32_t nb[6]) {
+  if (m.lattice) {
+    const uint32_t X = m.X, Y = m.Y, Z = m.Z;
+    const uint32_t x = c % X, y = (c / X) % Y, z = c / (X * Y);
+    int n = 0;
+    if (x > 0) nb[n++] = c - 1;
+    if (x + 1 < X) nb[n++] = c + 1;
+    if (y > 0) nb[n++] = c - X;
+    if (y + 1 < Y) nb[n++] = c + X;
+    if (z > 0) nb[n++] = c - X * Y;
+    if (z + 1 < Z) nb[n++] = c + X * Y;
+    return n;
+  }
+  const int n = m.ncount[c];
+#pragma unroll
+  for (int j = 0; j < 6; ++j) nb[j] = m.canon[(size_t)c * 6 + j];
+  return n;
+}
+
+__device__ __forceinline__ int nbr_count(const DevModel& m, uint32_t b) {
+  if (m.lattice) {
+    const uint32_t X = m.X, Y = m.Y, Z = m.Z;
+    const uint32_t x = b % X, y = (b / X) % Y, z = b / (X * Y);
+    return (x > 0) + (x + 1 < X) + (y > 0) + (y + 1 < Y) + (z > 0) + (z + 1 < Z);
+  }
+  return m.ncount[b];
+}
+
+// slot-th entry of the canonical 6-wide row of c (self padding beyond the neighbour count)
+__device__ __forceinline__ uint32_t canon_slot(const DevModel& m, uint32_t c, int slot) {
+  if (!m.lattice) return m.canon[(size_t)c * 6 + slot];
+  uint32_t nb[6];
+  const int n = nbrs(m, c, nb);
+  uint32_t r = c;
+#pragma unroll
+  for (int j = 0; j < 6; ++j)
+    if (j == slot && j < n) r = nb[j];
+  return r;
+}
+
+// the flat table entry the reference reads at leap.cu:192 (neigh.index[rdi])
+__device__ __forceinline__ uint32_t flat_table_entry(const DevModel& m, uint32_t flat) {
+  if (m.orig) return m.orig[flat];
+  return canon_slot(m, flat / 6, (int)(flat % 6));
+}
+
+__device__ __forceinline__ int comp_of(const DevModel& m, uint32_t c) { return m.comp ? m.comp[c] : 0; }
+
+// ------------------------------------------------------------------------------------------------
+// per-subvolume rates (rates.cu:3-96) and criticality (tau.cu:3-45)
+// ------------------------------------------------------------------------------------------------
+template <typename Real, int MAXS>
+__device__ __forceinline__ Real prop(const DevModel& m, const Counts<MAXS>& x, int r, int comp) {
+  const Real* rr = (const Real*)m.rr;
+  const int nr = m.n_reac[r];
+  Real prod = (Real)1;
+  for (int i = 0; i < nr; ++i) {
+    const int s = m.reac_s[r * 3 + i];
+    const int mu = m.reac_m[r * 3 + i];
+    const Real xs = (Real)x.get(s);
+    for (int j = 0; j < mu; ++j) prod = prod * (xs - (Real)j);
+  }
+  return (rr[(size_t)comp * m.R + r] * prod) * (Real)m.inv_denom[r];
+}
+
+template <typename Real>
+__device__ __forceinline__ Real drate(const DevModel& m, int comp, int s) {
+  return ((const Real*)m.dr)[(size_t)comp * m.S + s];
+}
+
+// reference criticality: the first two reactant species decide (tau.cu:3-40)
+template <int MAXS>
+__device__ __forceinline__ bool crit_ref(const DevModel& m, const Counts<MAXS>& x, int r, int nc) {
+  const int nr = m.n_reac[r];
+  const int lim = nr < 2 ? nr : 2;
+  bool crit = false;
+  for (int i = 0; i < lim; ++i) {
+    const int s = m.reac_s[r * 3 + i];
+    const int32_t xs = x.get(s);
+    if (xs == 0) return true;
+    const int nu = m.reac_nu[r * 3 + i];
+    if (nu < 0 && (long long)(-nu) * nc > xs) crit = true;
+  }
+  return crit;
+}
+
+// corrected criticality: a > 0 and L_j = min_{nu<0} floor(x/|nu|) < NC (Cao, Gillespie, Petzold 2005)
+template <typename Real, int MAXS>
+__device__ __forceinline__ bool crit_fix(const DevModel& m, const Counts<MAXS>& x, int r, Real a, int nc) {
+  if (!(a > (Real)0)) return false;
+  const int nn = m.n_net[r];
+  for (int i = 0; i < nn; ++i) {
+    const int nu = m.net_nu[r * 8 + i];
+    if (nu < 0 && x.get(m.net_s[r * 8 + i]) < (long long)(-nu) * nc) return true;
+  }
+  return false;
+}
+
+// Cao's g (tau.cu:47-66 for orders <= 2; orders 3 per Cao, Gillespie, Petzold 2006)
+template <typename Real>
+__device__ __forceinline__ Real gfun(int hor, int hmult, int32_t x) {
+  const Real xr = (Real)x;
+  switch (hor) {
+    case 0: return RT<Real>::inf();
+    case 1: return (Real)1;
+    case 2:
+      if (hmult == 1) return (Real)2;
+      return (Real)2 + (Real)1 / (xr - (Real)1);
+    default:
+      if (hmult == 1) return (Real)3;
+      if (hmult == 2) return (Real)1.5 * ((Real)2 + (Real)1 / (xr - (Real)1));
+      return ((Real)3 + (Real)1 / (xr - (Real)1)) + (Real)2 / (xr - (Real)2);
+  }
+}
+
+template <int MAXS>
+__device__ __forceinline__ void load_counts(const DevModel& m, const int32_t* X, uint32_t c, Counts<MAXS>& x) {
+#pragma unroll
+  for (int s = 0; s < MAXS; ++s) x.v[s] = (s < (int)m.S) ? X[(size_t)s * m.Npad + c] : 0;
+}
+
+// ------------------------------------------------------------------------------------------------
+// classification of one subvolume (compute_taus, tau.cu:197-252)
+// ------------------------------------------------------------------------------------------------
+template <typename Real, int MAXS>
+__device__ void classify_cell(const KArgs& A, uint32_t c, const Counts<MAXS>& x, const int32_t* Xe,
+                              double tau_cur, uint8_t flag_cur, uint64_t step, uint32_t attempt,
+                              double ff, double& tau_out, int& flag_out) {
+  const DevModel& m = A.m;
+  const int mode = A.o.mode;
+  const int nc = A.o.nc;
+  if (step > 0 && flag_cur == F_SSA_FF && !plis_isinf_d(tau_cur)) {
+    if (mode == 0) {
+      if (ff > 0.0 && ff != tau_cur) { tau_out = tau_cur - ff; flag_out = F_SSA_FF; return; }  // tau.cu:214-217
+    } else if (tau_cur > ff) {
+      tau_out = tau_cur - ff;
+      flag_out = F_SSA_FF;
+      return;
+    }
+  }
+  const int comp = comp_of(m, c);
+  uint32_t nb[6];
+  const int n = nbrs(m, c, nb);
+  const int S = (int)m.S, R = (int)m.R;
+  Real tau_ncr = RT<Real>::inf();
+  for (int s = 0; s < S; ++s) {
+    const int32_t xs = x.get(s);
+    bool include;
+    const int r0 = m.sr_off[s], r1 = m.sr_off[s + 1];
+    if (mode == 0) {
+      bool skip_r = false;
+      for (int i = r0; i < r1 && !skip_r; ++i) skip_r = crit_ref(m, x, m.sr_r[i], nc);
+      include = !(skip_r && xs < nc);  // tau.cu:165
+    } else {
+      include = false;
+      for (int i = r0; i < r1 && !include; ++i) {
+        const int r = m.sr_r[i];
+        const Real a = prop<Real>(m, x, r, comp);
+        include = (a > (Real)0) && !crit_fix(m, x, r, a, nc);
+      }
+      if (!include && xs >= nc && drate<Real>(m, comp, s) > (Real)0 && n > 0) include = true;
+    }
+    if (!include) continue;
+    // compute_tau_sp, tau.cu:68-143
+    const Real g = gfun<Real>(m.hor[s], m.hmult[s], xs);
+    Real mu = (Real)0, s2 = (Real)0;
+    const int p0 = m.sp_off[s], p1 = m.sp_off[s + 1];
+    for (int i = p0; i < p1; ++i) {
+      const int r = m.sp_r[i];
+      const int nu = m.sp_nu[i];
+      const Real a = prop<Real>(m, x, r, comp);
+      const bool ncrit = (mode == 0) ? !crit_ref(m, x, r, nc) : ((a > (Real)0) && !crit_fix(m, x, r, a, nc));
+      if (!ncrit) continue;
+      mu = mu + (Real)nu * a;
+      s2 = s2 + (Real)(nu * nu) * a;
+    }
+    const Real d = drate<Real>(m, comp, s) * (Real)xs;
+    if (mode == 0) {
+      if (xs >= nc) { mu = mu + d; s2 = s2 + d; }
+      for (int j = 0; j < n; ++j) {
+        const uint32_t b = nb[j];
+        const Real db = drate<Real>(m, comp_of(m, b), s) * (Real)Xe[(size_t)s * m.Npad + b];
+        const Real q = db / (Real)nbr_count(m, b);
+        mu = mu - q;
+        s2 = s2 + q;
+      }
+    } else {
+      if (xs >= nc && n > 0) {
+        const Real dout = (Real)n * d;
+        mu = mu - dout;
+        s2 = s2 + dout;
+      }
+      for (int j = 0; j < n; ++j) {
+        const uint32_t b = nb[j];
+        const int32_t xb = Xe[(size_t)s * m.Npad + b];
+        if (xb >= nc) {
+          const Real q = drate<Real>(m, comp_of(m, b), s) * (Real)xb;
+          mu = mu + q;
+          s2 = s2 + q;
+        }
+      }
+    }
+    Real mm = ((Real)A.o.eps * (Real)xs) / g;
+    if (!(mm > (Real)1)) mm = (Real)1;
+    const Real t1 = mm / fabs(mu);
+    const Real t2 = (mm * mm) / s2;
+    const Real ts = t1 < t2 ? t1 : t2;
+    if (ts < tau_ncr) tau_ncr = ts;
+  }
+  // critical (or, corrected SSA subvolume: total) rate, compute_tau_cr tau.cu:176-195
+  Real rsum = (Real)0, dsum = (Real)0;
+  const bool ncr_inf = plis_isinf_d((double)tau_ncr);
+  if (mode == 0 || !ncr_inf) {
+    for (int r = 0; r < R; ++r) {
+      const Real a = prop<Real>(m, x, r, comp);
+      const bool cr = (mode == 0) ? crit_ref(m, x, r, nc) : crit_fix(m, x, r, a, nc);
+      if (cr) rsum = rsum + a;
+    }
+    for (int s = 0; s < S; ++s) {
+      const int32_t xs = x.get(s);
+      if (xs < nc) {
+        const Real d = drate<Real>(m, comp, s) * (Real)xs;
+        dsum = dsum + (mode == 0 ? d : (Real)n * d);
+      }
+    }
+  } else {
+    for (int r = 0; r < R; ++r) rsum = rsum + prop<Real>(m, x, r, comp);
+    for (int s = 0; s < S; ++s) dsum = dsum + (Real)n * (drate<Real>(m, comp, s) * (Real)x.get(s));
+  }
+  double tcr;
+  if (rsum == (Real)0 && dsum == (Real)0) {
+    tcr = PLIS_INF_D;
+  } else {
+    plis_stream st = plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_TAU, step, attempt, 0);
+    tcr = plis_exponential_d(&st, (double)(rsum + dsum));
+  }
+  const double tn = (double)tau_ncr;
+  if (plis_isinf_d(tn)) {
+    flag_out = F_SSA_FF;
+    tau_out = tcr;
+  } else if (tn < tcr) {
+    flag_out = F_LEAP_NOCR;
+    tau_out = tn;
+  } else {
+    flag_out = F_LEAP_CR;
+    tau_out = tcr;
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// control (runs in one thread of the last CTA of k_classify, or in k_prepare)
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ void set_attempt(Ctrl* K, int mode) {
+  double scale = 1.0;
+  for (uint32_t i = 0; i < K->attempt; ++i) scale *= 0.5;
+  if (mode == 0) {  // the reference re-leaps with the un-halved tau but advances time by the halved one
+    K->tau_leap = K->tau_min;
+    K->dt = K->tau_min * scale;
+  } else {
+    K->tau_leap = K->tau_step * scale;
+    K->dt = K->tau_leap;
+  }
+  const uint32_t af = K->argmin_flag;
+  uint32_t ex = 0;
+  if (mode == 0) {
+    if (K->n_leap_cr > 0) ex |= 1u;
+    if (af == F_SSA || af == F_SSA_FF) ex |= 2u;
+  } else if (K->attempt == 0 && K->tau_step == K->tau_min &&
+             (af == F_LEAP_CR || af == F_SSA || af == F_SSA_FF)) {
+    ex |= 2u;
+  }
+  K->exact = ex;
+  K->ev_attempt = 0;
+  K->ex_attempt = 0;
+}
+
+__device__ __forceinline__ void prepare_step(Ctrl* K, int mode) {
+  if (K->done) return;
+  if (K->t >= K->t_end) { K->done = 1; K->stop_reason = PLIS_STOP_TIME; return; }
+  if (K->step >= K->max_step) { K->done = 1; K->stop_reason = PLIS_STOP_STEPS; return; }
+  if (K->argmin < 0 || plis_isinf_d(K->tau_min) || K->tau_min < 0.0) {  // driver.cu:269-272
+    if (mode == 1) { K->t = K->t_end; K->stop_reason = PLIS_STOP_TIME; }
+    else K->stop_reason = PLIS_STOP_NO_EVENT;
+    K->done = 1;
+    return;
+  }
+  K->tau_step = K->tau_min;
+  if (mode == 1 && K->t_end - K->t < K->tau_step) K->tau_step = K->t_end - K->t;
+  K->attempt = 0;
+  set_attempt(K, mode);
+}
+
+#ifdef PLIS_ENGINE_HOST_TU
+__global__ void k_prepare(KArgs A, double t_end, unsigned long long n_steps) {
+  Ctrl* K = A.b.ctrl;
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (K->status != PLIS_OK) { K->done = 1; K->stop_reason = PLIS_STOP_ERROR; return; }
+  K->t_end = t_end;
+  K->max_step = (n_steps == ~0ull) ? ~0ull : K->step + n_steps;
+  K->done = 0;
+  K->stop_reason = PLIS_STOP_NONE;
+  prepare_step(K, A.o.mode);
+}
+#endif
+
+// ------------------------------------------------------------------------------------------------
+// reductions
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ void min_pair(double& t, long long& i, double t2, long long i2) {
+  if (t2 < t || (t2 == t && i2 < i)) { t = t2; i = i2; }
+}
+__device__ __forceinline__ void warp_min_pair(double& t, long long& i) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double t2 = __shfl_xor_sync(0xffffffffu, t, o);
+    const long long i2 = __shfl_xor_sync(0xffffffffu, i, o);
+    min_pair(t, i, t2, i2);
+  }
+}
+__device__ __forceinline__ long long warp_sum(long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// ------------------------------------------------------------------------------------------------
+// k_leap (leap_step, leap.cu:3-65)
+// ------------------------------------------------------------------------------------------------
+template <typename Real, int MAXS>
+__global__ void __launch_bounds__(512) k_leap(KArgs A) {
+  Ctrl* K = A.b.ctrl;
+  if (K->done) return;
+  const DevModel& m = A.m;
+  const int mode = A.o.mode, nc = A.o.nc;
+  const int32_t* Xc = A.b.X[K->cur];
+  int32_t* Xt = A.b.X[K->tgt];
+  uint8_t* flag = A.b.flag[K->tf];
+  const uint64_t step = K->step + 1;
+  const uint32_t attempt = K->attempt;
+  const Real tl = (Real)K->tau_leap;
+  __shared__ long long s_ev[32];
+  __shared__ int s_big;
+  if (threadIdx.x == 0) s_big = 0;
+  __syncthreads();
+  uint32_t c = 0;
+  const bool valid = cell_of(A, c);
+  long long ev = 0;
+  int big = 0;
+  if (valid) {
+    Counts<MAXS> x;
+    load_counts(m, Xc, c, x);
+    Deltas<MAXS> dl;
+#pragma unroll
+    for (int s = 0; s < MAXS; ++s) dl.v[s] = 0;
+    const uint8_t f = flag[c];
+    if (f == F_LEAP_CR || f == F_LEAP_NOCR) {  // leap.cu:9-10
+      const int comp = comp_of(m, c);
+      const int S = (int)m.S, R = (int)m.R;
+      for (int r = 0; r < R; ++r) {
+        const Real a = prop<Real>(m, x, r, comp);
+        const bool fire = (mode == 0) ? !crit_ref(m, x, r, nc) : ((a > (Real)0) && !crit_fix(m, x, r, a, nc));
+        if (!fire) continue;
+        plis_stream st = plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_react(r));
+        const long long k = RT<Real>::count(RT<Real>::poisson(&st, tl * a));
+        ev += k;
+        const int nn = m.n_net[r];
+        for (int i = 0; i < nn; ++i) {
+          const long long v = k * (long long)m.net_nu[r * 8 + i];
+          if (v >= kBigDraw || v <= -kBigDraw) big = 1;
+          dl.add(m.net_s[r * 8 + i], v);
+        }
+      }
+      uint32_t nb[6];
+      const int n = nbrs(m, c, nb);
+      bool mark = false;
+      for (int s = 0; s < S; ++s) {
+        const int32_t xs = x.get(s);
+        if (xs < nc) continue;  // is_critical_diffusion, tau.cu:42-45
+        if (mode == 0 && n > 0) mark = true;
+        const Real lam = tl * (drate<Real>(m, comp, s) * (Real)xs);
+        long long out = 0;
+        for (int j = 0; j < n; ++j) {
+          plis_stream st = plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_diff(s, j));
+          const long long k = RT<Real>::count(RT<Real>::poisson(&st, lam));
+          if (k >= kBigJump) big = 1;
+          if (k > 0) {
+            atomicAdd(&Xt[(size_t)s * m.Npad + nb[j]], (int)k);
+            if (mode == 1 && flag[nb[j]] == F_SSA_FF) flag[nb[j]] = F_SSA;
+          }
+          out += k;
+        }
+        dl.add(s, -out);
+        ev += out;
+      }
+      if (mark) {  // leap.cu:54-56: every receiver leaves fast-forward
+        for (int j = 0; j < n; ++j)
+          if (flag[nb[j]] == F_SSA_FF) flag[nb[j]] = F_SSA;
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < MAXS; ++s) {
+      if (s < (int)m.S) {
+        const long long tv = (long long)x.v[s] + dl.v[s];
+        if (tv >= kBigTile || tv <= -kBigTile) big = 1;
+        atomicAdd(&Xt[(size_t)s * m.Npad + c], (int)tv);
+      }
+    }
+  }
+  // events and guard flags of the CTA
+  ev = warp_sum(ev);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (big) s_big = 1;
+  if (lane == 0) s_ev[wid] = ev;
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    long long v = lane < nw ? s_ev[lane] : 0;
+    v = warp_sum(v);
+    if (lane == 0) {
+      if (v) atomicAdd(&K->ev_attempt, (unsigned long long)v);
+      if (s_big) atomicOr(&K->blocks_done, 0x80000000u);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// exact events
+// ------------------------------------------------------------------------------------------------
+// Reference critical event of one LEAP_CR subvolume (leap.cu:86-199).
+template <typename Real, int MAXS>
+__device__ int critical_event_ref(const KArgs& A, uint32_t c, const Counts<MAXS>& x, const int32_t* Xt,
+                                  uint64_t step, uint32_t attempt, int32_t* D, uint8_t* flag) {
+  const DevModel& m = A.m;
+  const int nc = A.o.nc;
+  const int S = (int)m.S, R = (int)m.R;
+  const int comp = comp_of(m, c);
+  plis_stream su = plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_CRIT, step, attempt, 0);
+  const Real u = RT<Real>::uniform(&su);
+  Real rsum = (Real)0, dsum = (Real)0;
+  for (int r = 0; r < R; ++r)
+    if (crit_ref(m, x, r, nc)) rsum = rsum + prop<Real>(m, x, r, comp);
+  for (int s = 0; s < S; ++s)
+    if (x.get(s) < nc) dsum = dsum + drate<Real>(m, comp, s) * (Real)x.get(s);
+  if (rsum + dsum == (Real)0) return 0;
+  if (u < rsum / (rsum + dsum)) {
+    const Real scaled = rsum * u;
+    Real partial = (Real)0;
+    int ric = 0;
+    while (partial <= scaled && ric < R) {
+      if (crit_ref(m, x, ric, nc)) partial = partial + prop<Real>(m, x, ric, comp);
+      ++ric;
+    }
+    int ri = 0;
+    for (ri = 0; ri < R && ric > 0; ++ri)
+      if (crit_ref(m, x, ri, nc)) --ric;
+    ri = ri - 1;  // leap.cu:121-126 as written
+    if (ri < 0) ri = 0;
+    bool fire = true;
+    for (int s = 0; s < S; ++s) {
+      int need = 0;
+      for (int i = 0; i < m.n_reac[ri]; ++i)
+        if (m.reac_s[ri * 3 + i] == s) need = m.reac_m[ri * 3 + i];
+      fire = fire && x.get(s) >= need && Xt[(size_t)s * m.Npad + c] >= need;
+    }
+    if (!fire) return 0;
+    for (int i = 0; i < m.n_net[ri]; ++i)
+      atomicAdd(&D[(size_t)m.net_s[ri * 8 + i] * m.Npad + c], (int)m.net_nu[ri * 8 + i]);
+    return 1;
+  }
+  const Real scaled = dsum * u;
+  Real partial = (Real)0;
+  int spic = 0;
+  while (partial <= scaled && spic < S) {
+    if (x.get(spic) < nc) partial = partial + drate<Real>(m, comp, spic) * (Real)x.get(spic);
+    ++spic;
+  }
+  int spi = 0;
+  for (spi = 0; spi < S && spic > 0; ++spi)
+    if (x.get(spi) < nc) --spic;
+  spi = spi - 1;  // leap.cu:160-166
+  if (spi < 0) spi = 0;
+  const bool fire = x.get(spi) > 0 && Xt[(size_t)spi * m.Npad + c] > 0;
+  if (!fire) return 0;
+  plis_stream sd = plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_CRIT, step, attempt, 1);
+  const Real u2 = RT<Real>::uniform(&sd);
+  int slot = (int)(u2 * (Real)6);
+  if (slot > 5) slot = 5;
+  const uint32_t target = canon_slot(m, c, slot);
+  if (target == c) return 0;
+  atomicAdd(&D[(size_t)spi * m.Npad + c], -1);
+  atomicAdd(&D[(size_t)spi * m.Npad + target], 1);
+  const uint32_t q = flat_table_entry(m, target);  // leap.cu:192-193
+  if (flag[q] == F_SSA_FF) flag[q] = F_SSA;
+  return 1;
+}
+
+// Exact event of the arg-min subvolume: reference ssa_step (ssa.cu:270-324), or in corrected mode
+// an SSA over the critical channels (LEAP_CR) or over every channel (SSA subvolumes).
+template <typename Real, int MAXS>
+__device__ int argmin_event(const KArgs& A, uint32_t mcell, const Counts<MAXS>& x, uint64_t step, uint32_t attempt,
+                            int32_t* dst, uint8_t* flag, bool critical_only) {
+  const DevModel& m = A.m;
+  const int mode = A.o.mode, nc = A.o.nc;
+  const int S = (int)m.S, R = (int)m.R;
+  const int comp = comp_of(m, mcell);
+  uint32_t nb[6];
+  const int n = nbrs(m, mcell, nb);
+  plis_stream su = plis_stream_make(A.o.seed, A.o.replica, mcell, PLIS_PHASE_SSA, step, attempt, 0);
+  const Real u = RT<Real>::uniform(&su);
+  if (mode == 0) {
+    Real rsum = (Real)0, dsum = (Real)0;
+    for (int r = 0; r < R; ++r) rsum = rsum + prop<Real>(m, x, r, comp);
+    for (int s = 0; s < S; ++s) dsum = dsum + drate<Real>(m, comp, s) * (Real)x.get(s);
+    const Real dtot = dsum * (Real)n;  // rates.cu:165-172
+    const Real total = rsum + dtot;
+    if (!(total > (Real)0)) return 0;
+    if (u < rsum / total) {
+      const Real scaled = rsum * u;
+      Real partial = (Real)0;
+      int ri = 0;
+      while (partial <= scaled && ri < R) { partial = partial + prop<Real>(m, x, ri, comp); ++ri; }
+      ri = ri - 1;
+      if (ri < 0) ri = 0;
+      for (int i = 0; i < m.n_net[ri]; ++i)
+        atomicAdd(&dst[(size_t)m.net_s[ri * 8 + i] * m.Npad + mcell], (int)m.net_nu[ri * 8 + i]);
+      flag[mcell] = F_SSA;  // ssa.cu:295
+      return 1;
+    }
+    if (!(dtot > (Real)0)) return 0;
+    const Real scaled = (dtot / (Real)n) * u;  // ssa.cu:256-266
+    Real partial = (Real)0;
+    int spi = 0;
+    while (partial <= scaled && spi < S) {
+      partial = partial + drate<Real>(m, comp, spi) * (Real)x.get(spi);
+      ++spi;
+    }
+    spi = spi - 1;
+    if (spi < 0) spi = 0;
+    plis_stream sd = plis_stream_make(A.o.seed, A.o.replica, mcell, PLIS_PHASE_SSA, step, attempt, 1);
+    const Real u2 = RT<Real>::uniform(&sd);
+    int slot = (int)(u2 * (Real)6);
+    if (slot > 5) slot = 5;
+    const uint32_t target = canon_slot(m, mcell, slot);
+    if (target == mcell) return 0;
+    atomicAdd(&dst[(size_t)spi * m.Npad + mcell], -1);
+    atomicAdd(&dst[(size_t)spi * m.Npad + target], 1);
+    if (flag[target] == F_SSA_FF) flag[target] = F_SSA;
+    return 1;
+  }
+  Real total = (Real)0;
+  for (int r = 0; r < R; ++r) {
+    const Real a = prop<Real>(m, x, r, comp);
+    if (!critical_only || crit_fix(m, x, r, a, nc)) total = total + a;
+  }
+  for (int s = 0; s < S; ++s)
+    if (!critical_only || x.get(s) < nc) total = total + (Real)n * (drate<Real>(m, comp, s) * (Real)x.get(s));
+  if (!(total > (Real)0)) return 0;
+  const Real scaled = total * u;
+  Real partial = (Real)0;
+  int chosen_r = -1, chosen_s = -1, last_r = -1, last_s = -1;
+  for (int r = 0; r < R && chosen_r < 0; ++r) {
+    const Real a = prop<Real>(m, x, r, comp);
+    const bool use = critical_only ? crit_fix(m, x, r, a, nc) : true;
+    if (!use || !(a > (Real)0)) continue;
+    partial = partial + a;
+    last_r = r;
+    if (partial > scaled) chosen_r = r;
+  }
+  if (chosen_r < 0) {
+    for (int s = 0; s < S && chosen_s < 0; ++s) {
+      const bool use = critical_only ? (x.get(s) < nc) : true;
+      const Real w = (Real)n * (drate<Real>(m, comp, s) * (Real)x.get(s));
+      if (!use || !(w > (Real)0)) continue;
+      partial = partial + w;
+      last_s = s;
+      if (partial > scaled) chosen_s = s;
+    }
+  }
+  if (chosen_r < 0 && chosen_s < 0) {
+    if (last_s >= 0) chosen_s = last_s;
+    else chosen_r = last_r;
+  }
+  if (chosen_r >= 0) {
+    for (int i = 0; i < m.n_net[chosen_r]; ++i)
+      atomicAdd(&dst[(size_t)m.net_s[chosen_r * 8 + i] * m.Npad + mcell], (int)m.net_nu[chosen_r * 8 + i]);
+    return 1;
+  }
+  plis_stream sd = plis_stream_make(A.o.seed, A.o.replica, mcell, PLIS_PHASE_SSA, step, attempt, 1);
+  const Real u2 = RT<Real>::uniform(&sd);
+  int slot = (int)(u2 * (Real)n);
+  if (slot > n - 1) slot = n - 1;
+  const uint32_t target = nb[slot];
+  atomicAdd(&dst[(size_t)chosen_s * m.Npad + mcell], -1);
+  atomicAdd(&dst[(size_t)chosen_s * m.Npad + target], 1);
+  if (flag[target] == F_SSA_FF) flag[target] = F_SSA;
+  return 1;
+}
+
+template <typename Real, int MAXS>
+__global__ void __launch_bounds__(256) k_exact(KArgs A) {
+  Ctrl* K = A.b.ctrl;
+  if (K->done) return;
+  const uint32_t ex = K->exact;
+  if (ex == 0) return;
+  const DevModel& m = A.m;
+  const int32_t* Xc = A.b.X[K->cur];
+  int32_t* Xt = A.b.X[K->tgt];
+  uint8_t* flag = A.b.flag[K->tf];
+  const uint64_t step = K->step + 1;
+  const uint32_t attempt = K->attempt;
+  int fired = 0;
+  if (ex & 1u) {  // reference: every LEAP_CR subvolume
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < m.N && flag[c] == F_LEAP_CR) {
+      Counts<MAXS> x;
+      load_counts(m, Xc, c, x);
+      fired += critical_event_ref<Real>(A, c, x, Xt, step, attempt, A.b.D, flag);
+    }
+  }
+  if ((ex & 2u) && blockIdx.x == 0 && threadIdx.x == 0) {
+    const uint32_t am = (uint32_t)K->argmin;
+    const uint8_t fa = flag[am];
+    Counts<MAXS> x;
+    load_counts(m, Xc, am, x);
+    int32_t* dst = (ex & 1u) ? A.b.D : Xt;
+    if (A.o.mode == 0) {
+      if (fa == F_SSA || fa == F_SSA_FF) fired += argmin_event<Real>(A, am, x, step, attempt, dst, flag, false);
+    } else {
+      if (fa == F_LEAP_CR) fired += argmin_event<Real>(A, am, x, step, attempt, dst, flag, true);
+      else if (fa == F_SSA || fa == F_SSA_FF) fired += argmin_event<Real>(A, am, x, step, attempt, dst, flag, false);
+    }
+  }
+  if (fired) {  // exact events are rare: one atomic per firing thread
+    atomicAdd(&K->ev_attempt, (unsigned long long)fired);
+    atomicAdd(&K->ex_attempt, (unsigned long long)fired);
+  }
+}
+
+#ifdef PLIS_ENGINE_HOST_TU
+__global__ void __launch_bounds__(256) k_apply(KArgs A) {
+  Ctrl* K = A.b.ctrl;
+  if (K->done || !(K->exact & 1u)) return;
+  const DevModel& m = A.m;
+  int32_t* Xt = A.b.X[K->tgt];
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.N) return;
+  for (uint32_t s = 0; s < m.S; ++s) {
+    const size_t i = (size_t)s * m.Npad + c;
+    const int32_t v = A.b.D[i];
+    if (v) {
+      Xt[i] += v;
+      A.b.D[i] = 0;
+    }
+  }
+}
+#endif
+
+// ------------------------------------------------------------------------------------------------
+// k_classify + last-CTA control
+// ------------------------------------------------------------------------------------------------
+template <typename Real, int MAXS>
+__global__ void __launch_bounds__(512) k_classify(KArgs A) {
+  Ctrl* K = A.b.ctrl;
+  if (K->done) return;
+  const DevModel& m = A.m;
+  const uint32_t phase = K->phase;
+  const int32_t* Xe = A.b.X[phase == 0 ? K->cur : K->tgt];
+  int32_t* Xz = A.b.X[K->spare];
+  const uint32_t tf = K->tf;
+  const double* tau_cur = A.b.tau[tf];
+  double* tau_new = A.b.tau[tf ^ 1u];
+  const uint8_t* flag_cur = A.b.flag[tf];
+  uint8_t* flag_new = A.b.flag[tf ^ 1u];
+  const uint64_t step = phase == 0 ? 0 : K->step + 1;
+  const uint32_t attempt = phase == 0 ? 0 : K->attempt;
+  const double ff = K->dt;
+
+  __shared__ double s_t[32];
+  __shared__ long long s_i[32];
+  __shared__ bool s_last;
+
+  uint32_t c = 0;
+  const bool valid = cell_of(A, c);
+  double tn = PLIS_INF_D;
+  long long ti = 0x7FFFFFFFFFFFFFFFll;
+  int fl = F_SSA_FF;
+  int bad = 0;
+  if (valid) {
+    Counts<MAXS> x;
+    load_counts(m, Xe, c, x);
+#pragma unroll
+    for (int s = 0; s < MAXS; ++s)
+      if (s < (int)m.S) {
+        if (x.v[s] < 0) bad = 1;
+        Xz[(size_t)s * m.Npad + c] = 0;
+      }
+    classify_cell<Real>(A, c, x, Xe, tau_cur[c], flag_cur[c], step, attempt, ff, tn, fl);
+    tau_new[c] = tn;
+    flag_new[c] = (uint8_t)fl;
+    ti = c;
+  }
+  const int ncr = __syncthreads_count(valid && fl == F_LEAP_CR);
+  const int nbad = __syncthreads_or(bad);
+  warp_min_pair(tn, ti);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) { s_t[wid] = tn; s_i[wid] = ti; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    double bt = s_t[0];
+    long long bi = s_i[0];
+    for (int w = 1; w < nw; ++w) min_pair(bt, bi, s_t[w], s_i[w]);
+    A.b.slot_tau[blockIdx.x] = bt;
+    A.b.slot_idx[blockIdx.x] = bi;
+    A.b.slot_cr[blockIdx.x] = (uint32_t)ncr;
+    A.b.slot_bad[blockIdx.x] = nbad ? 1u : 0u;
+    __threadfence();
+    const uint32_t prev = atomicAdd(&K->blocks_done, 1u);
+    s_last = ((prev & 0x7FFFFFFFu) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_last || wid != 0) return;
+
+  // ---- last CTA: grid-wide arg-min and the step decision ----
+  __threadfence();
+  double gt = PLIS_INF_D;
+  long long gi = 0x7FFFFFFFFFFFFFFFll;
+  unsigned long long gcr = 0;
+  uint32_t gbad = 0;
+  for (uint32_t b = lane; b < gridDim.x; b += 32) {
+    min_pair(gt, gi, __ldcg(&A.b.slot_tau[b]), __ldcg(&A.b.slot_idx[b]));
+    gcr += __ldcg(&A.b.slot_cr[b]);
+    gbad |= __ldcg(&A.b.slot_bad[b]);
+  }
+  warp_min_pair(gt, gi);
+  gcr = (unsigned long long)warp_sum((long long)gcr);
+  gbad = __reduce_or_sync(0xffffffffu, gbad);
+  if (lane != 0) return;
+  const int mode = A.o.mode;
+  const uint32_t leap_bad = (__ldcg(&K->blocks_done) & 0x80000000u) ? 1u : 0u;
+  K->blocks_done = 0;
+  if (gi == 0x7FFFFFFFFFFFFFFFll) gi = -1;
+  if (phase == 0) {
+    K->tau_min = gt;
+    K->argmin = gi;
+    K->n_leap_cr = (uint32_t)gcr;
+    K->argmin_flag = gi >= 0 ? __ldcg(&flag_new[gi]) : F_SSA_FF;
+    K->tf = tf ^ 1u;
+    K->phase = 1;
+    K->done = 1;  // idle until a run call
+    return;
+  }
+  if (gbad || leap_bad) {  // check_state + revert (leap.cu:203-212, driver.cu:292-315)
+    K->attempt += 1;
+    if ((int)K->attempt > A.o.max_rollbacks) {
+      K->status = PLIS_ERR_STUCK;
+      K->stop_reason = PLIS_STOP_ERROR;
+      K->done = 1;
+      return;
+    }
+    const uint32_t t = K->tgt;
+    K->tgt = K->spare;
+    K->spare = t;
+    set_attempt(K, mode);
+    return;
+  }
+  // accept: swap state (driver.cu:320-323) by rotating buffer indices
+  K->t = K->t + K->dt;
+  K->step = K->step + 1;
+  K->events += K->ev_attempt;
+  K->exact_events += K->ex_attempt;
+  K->rollbacks += K->attempt;
+  K->last_tau = K->tau_min;
+  K->last_argmin = K->argmin;
+  const uint32_t oc = K->cur;
+  K->cur = K->tgt;
+  K->tgt = K->spare;
+  K->spare = oc;
+  K->tf = tf ^ 1u;
+  K->tau_min = gt;
+  K->argmin = gi;
+  K->n_leap_cr = (uint32_t)gcr;
+  K->argmin_flag = gi >= 0 ? __ldcg(&flag_new[gi]) : F_SSA_FF;
+  prepare_step(K, mode);
+}
+
+#ifdef PLIS_ENGINE_HOST_TU
+__global__ void k_fill_tau(double* t, uint8_t* f, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) { t[i] = PLIS_INF_D; f[i] = F_SSA_FF; }
+}
+#endif
+
+// kernel launchers of each (precision, species capacity)
+template <typename Real, int MAXS>
+struct KernelSet {
+  static void leap(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) { k_leap<Real, MAXS><<<g, b, 0, s>>>(a); }
+  static void exact(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) { k_exact<Real, MAXS><<<g, b, 0, s>>>(a); }
+  static void classify(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) { k_classify<Real, MAXS><<<g, b, 0, s>>>(a); }
+};
+
+template <typename Real>
+Launchers pick_impl(uint32_t S) {
+  if (S <= 1) return {KernelSet<Real, 1>::leap, KernelSet<Real, 1>::exact, KernelSet<Real, 1>::classify};
+  if (S <= 2) return {KernelSet<Real, 2>::leap, KernelSet<Real, 2>::exact, KernelSet<Real, 2>::classify};
+  if (S <= 4) return {KernelSet<Real, 4>::leap, KernelSet<Real, 4>::exact, KernelSet<Real, 4>::classify};
+  if (S <= 8) return {KernelSet<Real, 8>::leap, KernelSet<Real, 8>::exact, KernelSet<Real, 8>::classify};
+  if (S <= 16) return {KernelSet<Real, 16>::leap, KernelSet<Real, 16>::exact, KernelSet<Real, 16>::classify};
+  if (S <= 32) return {KernelSet<Real, 32>::leap, KernelSet<Real, 32>::exact, KernelSet<Real, 32>::classify};
+  if (S <= 64) return {KernelSet<Real, 64>::leap, KernelSet<Real, 64>::exact, KernelSet<Real, 64>::classify};
+  return {KernelSet<Real, 256>::leap, KernelSet<Real, 256>::exact, KernelSet<Real, 256>::classify};
+}
+
+
+Launchers pick_f64(uint32_t S);
+Launchers pick_f32(uint32_t S);
+
+}  // namespace plis
+
+#endif

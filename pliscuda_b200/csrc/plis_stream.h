@@ -1,0 +1,468 @@
+// plis_stream.h — the random stream and the scalar numerics of the tau-leaping step.
+//
+// This header is compiled unchanged by nvcc (device code of the CUDA step) and by g++ (the FP64/FP32
+// host oracle under oracle/, which is test infrastructure).  Everything here is plain IEEE-754
+// arithmetic (+ - * / sqrt floor fma), integer operations and bit manipulation, so both compilers
+// produce the same bits provided no floating-point contraction is added behind our back:
+// nvcc gets -fmad=false, g++ gets -ffp-contract=off.  Explicit fma() calls are used where wanted
+// (they are correctly rounded on both sides).
+//
+// What lives here and why:
+//  * Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3", SC'11):
+//    a counter-based generator.  The reference keeps one stateful cuRAND MRG32k3a state per
+//    subvolume (PLISCuda/src/init.cu:3-13, 192 bytes each, read-modify-written on every draw);
+//    here a draw is a pure function of (seed, replica, subvolume, step, attempt, channel, sub),
+//    so no generator state lives in memory and a step can be replayed bit-exactly.
+//  * exp / log written from the mathematics: Cody-Waite range reduction by ln 2 followed by the
+//    Taylor series of e^r (|r| <= ln2/2), and the atanh series ln m = 2 atanh((m-1)/(m+1)) for
+//    m in [sqrt(1/2), sqrt(2)).  The split of ln 2 into a 32-bit head and a tail was derived with
+//    mpmath; the series coefficients are 1/n! and 1/(2k+1) rounded to nearest.
+//  * ln k! : exact table for k <= 16 (mpmath, rounded to nearest), Stirling's series above.
+//  * Poisson variates: inversion by sequential search for lambda < 10, and PTRS
+//    (W. Hormann, "The transformed rejection method for generating Poisson random variables",
+//    Insurance: Mathematics and Economics 12 (1993) 39-45) for lambda >= 10.
+//    The reference calls curand_poisson (PLISCuda/src/leap.cu:27, :51).
+//  * Exponential variates -ln(U)/a (the reference: -logf(curand_uniform)/a, PLISCuda/src/tau.cu:193-194).
+#ifndef PLIS_STREAM_H_
+#define PLIS_STREAM_H_
+
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define PLIS_HD __host__ __device__ __forceinline__
+#define PLIS_FMA(a, b, c) fma((a), (b), (c))
+#define PLIS_FMAF(a, b, c) fmaf((a), (b), (c))
+#define PLIS_FLOOR(x) floor(x)
+#define PLIS_FLOORF(x) floorf(x)
+#define PLIS_SQRT(x) sqrt(x)
+#define PLIS_SQRTF(x) sqrtf(x)
+#define PLIS_FABS(x) fabs(x)
+#define PLIS_FABSF(x) fabsf(x)
+#else
+#include <math.h>
+#include <string.h>
+#define PLIS_HD static inline
+#define PLIS_FMA(a, b, c) fma((a), (b), (c))
+#define PLIS_FMAF(a, b, c) fmaf((a), (b), (c))
+#define PLIS_FLOOR(x) floor(x)
+#define PLIS_FLOORF(x) floorf(x)
+#define PLIS_SQRT(x) sqrt(x)
+#define PLIS_SQRTF(x) sqrtf(x)
+#define PLIS_FABS(x) fabs(x)
+#define PLIS_FABSF(x) fabsf(x)
+#endif
+
+// ------------------------------------------------------------------------------------------------
+// bit casts
+// ------------------------------------------------------------------------------------------------
+PLIS_HD uint64_t plis_d2u(double x) {
+#if defined(__CUDA_ARCH__)
+  return (uint64_t)__double_as_longlong(x);
+#else
+  uint64_t u; memcpy(&u, &x, 8); return u;
+#endif
+}
+PLIS_HD double plis_u2d(uint64_t u) {
+#if defined(__CUDA_ARCH__)
+  return __longlong_as_double((long long)u);
+#else
+  double x; memcpy(&x, &u, 8); return x;
+#endif
+}
+PLIS_HD uint32_t plis_f2u(float x) {
+#if defined(__CUDA_ARCH__)
+  return (uint32_t)__float_as_uint(x);
+#else
+  uint32_t u; memcpy(&u, &x, 4); return u;
+#endif
+}
+PLIS_HD float plis_u2f(uint32_t u) {
+#if defined(__CUDA_ARCH__)
+  return __uint_as_float(u);
+#else
+  float x; memcpy(&x, &u, 4); return x;
+#endif
+}
+
+#define PLIS_INF_D (plis_u2d(0x7FF0000000000000ull))
+#define PLIS_NAN_D (plis_u2d(0x7FF8000000000000ull))
+#define PLIS_INF_F (plis_u2f(0x7F800000u))
+#define PLIS_NAN_F (plis_u2f(0x7FC00000u))
+
+PLIS_HD int plis_isinf_d(double x) { return (plis_d2u(x) & 0x7FFFFFFFFFFFFFFFull) == 0x7FF0000000000000ull; }
+PLIS_HD int plis_isinf_f(float x) { return (plis_f2u(x) & 0x7FFFFFFFu) == 0x7F800000u; }
+
+// ------------------------------------------------------------------------------------------------
+// Philox4x32-10
+// ------------------------------------------------------------------------------------------------
+#define PLIS_PHILOX_M0 0xD2511F53u
+#define PLIS_PHILOX_M1 0xCD9E8D57u
+#define PLIS_PHILOX_W0 0x9E3779B9u
+#define PLIS_PHILOX_W1 0xBB67AE85u
+
+typedef struct plis_u32x4 { uint32_t x, y, z, w; } plis_u32x4;
+
+PLIS_HD plis_u32x4 plis_philox4x32_10(plis_u32x4 c, uint32_t k0, uint32_t k1) {
+#if defined(__CUDA_ARCH__)
+#pragma unroll
+#endif
+  for (int i = 0; i < 10; ++i) {
+    uint64_t p0 = (uint64_t)PLIS_PHILOX_M0 * (uint64_t)c.x;
+    uint64_t p1 = (uint64_t)PLIS_PHILOX_M1 * (uint64_t)c.z;
+    uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+    uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+    plis_u32x4 n;
+    n.x = hi1 ^ c.y ^ k0;
+    n.y = lo1;
+    n.z = hi0 ^ c.w ^ k1;
+    n.w = lo0;
+    c = n;
+    k0 += PLIS_PHILOX_W0;
+    k1 += PLIS_PHILOX_W1;
+  }
+  return c;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Counter layout.  One "channel" of one subvolume in one phase of one attempt of one step owns the
+// sub-stream (c.y low 12 bits = sub, incremented per Philox block):
+//   c.x = subvolume index (within its replica)
+//   c.y = channel << 12 | sub          (channel < 2^20)
+//   c.z = step (low 32 bits)
+//   c.w = phase << 28 | (attempt & 0xFFF) << 16 | (step >> 32) & 0xFFFF
+//   key = (seed low 32, seed high 32 xor replica * 0x632BE5AB)
+// ------------------------------------------------------------------------------------------------
+enum {
+  PLIS_PHASE_TAU = 1,    // exponential next-event times drawn while classifying
+  PLIS_PHASE_LEAP = 2,   // Poisson firings of non-critical reactions and diffusions
+  PLIS_PHASE_CRIT = 3,   // the single critical event of a LEAP_CR subvolume
+  PLIS_PHASE_SSA = 4,    // the exact event of the arg-min subvolume
+  PLIS_PHASE_INIT = 5    // synthetic initial states (generators)
+};
+
+#define PLIS_CH_DIFF_BASE 0x40000u  // diffusion channels: base + species * 8 + slot
+PLIS_HD uint32_t plis_ch_react(uint32_t r) { return r; }
+PLIS_HD uint32_t plis_ch_diff(uint32_t s, uint32_t slot) { return PLIS_CH_DIFF_BASE + s * 8u + slot; }
+
+typedef struct plis_stream {
+  plis_u32x4 ctr;
+  uint32_t k0, k1;
+  plis_u32x4 buf;
+  int avail;  // 32-bit words left in buf
+} plis_stream;
+
+PLIS_HD plis_stream plis_stream_make(uint64_t seed, uint32_t replica, uint32_t cell, uint32_t phase,
+                                     uint64_t step, uint32_t attempt, uint32_t channel) {
+  plis_stream s;
+  s.ctr.x = cell;
+  s.ctr.y = (channel & 0xFFFFFu) << 12;
+  s.ctr.z = (uint32_t)step;
+  s.ctr.w = ((phase & 0xFu) << 28) | ((attempt & 0xFFFu) << 16) | (uint32_t)((step >> 32) & 0xFFFFu);
+  s.k0 = (uint32_t)seed;
+  s.k1 = (uint32_t)(seed >> 32) ^ (replica * 0x632BE5ABu);
+  s.buf.x = s.buf.y = s.buf.z = s.buf.w = 0u;
+  s.avail = 0;
+  return s;
+}
+
+PLIS_HD void plis_stream_refill(plis_stream* s) {
+  s->buf = plis_philox4x32_10(s->ctr, s->k0, s->k1);
+  s->ctr.y = (s->ctr.y & 0xFFFFF000u) | ((s->ctr.y + 1u) & 0xFFFu);
+  s->avail = 4;
+}
+
+PLIS_HD uint32_t plis_stream_u32(plis_stream* s) {
+  if (s->avail == 0) plis_stream_refill(s);
+  uint32_t r;
+  switch (s->avail) {
+    case 4: r = s->buf.x; break;
+    case 3: r = s->buf.y; break;
+    case 2: r = s->buf.z; break;
+    default: r = s->buf.w; break;
+  }
+  s->avail -= 1;
+  return r;
+}
+
+// Uniform double strictly inside (0,1): 52 random bits, (x + 1/2) * 2^-52.  Exact in binary64.
+PLIS_HD double plis_uniform_d(plis_stream* s) {
+  uint32_t hi = plis_stream_u32(s);
+  uint32_t lo = plis_stream_u32(s);
+  uint64_t x = (((uint64_t)hi << 32) | (uint64_t)lo) >> 12;
+  return ((double)x + 0.5) * 2.220446049250313e-16;  // 2^-52
+}
+
+// Uniform float strictly inside (0,1): 23 random bits, (x + 1/2) * 2^-23.  Exact in binary32.
+PLIS_HD float plis_uniform_f(plis_stream* s) {
+  uint32_t x = plis_stream_u32(s) >> 9;
+  return ((float)x + 0.5f) * 1.1920928955078125e-07f;  // 2^-23
+}
+
+// ------------------------------------------------------------------------------------------------
+// exp / log, binary64
+// ------------------------------------------------------------------------------------------------
+#define PLIS_LN2_HI 0.6931471803691238      // ln 2 rounded to 32 significant bits
+#define PLIS_LN2_LO 1.9082149292705877e-10  // ln 2 - PLIS_LN2_HI
+#define PLIS_INV_LN2 1.4426950408889634
+#define PLIS_SQRT2 1.4142135623730951
+#define PLIS_HALF_LN_2PI 0.9189385332046728
+
+// 2^k for -1022 <= k <= 1023, by construction of the exponent field (exact).
+PLIS_HD double plis_pow2i(int k) { return plis_u2d((uint64_t)(k + 1023) << 52); }
+
+PLIS_HD double plis_exp(double x) {
+  if (x != x) return x;
+  if (x < -745.2) return 0.0;
+  if (x > 709.78) return PLIS_INF_D;
+  double kd = PLIS_FLOOR(x * PLIS_INV_LN2 + 0.5);
+  int k = (int)kd;
+  double r = (x - kd * PLIS_LN2_HI) - kd * PLIS_LN2_LO;
+  // Taylor series of e^r through r^13 (|r| <= 0.3466: truncation < 5e-18)
+  double p = 1.6059043836821613e-10;
+  p = PLIS_FMA(p, r, 2.08767569878681e-09);
+  p = PLIS_FMA(p, r, 2.505210838544172e-08);
+  p = PLIS_FMA(p, r, 2.755731922398589e-07);
+  p = PLIS_FMA(p, r, 2.7557319223985893e-06);
+  p = PLIS_FMA(p, r, 2.48015873015873e-05);
+  p = PLIS_FMA(p, r, 0.0001984126984126984);
+  p = PLIS_FMA(p, r, 0.001388888888888889);
+  p = PLIS_FMA(p, r, 0.008333333333333333);
+  p = PLIS_FMA(p, r, 0.041666666666666664);
+  p = PLIS_FMA(p, r, 0.16666666666666666);
+  p = PLIS_FMA(p, r, 0.5);
+  p = PLIS_FMA(p, r, 1.0);
+  p = PLIS_FMA(p, r, 1.0);
+  if (k >= -1022) {
+    if (k > 1023) return (p * plis_pow2i(1023)) * 2.0;
+    return p * plis_pow2i(k);
+  }
+  return (p * plis_pow2i(k + 60)) * 8.673617379884035e-19;  // 2^-60; rounds once into the subnormals
+}
+
+PLIS_HD double plis_log(double x) {
+  if (!(x > 0.0)) return (x == 0.0) ? -PLIS_INF_D : PLIS_NAN_D;
+  if (plis_isinf_d(x)) return x;
+  uint64_t b = plis_d2u(x);
+  int e = (int)((b >> 52) & 0x7FF);
+  if (e == 0) {  // subnormal: scale by 2^54 exactly
+    x = x * 18014398509481984.0;
+    b = plis_d2u(x);
+    e = (int)((b >> 52) & 0x7FF) - 54;
+  }
+  e -= 1023;
+  double m = plis_u2d((b & 0x000FFFFFFFFFFFFFull) | 0x3FF0000000000000ull);  // [1, 2)
+  if (m > PLIS_SQRT2) { m = m * 0.5; e += 1; }
+  double s = (m - 1.0) / (m + 1.0);
+  double s2 = s * s;
+  // atanh series: ln m = 2 (s + s^3/3 + ... + s^21/21); |s| <= 0.1716
+  double q = 0.047619047619047616;
+  q = PLIS_FMA(q, s2, 0.05263157894736842);
+  q = PLIS_FMA(q, s2, 0.058823529411764705);
+  q = PLIS_FMA(q, s2, 0.06666666666666667);
+  q = PLIS_FMA(q, s2, 0.07692307692307693);
+  q = PLIS_FMA(q, s2, 0.09090909090909091);
+  q = PLIS_FMA(q, s2, 0.1111111111111111);
+  q = PLIS_FMA(q, s2, 0.14285714285714285);
+  q = PLIS_FMA(q, s2, 0.2);
+  q = PLIS_FMA(q, s2, 0.3333333333333333);
+  double lm = 2.0 * PLIS_FMA(s * s2, q, s);
+  double ed = (double)e;
+  return ed * PLIS_LN2_HI + (ed * PLIS_LN2_LO + lm);
+}
+
+// ln k!  (k >= 0)
+PLIS_HD double plis_lnfact(double k) {
+  if (k <= 16.0) {
+    int i = (int)k;
+    switch (i) {
+      case 0: case 1: return 0.0;
+      case 2: return 0.6931471805599453;
+      case 3: return 1.791759469228055;
+      case 4: return 3.1780538303479458;
+      case 5: return 4.787491742782046;
+      case 6: return 6.579251212010101;
+      case 7: return 8.525161361065415;
+      case 8: return 10.60460290274525;
+      case 9: return 12.801827480081469;
+      case 10: return 15.104412573075516;
+      case 11: return 17.502307845873887;
+      case 12: return 19.987214495661885;
+      case 13: return 22.552163853123425;
+      case 14: return 25.19122118273868;
+      case 15: return 27.89927138384089;
+      default: return 30.671860106080672;
+    }
+  }
+  // Stirling: ln Gamma(z) = (z - 1/2) ln z - z + ln(2 pi)/2 + 1/(12z) - 1/(360z^3) + 1/(1260z^5)
+  //                         - 1/(1680z^7) + 1/(1188z^9),  z = k + 1 >= 18
+  double z = k + 1.0;
+  double w = 1.0 / z;
+  double w2 = w * w;
+  double c = 0.0008417508417508417;
+  c = 0.0005952380952380953 - w2 * c;
+  c = 0.0007936507936507937 - w2 * c;
+  c = 0.002777777777777778 - w2 * c;
+  c = 0.08333333333333333 - w2 * c;
+  return ((z - 0.5) * plis_log(z) - z) + (PLIS_HALF_LN_2PI + w * c);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Poisson, binary64
+// ------------------------------------------------------------------------------------------------
+#define PLIS_POISSON_BIG 1099511627776.0  // 2^40: returned for lambda >= 2^40 (counts overflow anyway)
+
+PLIS_HD double plis_poisson_d(plis_stream* st, double lam) {
+  if (!(lam > 0.0)) return 0.0;
+  if (lam >= PLIS_POISSON_BIG) return PLIS_POISSON_BIG;
+  if (lam < 10.0) {
+    // inversion by sequential search
+    double u = plis_uniform_d(st);
+    double p = plis_exp(-lam);
+    double F = p;
+    double k = 0.0;
+    while (u > F) {
+      k += 1.0;
+      p = p * lam / k;
+      F += p;
+      if (p <= F * 8.673617379884035e-19 || k >= 200.0) break;  // tail below 2^-60: stop
+    }
+    return k;
+  }
+  // PTRS, Hormann (1993)
+  double slam = PLIS_SQRT(lam);
+  double loglam = plis_log(lam);
+  double b = 0.931 + 2.53 * slam;
+  double a = -0.059 + 0.02483 * b;
+  double invalpha = 1.1239 + 1.1328 / (b - 3.4);
+  double vr = 0.9277 - 3.6224 / (b - 2.0);
+  for (int it = 0; it < 64; ++it) {
+    double U = plis_uniform_d(st) - 0.5;
+    double V = plis_uniform_d(st);
+    double us = 0.5 - PLIS_FABS(U);
+    double k = PLIS_FLOOR((2.0 * a / us + b) * U + lam + 0.43);
+    if (us >= 0.07 && V <= vr) return k;
+    if (k < 0.0 || (us < 0.013 && V > us)) continue;
+    double lhs = plis_log(V) + plis_log(invalpha) - plis_log(a / (us * us) + b);
+    double rhs = -lam + k * loglam - plis_lnfact(k);
+    if (lhs <= rhs) return k;
+  }
+  return PLIS_FLOOR(lam);
+}
+
+// Integer value of a drawn count (clamped at 2^40 so the conversion is always defined).
+PLIS_HD long long plis_count_d(double k) { return k >= PLIS_POISSON_BIG ? (1LL << 40) : (long long)k; }
+PLIS_HD long long plis_count_f(float k) { return k >= 1099511627776.0f ? (1LL << 40) : (long long)k; }
+
+PLIS_HD double plis_exponential_d(plis_stream* st, double rate) {
+  double u = plis_uniform_d(st);
+  return -plis_log(u) / rate;
+}
+
+// ------------------------------------------------------------------------------------------------
+// binary32 variants (the FP32 precision form).  Same methods, shorter series.
+// ------------------------------------------------------------------------------------------------
+#define PLIS_LN2_HI_F 0.69311523f      // ln 2 rounded to 12 significant bits
+#define PLIS_LN2_LO_F 3.1946183e-05f   // ln 2 - PLIS_LN2_HI_F
+#define PLIS_INV_LN2_F 1.442695f
+#define PLIS_SQRT2_F 1.4142135f
+
+PLIS_HD float plis_pow2i_f(int k) { return plis_u2f((uint32_t)(k + 127) << 23); }
+
+PLIS_HD float plis_expf(float x) {
+  if (x != x) return x;
+  if (x < -103.9f) return 0.0f;
+  if (x > 88.72f) return PLIS_INF_F;
+  float kf = PLIS_FLOORF(x * PLIS_INV_LN2_F + 0.5f);
+  int k = (int)kf;
+  float r = (x - kf * PLIS_LN2_HI_F) - kf * PLIS_LN2_LO_F;
+  float p = 2.4801588e-05f;  // Taylor through r^8
+  p = PLIS_FMAF(p, r, 0.0001984127f);
+  p = PLIS_FMAF(p, r, 0.0013888889f);
+  p = PLIS_FMAF(p, r, 0.008333334f);
+  p = PLIS_FMAF(p, r, 0.041666668f);
+  p = PLIS_FMAF(p, r, 0.16666667f);
+  p = PLIS_FMAF(p, r, 0.5f);
+  p = PLIS_FMAF(p, r, 1.0f);
+  p = PLIS_FMAF(p, r, 1.0f);
+  if (k >= -126) {
+    if (k > 127) return (p * plis_pow2i_f(127)) * 2.0f;
+    return p * plis_pow2i_f(k);
+  }
+  return (p * plis_pow2i_f(k + 30)) * 9.3132257e-10f;  // 2^-30
+}
+
+PLIS_HD float plis_logf(float x) {
+  if (!(x > 0.0f)) return (x == 0.0f) ? -PLIS_INF_F : PLIS_NAN_F;
+  if (plis_isinf_f(x)) return x;
+  uint32_t b = plis_f2u(x);
+  int e = (int)((b >> 23) & 0xFF);
+  if (e == 0) {
+    x = x * 16777216.0f;  // 2^24
+    b = plis_f2u(x);
+    e = (int)((b >> 23) & 0xFF) - 24;
+  }
+  e -= 127;
+  float m = plis_u2f((b & 0x007FFFFFu) | 0x3F800000u);
+  if (m > PLIS_SQRT2_F) { m = m * 0.5f; e += 1; }
+  float s = (m - 1.0f) / (m + 1.0f);
+  float s2 = s * s;
+  float q = 0.09090909f;  // through s^11/11
+  q = PLIS_FMAF(q, s2, 0.11111111f);
+  q = PLIS_FMAF(q, s2, 0.14285715f);
+  q = PLIS_FMAF(q, s2, 0.2f);
+  q = PLIS_FMAF(q, s2, 0.33333334f);
+  float lm = 2.0f * PLIS_FMAF(s * s2, q, s);
+  float ef = (float)e;
+  return ef * PLIS_LN2_HI_F + (ef * PLIS_LN2_LO_F + lm);
+}
+
+PLIS_HD float plis_lnfactf(float k) {
+  if (k <= 16.0f) return (float)plis_lnfact((double)k);
+  float z = k + 1.0f;
+  float w = 1.0f / z;
+  float w2 = w * w;
+  float c = 0.0007936508f;
+  c = 0.0027777778f - w2 * c;
+  c = 0.083333336f - w2 * c;
+  return ((z - 0.5f) * plis_logf(z) - z) + (0.9189385f + w * c);
+}
+
+#define PLIS_POISSON_BIG_F 16777216.0f  // 2^24: float spacing exceeds 1 beyond this
+
+PLIS_HD float plis_poisson_f(plis_stream* st, float lam) {
+  if (!(lam > 0.0f)) return 0.0f;
+  if (lam >= PLIS_POISSON_BIG_F) return PLIS_FLOORF(lam);
+  if (lam < 10.0f) {
+    float u = plis_uniform_f(st);
+    float p = plis_expf(-lam);
+    float F = p;
+    float k = 0.0f;
+    while (u > F) {
+      k += 1.0f;
+      p = p * lam / k;
+      F += p;
+      if (p <= F * 2.9802322e-08f || k >= 100.0f) break;  // tail below 2^-25
+    }
+    return k;
+  }
+  float slam = PLIS_SQRTF(lam);
+  float loglam = plis_logf(lam);
+  float b = 0.931f + 2.53f * slam;
+  float a = -0.059f + 0.02483f * b;
+  float invalpha = 1.1239f + 1.1328f / (b - 3.4f);
+  float vr = 0.9277f - 3.6224f / (b - 2.0f);
+  for (int it = 0; it < 64; ++it) {
+    float U = plis_uniform_f(st) - 0.5f;
+    float V = plis_uniform_f(st);
+    float us = 0.5f - PLIS_FABSF(U);
+    float k = PLIS_FLOORF((2.0f * a / us + b) * U + lam + 0.43f);
+    if (us >= 0.07f && V <= vr) return k;
+    if (k < 0.0f || (us < 0.013f && V > us)) continue;
+    float lhs = plis_logf(V) + plis_logf(invalpha) - plis_logf(a / (us * us) + b);
+    float rhs = -lam + k * loglam - plis_lnfactf(k);
+    if (lhs <= rhs) return k;
+  }
+  return PLIS_FLOORF(lam);
+}
+
+#endif  // PLIS_STREAM_H_

@@ -1,0 +1,77 @@
+"""Bit-exact parity of the CUDA step (through the C ABI) with the host oracle on the same injected
+Philox stream: integer states, tau bits, flags, time bits, step/rollback/event counts, step by step
+and over whole runs (the latter through the CUDA-graph batches)."""
+import numpy as np
+import pytest
+
+from helpers import assert_same, chain_model, random_graph_model, ref_fixture
+
+pytestmark = pytest.mark.gpu
+
+
+def _pair(model, state, mode, precision, seed=11, epsilon=0.05, **kw):
+    from oracle.oracle import Oracle
+    from pliscuda_b200 import Simulation
+    sim = Simulation(model, mode=mode, precision=precision, seed=seed, epsilon=epsilon, **kw)
+    orc = Oracle.from_model(model, mode=mode, precision=precision, seed=seed, epsilon=epsilon)
+    sim.set_state(state)
+    orc.set_state(state)
+    return sim, orc
+
+
+def _cases():
+    """(id, builder, t_end or None, max steps of the final run, extra options)."""
+    from pliscuda_b200 import workloads
+    yield "schlogl8", lambda: workloads.schlogl(8), 0.5, 10**6, {}
+    yield "small_ab6", lambda: workloads.small_ab(6, seed=4), 1.0, 10**6, {}
+    yield "chain41", lambda: (chain_model(), np.where(np.arange(41) == 20, 100000, 0).astype(np.uint32)), 0.3, 10**6, {}
+    yield "react9", lambda: ref_fixture("test_react-9")[:2], 8.0, 10**6, {}          # critical + SSA events
+    yield "react64", lambda: ref_fixture("test_react-64")[:2], 8.0, 10**6, {}
+    yield "diff64", lambda: ref_fixture("test_diff-64")[:2], 0.2, 10**6, {}
+    yield "chemotaxis", lambda: ref_fixture("test_chemotaxis")[:2], 0.3, 10**6, {}  # 2 compartments, S=32
+    yield "randgraph", lambda: random_graph_model(), 1.0, 10**6, {}                 # explicit table, dimers
+    yield "network10", lambda: workloads.random_network(5), None, 300, {}            # S=10, stiff: step-bounded
+    yield "schlogl8_eps1", lambda: workloads.schlogl(8), 0.3, 10**6, {"epsilon": 1.0}      # rollbacks
+    yield "react9_eps3", lambda: ref_fixture("test_react-9")[:2], 8.0, 10**6, {"epsilon": 3.0}
+
+
+CASES = list(_cases())
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32"])
+@pytest.mark.parametrize("mode", [0, 1], ids=["ref", "corr"])
+@pytest.mark.parametrize("name,make,t_end,max_steps,kw", CASES, ids=[c[0] for c in CASES])
+def test_stepwise_bitexact(name, make, t_end, max_steps, kw, mode, precision):
+    from pliscuda_b200 import PlisError
+    model, state = make()
+    sim, orc = _pair(model, state, mode, precision, **kw)
+    assert_same(sim, orc, "init")
+    for k in range(12):
+        try:
+            sim.step(1)
+        except PlisError as e:  # the reference's rollback can get stuck; the oracle must agree
+            assert orc.step(1) == e.status
+            return
+        assert orc.step(1) == 0
+        assert_same(sim, orc, f"step {k + 1}")
+    t = float("inf") if t_end is None else t_end
+    if max_steps >= 10**6:
+        sim.run(t)
+    else:
+        sim.step(max_steps)
+    orc.advance(t, max_steps)
+    assert_same(sim, orc, f"final run")
+    assert sim.stats().stop_reason == orc.stats().stop_reason
+    assert sim.stats().exact_events == orc.stats().exact_events
+
+
+@pytest.mark.parametrize("mode", [0, 1], ids=["ref", "corr"])
+def test_graph_batches_match_single_steps(mode):
+    """A long run through CUDA-graph batches equals the oracle (rollbacks included)."""
+    from pliscuda_b200 import workloads
+    model, state = workloads.schlogl(16)
+    sim, orc = _pair(model, state, mode, 0, seed=3, steps_per_launch=16)
+    sim.run(2.0)
+    orc.run(2.0)
+    assert_same(sim, orc, "run 2.0")
+    assert sim.stats().steps > 100
