@@ -169,6 +169,20 @@ def cpu_baseline_sample(model, state, threads, budget_s=12.0):
                       f"oracle, OpenMP {threads} threads, {el:.1f} s"}
 
 
+def ncu_case(args):
+    """Fixed small case for ncu captures: the bench workload, 40 leap steps of warm-up, then 3
+    profiled ones (capture with -k regex:k_leap -s 40 -c 3, or the classify kernel likewise)."""
+    from pliscuda_b200 import Simulation
+    model, state = _workload(args.workload)
+    with Simulation(model, mode=args.mode, precision=args.precision, seed=1000) as sim:
+        sim.set_state(state)
+        for _ in range(4):  # chunks below the graph batch size: plain launches, no idle graph tail
+            sim.step(10)
+        st = sim.step(3)
+    print(json.dumps({"ncu_case": args.workload, "steps": st.steps, "events": st.events}))
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -181,9 +195,12 @@ def main(argv=None):
     ap.add_argument("--ref-slice", type=float, default=0.01)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--ncu-case", action="store_true", help="run only the fixed ncu capture case")
     args = ap.parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
+    if args.ncu_case:
+        return ncu_case(args)
 
     import numpy as np
     import torch

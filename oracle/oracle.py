@@ -150,3 +150,52 @@ class Oracle:
         st = Stats()
         lib().oracle_get_stats(self._h, ctypes.byref(st))
         return st
+
+
+# ---------------------------------------------------------------------------------------------
+# stream numerics (shared with the CUDA step) for known-answer and statistical tests
+# ---------------------------------------------------------------------------------------------
+def philox(ctr, key):
+    L = lib()
+    c = (ctypes.c_uint32 * 4)(*ctr)
+    k = (ctypes.c_uint32 * 2)(*key)
+    o = (ctypes.c_uint32 * 4)()
+    L.oracle_philox(c, k, o)
+    return list(o)
+
+
+def poisson(lam, n, seed=1, step=1, channel=0, precision=0):
+    L = lib()
+    out = np.empty(n, np.float64)
+    L.oracle_poisson.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_double,
+                                 ctypes.c_int, ctypes.c_int64, ctypes.c_void_p]
+    L.oracle_poisson(seed, step, channel, float(lam), precision, n, _p(out))
+    return out
+
+
+def uniforms(n, seed=1, cell=0, precision=0):
+    L = lib()
+    out = np.empty(n, np.float64)
+    L.oracle_uniforms.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int, ctypes.c_int64, ctypes.c_void_p]
+    L.oracle_uniforms(seed, cell, precision, n, _p(out))
+    return out
+
+
+def exponential(rate, n, seed=1):
+    L = lib()
+    out = np.empty(n, np.float64)
+    L.oracle_exponential.argtypes = [ctypes.c_uint64, ctypes.c_double, ctypes.c_int64, ctypes.c_void_p]
+    L.oracle_exponential(seed, float(rate), n, _p(out))
+    return out
+
+
+_MATH = {"exp": 0, "log": 1, "expf": 2, "logf": 3, "lnfact": 4}
+
+
+def math(fn, x):
+    L = lib()
+    x = np.ascontiguousarray(x, np.float64)
+    out = np.empty_like(x)
+    L.oracle_math.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]
+    L.oracle_math(_MATH[fn], _p(x), x.size, _p(out))
+    return out

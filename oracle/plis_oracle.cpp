@@ -46,14 +46,24 @@ enum Flag : uint8_t { LEAP_CR = 0, LEAP_NOCR = 1, SSA = 2, SSA_FF = 3 };  // enu
 template <typename Real> struct RealOps;
 template <> struct RealOps<double> {
   static double poisson(plis_stream* s, double lam) { return plis_poisson_d(s, lam); }
+  static double emlam(double lam) { return lam < 10.0 ? plis_exp(-lam) : 0.0; }
+  static double poisson_shared(plis_stream* s, double lam, double em) {
+    if (!(lam > 0.0)) return 0.0;
+    return lam < 10.0 ? plis_poisson_small_d(s, lam, em) : plis_poisson_d(s, lam);
+  }
   static int64_t count(double k) { return (int64_t)plis_count_d(k); }
   static double uniform(plis_stream* s) { return plis_uniform_d(s); }
   static double inf() { return PLIS_INF_D; }
   static double fabs_(double x) { return fabs(x); }
 };
 template <> struct RealOps<float> {
-  static float poisson(plis_stream* s, float lam) { return plis_poisson_f(s, lam); }
-  static int64_t count(float k) { return (int64_t)plis_count_f(k); }
+  static double poisson(plis_stream* s, float lam) { return plis_poisson_f(s, lam); }
+  static float emlam(float lam) { return lam < 10.0f ? plis_expf(-lam) : 0.0f; }
+  static double poisson_shared(plis_stream* s, float lam, float em) {
+    if (!(lam > 0.0f)) return 0.0;
+    return lam < 10.0f ? plis_poisson_small_f(s, lam, em) : plis_poisson_d(s, (double)lam);
+  }
+  static int64_t count(double k) { return (int64_t)plis_count_d(k); }
   static float uniform(plis_stream* s) { return plis_uniform_f(s); }
   static float inf() { return PLIS_INF_F; }
   static float fabs_(float x) { return fabsf(x); }
@@ -393,9 +403,10 @@ struct Sim : Base {
         if (cnt(x, s, c) < nc) continue;  // is_critical_diffusion, tau.cu:42-45
         if (mode == 0 && n > 0) mark = 1;  // leap.cu:54-56 marks every receiver
         Real lam = tl * dr_c[(size_t)s * N + c];
+        Real em = Ops::emlam(lam);
         for (int j = 0; j < n; ++j) {
           plis_stream sd = plis_stream_make(opt.seed, opt.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_diff(s, j));
-          int64_t k = Ops::count(Ops::poisson(&sd, lam));
+          int64_t k = Ops::count(Ops::poisson_shared(&sd, lam, em));
           if (k >= kBigJump) big = 1;
           outk[((size_t)c * S + s) * 6 + j] = k;
           own[(size_t)c * S + s] -= k;
@@ -729,6 +740,51 @@ int oracle_get_stats(void* h, oracle_stats* st) {
 }
 int oracle_advance(void* h, double t_end, uint64_t max_steps) {
   return static_cast<Base*>(h)->advance(t_end, max_steps);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Test hooks over the shared stream numerics (pliscuda_b200/csrc/plis_stream.h).
+// ---------------------------------------------------------------------------------------------
+extern "C" {
+
+void oracle_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
+  plis_u32x4 c = {ctr[0], ctr[1], ctr[2], ctr[3]};
+  plis_u32x4 r = plis_philox4x32_10(c, key[0], key[1]);
+  out[0] = r.x; out[1] = r.y; out[2] = r.z; out[3] = r.w;
+}
+
+// n draws, draw i from the stream of (seed, cell=i, phase LEAP, step, attempt 0, channel)
+void oracle_poisson(uint64_t seed, uint64_t step, uint32_t channel, double lam, int precision, int64_t n, double* out) {
+  for (int64_t i = 0; i < n; ++i) {
+    plis_stream s = plis_stream_make(seed, 0, (uint32_t)i, PLIS_PHASE_LEAP, step, 0, channel);
+    out[i] = precision ? plis_poisson_f(&s, (float)lam) : plis_poisson_d(&s, lam);
+  }
+}
+
+void oracle_uniforms(uint64_t seed, uint32_t cell, int precision, int64_t n, double* out) {
+  plis_stream s = plis_stream_make(seed, 0, cell, PLIS_PHASE_INIT, 0, 0, 0);
+  for (int64_t i = 0; i < n; ++i) out[i] = precision ? (double)plis_uniform_f(&s) : plis_uniform_d(&s);
+}
+
+void oracle_exponential(uint64_t seed, double rate, int64_t n, double* out) {
+  for (int64_t i = 0; i < n; ++i) {
+    plis_stream s = plis_stream_make(seed, 0, (uint32_t)i, PLIS_PHASE_TAU, 1, 0, 0);
+    out[i] = plis_exponential_d(&s, rate);
+  }
+}
+
+void oracle_math(int which, const double* x, int64_t n, double* out) {
+  for (int64_t i = 0; i < n; ++i) {
+    switch (which) {
+      case 0: out[i] = plis_exp(x[i]); break;
+      case 1: out[i] = plis_log(x[i]); break;
+      case 2: out[i] = (double)plis_expf((float)x[i]); break;
+      case 3: out[i] = (double)plis_logf((float)x[i]); break;
+      default: out[i] = plis_lnfact(x[i]); break;
+    }
+  }
 }
 
 }  // extern "C"

@@ -149,7 +149,7 @@ int Engine::create(const Model& model, const plis_options& opt) {
     if (tx * ty * tz > 512 || tx * ty * tz == 0) { err_ = "tile has more than 512 subvolumes"; return PLIS_ERR_INVALID; }
     g.tx = tx; g.ty = ty; g.tz = tz;
     g.ntx = (dm.X + tx - 1) / tx; g.nty = (dm.Y + ty - 1) / ty; g.ntz = (dm.Z + tz - 1) / tz;
-    g.threads = tx * ty * tz;
+    g.threads = (tx * ty * tz + 31u) & ~31u;  // whole warps: the CTA reductions shuffle full warps
     const uint64_t nb = (uint64_t)g.ntx * g.nty * g.ntz;
     if (nb > 0x7FFFFFFFull) { err_ = "grid too large"; return PLIS_ERR_LIMIT; }
     g.nblocks = (uint32_t)nb;

@@ -39,14 +39,24 @@ namespace plis {
 template <typename Real> struct RT;
 template <> struct RT<double> {
   static __device__ __forceinline__ double poisson(plis_stream* s, double lam) { return plis_poisson_d(s, lam); }
+  static __device__ __forceinline__ double emlam(double lam) { return lam < 10.0 ? plis_exp(-lam) : 0.0; }
+  static __device__ __forceinline__ double poisson_shared(plis_stream* s, double lam, double em) {
+    if (!(lam > 0.0)) return 0.0;
+    return lam < 10.0 ? plis_poisson_small_d(s, lam, em) : plis_poisson_d(s, lam);
+  }
   static __device__ __forceinline__ double uniform(plis_stream* s) { return plis_uniform_d(s); }
   static __device__ __forceinline__ long long count(double k) { return plis_count_d(k); }
   static __device__ __forceinline__ double inf() { return PLIS_INF_D; }
 };
 template <> struct RT<float> {
-  static __device__ __forceinline__ float poisson(plis_stream* s, float lam) { return plis_poisson_f(s, lam); }
+  static __device__ __forceinline__ double poisson(plis_stream* s, float lam) { return plis_poisson_f(s, lam); }
+  static __device__ __forceinline__ float emlam(float lam) { return lam < 10.0f ? plis_expf(-lam) : 0.0f; }
+  static __device__ __forceinline__ double poisson_shared(plis_stream* s, float lam, float em) {
+    if (!(lam > 0.0f)) return 0.0;
+    return lam < 10.0f ? plis_poisson_small_f(s, lam, em) : plis_poisson_d(s, (double)lam);
+  }
   static __device__ __forceinline__ float uniform(plis_stream* s) { return plis_uniform_f(s); }
-  static __device__ __forceinline__ long long count(float k) { return plis_count_f(k); }
+  static __device__ __forceinline__ long long count(double k) { return plis_count_d(k); }
   static __device__ __forceinline__ float inf() { return PLIS_INF_F; }
 };
 
@@ -84,6 +94,7 @@ template <int MAXS> struct Deltas {
 __device__ __forceinline__ bool cell_of(const KArgs& A, uint32_t& c) {
   if (A.m.lattice) {
     const uint32_t b = blockIdx.x, t = threadIdx.x;
+    if (t >= A.g.tx * A.g.ty * A.g.tz) return false;  // block rounded up to whole warps
     const uint32_t bx = b % A.g.ntx, br = b / A.g.ntx;
     const uint32_t by = br % A.g.nty, bz = br / A.g.nty;
     const uint32_t lx = t % A.g.tx, tr = t / A.g.tx;
@@ -478,10 +489,11 @@ __global__ void __launch_bounds__(512) k_leap(KArgs A) {
         if (xs < nc) continue;  // is_critical_diffusion, tau.cu:42-45
         if (mode == 0 && n > 0) mark = true;
         const Real lam = tl * (drate<Real>(m, comp, s) * (Real)xs);
+        const Real em = RT<Real>::emlam(lam);  // one exp for the n draws of this species
         long long out = 0;
         for (int j = 0; j < n; ++j) {
           plis_stream st = plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_diff(s, j));
-          const long long k = RT<Real>::count(RT<Real>::poisson(&st, lam));
+          const long long k = RT<Real>::count(RT<Real>::poisson_shared(&st, lam, em));
           if (k >= kBigJump) big = 1;
           if (k > 0) {
             atomicAdd(&Xt[(size_t)s * m.Npad + nb[j]], (int)k);
@@ -819,15 +831,17 @@ __global__ void __launch_bounds__(512) k_classify(KArgs A) {
     s_last = ((prev & 0x7FFFFFFFu) == gridDim.x - 1);
   }
   __syncthreads();
-  if (!s_last || wid != 0) return;
+  if (!s_last) return;
 
   // ---- last CTA: grid-wide arg-min and the step decision ----
+  // every thread loads a strided share of the per-CTA slots (independent L2 loads in flight),
+  // then warp shuffles and one more pass over the warp results
   __threadfence();
   double gt = PLIS_INF_D;
   long long gi = 0x7FFFFFFFFFFFFFFFll;
   unsigned long long gcr = 0;
   uint32_t gbad = 0;
-  for (uint32_t b = lane; b < gridDim.x; b += 32) {
+  for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
     min_pair(gt, gi, __ldcg(&A.b.slot_tau[b]), __ldcg(&A.b.slot_idx[b]));
     gcr += __ldcg(&A.b.slot_cr[b]);
     gbad |= __ldcg(&A.b.slot_bad[b]);
@@ -835,6 +849,21 @@ __global__ void __launch_bounds__(512) k_classify(KArgs A) {
   warp_min_pair(gt, gi);
   gcr = (unsigned long long)warp_sum((long long)gcr);
   gbad = __reduce_or_sync(0xffffffffu, gbad);
+  __shared__ unsigned long long s_cr[32];
+  __shared__ uint32_t s_bad[32];
+  if (lane == 0) { s_t[wid] = gt; s_i[wid] = gi; s_cr[wid] = gcr; s_bad[wid] = gbad; }
+  __syncthreads();
+  if (wid != 0) return;
+  {
+    const int nw = (blockDim.x + 31) >> 5;
+    gt = lane < nw ? s_t[lane] : PLIS_INF_D;
+    gi = lane < nw ? s_i[lane] : 0x7FFFFFFFFFFFFFFFll;
+    gcr = lane < nw ? s_cr[lane] : 0ull;
+    gbad = lane < nw ? s_bad[lane] : 0u;
+    warp_min_pair(gt, gi);
+    gcr = (unsigned long long)warp_sum((long long)gcr);
+    gbad = __reduce_or_sync(0xffffffffu, gbad);
+  }
   if (lane != 0) return;
   const int mode = A.o.mode;
   const uint32_t leap_bad = (__ldcg(&K->blocks_done) & 0x80000000u) ? 1u : 0u;

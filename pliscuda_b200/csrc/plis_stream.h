@@ -125,7 +125,9 @@ PLIS_HD plis_u32x4 plis_philox4x32_10(plis_u32x4 c, uint32_t k0, uint32_t k1) {
 
 // ------------------------------------------------------------------------------------------------
 // Counter layout.  One "channel" of one subvolume in one phase of one attempt of one step owns the
-// sub-stream (c.y low 12 bits = sub, incremented per Philox block):
+// sub-stream (c.y low 12 bits = sub, incremented per Philox block).  A sub-stream holds 4096 blocks
+// (8192 binary64 or 16384 binary32 uniforms); the step never needs more than 64 blocks from one
+// (PTRS gives up after 64 rejections, the inversion search draws one uniform):
 //   c.x = subvolume index (within its replica)
 //   c.y = channel << 12 | sub          (channel < 2^20)
 //   c.z = step (low 32 bits)
@@ -311,6 +313,22 @@ PLIS_HD double plis_lnfact(double k) {
 // ------------------------------------------------------------------------------------------------
 #define PLIS_POISSON_BIG 1099511627776.0  // 2^40: returned for lambda >= 2^40 (counts overflow anyway)
 
+// Poisson(lam) for lam < 10 by inversion (sequential search from 0), given emlam = exp(-lam):
+// draws that share a mean (the per-neighbour diffusion draws of one species) share the exp.
+PLIS_HD double plis_poisson_small_d(plis_stream* st, double lam, double emlam) {
+  double u = plis_uniform_d(st);
+  double p = emlam;
+  double F = p;
+  double k = 0.0;
+  while (u > F) {
+    k += 1.0;
+    p = p * lam / k;
+    F += p;
+    if (p <= F * 8.673617379884035e-19 || k >= 200.0) break;  // tail below 2^-60: stop
+  }
+  return k;
+}
+
 PLIS_HD double plis_poisson_d(plis_stream* st, double lam) {
   if (!(lam > 0.0)) return 0.0;
   if (lam >= PLIS_POISSON_BIG) return PLIS_POISSON_BIG;
@@ -351,7 +369,6 @@ PLIS_HD double plis_poisson_d(plis_stream* st, double lam) {
 
 // Integer value of a drawn count (clamped at 2^40 so the conversion is always defined).
 PLIS_HD long long plis_count_d(double k) { return k >= PLIS_POISSON_BIG ? (1LL << 40) : (long long)k; }
-PLIS_HD long long plis_count_f(float k) { return k >= 1099511627776.0f ? (1LL << 40) : (long long)k; }
 
 PLIS_HD double plis_exponential_d(plis_stream* st, double rate) {
   double u = plis_uniform_d(st);
@@ -359,7 +376,8 @@ PLIS_HD double plis_exponential_d(plis_stream* st, double rate) {
 }
 
 // ------------------------------------------------------------------------------------------------
-// binary32 variants (the FP32 precision form).  Same methods, shorter series.
+// binary32 variants (the FP32 precision form).  Same methods, shorter series; Poisson means of 10
+// and above are sampled by the binary64 PTRS.
 // ------------------------------------------------------------------------------------------------
 #define PLIS_LN2_HI_F 0.69311523f      // ln 2 rounded to 12 significant bits
 #define PLIS_LN2_LO_F 3.1946183e-05f   // ln 2 - PLIS_LN2_HI_F
@@ -416,22 +434,23 @@ PLIS_HD float plis_logf(float x) {
   return ef * PLIS_LN2_HI_F + (ef * PLIS_LN2_LO_F + lm);
 }
 
-PLIS_HD float plis_lnfactf(float k) {
-  if (k <= 16.0f) return (float)plis_lnfact((double)k);
-  float z = k + 1.0f;
-  float w = 1.0f / z;
-  float w2 = w * w;
-  float c = 0.0007936508f;
-  c = 0.0027777778f - w2 * c;
-  c = 0.083333336f - w2 * c;
-  return ((z - 0.5f) * plis_logf(z) - z) + (0.9189385f + w * c);
+PLIS_HD double plis_poisson_small_f(plis_stream* st, float lam, float emlam) {
+  float u = plis_uniform_f(st);
+  float p = emlam;
+  float F = p;
+  float k = 0.0f;
+  while (u > F) {
+    k += 1.0f;
+    p = p * lam / k;
+    F += p;
+    if (p <= F * 2.9802322e-08f || k >= 100.0f) break;  // tail below 2^-25
+  }
+  return (double)k;
 }
 
-#define PLIS_POISSON_BIG_F 16777216.0f  // 2^24: float spacing exceeds 1 beyond this
-
-PLIS_HD float plis_poisson_f(plis_stream* st, float lam) {
-  if (!(lam > 0.0f)) return 0.0f;
-  if (lam >= PLIS_POISSON_BIG_F) return PLIS_FLOORF(lam);
+// Returns the count as a double (exact integer), like plis_poisson_d.
+PLIS_HD double plis_poisson_f(plis_stream* st, float lam) {
+  if (!(lam > 0.0f)) return 0.0;
   if (lam < 10.0f) {
     float u = plis_uniform_f(st);
     float p = plis_expf(-lam);
@@ -443,26 +462,11 @@ PLIS_HD float plis_poisson_f(plis_stream* st, float lam) {
       F += p;
       if (p <= F * 2.9802322e-08f || k >= 100.0f) break;  // tail below 2^-25
     }
-    return k;
+    return (double)k;
   }
-  float slam = PLIS_SQRTF(lam);
-  float loglam = plis_logf(lam);
-  float b = 0.931f + 2.53f * slam;
-  float a = -0.059f + 0.02483f * b;
-  float invalpha = 1.1239f + 1.1328f / (b - 3.4f);
-  float vr = 0.9277f - 3.6224f / (b - 2.0f);
-  for (int it = 0; it < 64; ++it) {
-    float U = plis_uniform_f(st) - 0.5f;
-    float V = plis_uniform_f(st);
-    float us = 0.5f - PLIS_FABSF(U);
-    float k = PLIS_FLOORF((2.0f * a / us + b) * U + lam + 0.43f);
-    if (us >= 0.07f && V <= vr) return k;
-    if (k < 0.0f || (us < 0.013f && V > us)) continue;
-    float lhs = plis_logf(V) + plis_logf(invalpha) - plis_logf(a / (us * us) + b);
-    float rhs = -lam + k * loglam - plis_lnfactf(k);
-    if (lhs <= rhs) return k;
-  }
-  return PLIS_FLOORF(lam);
+  // lambda >= 10: the PTRS acceptance test compares ln-probabilities of size ~lambda*ln(lambda),
+  // which binary32 cannot resolve (its spacing near 1e6 is 0.125), so it runs in binary64.
+  return plis_poisson_d(st, (double)lam);
 }
 
 #endif  // PLIS_STREAM_H_
