@@ -146,7 +146,7 @@ int Engine::create(const Model& model, const plis_options& opt) {
     uint32_t tx = opt.tile[0] > 0 ? (uint32_t)opt.tile[0] : std::min<uint32_t>(32, pow2_at_least(dm.X));
     uint32_t ty = opt.tile[1] > 0 ? (uint32_t)opt.tile[1] : std::min<uint32_t>(std::max<uint32_t>(1, 256 / tx), pow2_at_least(dm.Y));
     uint32_t tz = opt.tile[2] > 0 ? (uint32_t)opt.tile[2] : std::min<uint32_t>(std::max<uint32_t>(1, 256 / (tx * ty)), pow2_at_least(dm.Z));
-    if (tx * ty * tz > 512 || tx * ty * tz == 0) { err_ = "tile has more than 512 subvolumes"; return PLIS_ERR_INVALID; }
+    if (tx * ty * tz > 256 || tx * ty * tz == 0) { err_ = "tile must hold 1..256 subvolumes"; return PLIS_ERR_INVALID; }
     g.tx = tx; g.ty = ty; g.tz = tz;
     g.ntx = (dm.X + tx - 1) / tx; g.nty = (dm.Y + ty - 1) / ty; g.ntz = (dm.Z + tz - 1) / tz;
     g.threads = (tx * ty * tz + 31u) & ~31u;  // whole warps: the CTA reductions shuffle full warps

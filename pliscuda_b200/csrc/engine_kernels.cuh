@@ -60,6 +60,116 @@ template <> struct RT<float> {
   static __device__ __forceinline__ float inf() { return PLIS_INF_F; }
 };
 
+// Per-neighbour diffusion draws of one species (leap.cu:49-53).  All n draws have the same mean, so
+// for lam < 10 the inversion CDF is built once, up to the largest of the n uniforms, and each draw
+// reads its result off it: identical results to n separate sequential searches
+// (plis_poisson_small_d / _f), max_j k_j iterations instead of sum_j k_j.
+template <typename Real> struct DiffTraits;
+template <> struct DiffTraits<double> {
+  static __device__ __forceinline__ double uni(plis_stream* s) { return plis_uniform_d(s); }
+  static constexpr double tail = 8.673617379884035e-19;
+  static constexpr int kmax = 200;
+};
+template <> struct DiffTraits<float> {
+  static __device__ __forceinline__ float uni(plis_stream* s) { return plis_uniform_f(s); }
+  static constexpr float tail = 2.9802322e-08f;
+  static constexpr int kmax = 100;
+};
+
+template <typename Real>
+__device__ __forceinline__ void diffusion_draws(const KArgs& A, uint32_t c, int s, int n, Real lam, Real em,
+                                                uint64_t step, uint32_t attempt, long long k[6]) {
+  if (!(lam > (Real)0)) {
+#pragma unroll
+    for (int j = 0; j < 6; ++j) k[j] = 0;
+    return;
+  }
+  if (!(lam < (Real)10)) {
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+      k[j] = 0;
+      if (j < n) {
+        plis_stream st = plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_diff(s, j));
+        k[j] = plis_count_d(plis_poisson_d(&st, (double)lam));
+      }
+    }
+    return;
+  }
+  Real u[6];
+  bool open_[6];
+  Real p = em, F = em;
+  bool pending = false;
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    u[j] = (Real)0;
+    open_[j] = false;
+    k[j] = 0;
+    if (j < n) {
+      plis_stream st = plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_diff(s, j));
+      u[j] = DiffTraits<Real>::uni(&st);
+      open_[j] = u[j] > F;
+      pending |= open_[j];
+    }
+  }
+  int ki = 0;
+  while (pending) {
+    ki += 1;
+    p = (p * lam) * (Real)plis_inv_k_tab[ki];
+    F += p;
+    const bool brk = (p <= F * DiffTraits<Real>::tail) || ki >= DiffTraits<Real>::kmax;
+    pending = false;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+      if (open_[j] && (!(u[j] > F) || brk)) {
+        open_[j] = false;
+        k[j] = ki;
+      }
+      pending |= open_[j];
+    }
+  }
+}
+
+// Up to 4 reaction draws with means in (0, 10) advanced in lockstep: each is exactly the sequential
+// search of plis_poisson_small_d / _f (same arithmetic per draw), but the independent chains give
+// the FP64 pipe four times the instruction-level parallelism and the loop runs max_i k_i times.
+template <typename Real>
+__device__ __forceinline__ void batched_small_draws(const Real u[4], const Real lam[4], const bool act[4], long long k[4]) {
+  Real p[4], F[4];
+  bool open_[4];
+  bool pending = false;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    k[i] = 0;
+    open_[i] = false;
+    p[i] = F[i] = (Real)0;
+    if (act[i]) {
+      p[i] = RT<Real>::emlam(lam[i]);
+      F[i] = p[i];
+      open_[i] = u[i] > F[i];
+      pending |= open_[i];
+    }
+  }
+  int ki = 0;
+  while (pending) {
+    ki += 1;
+    const Real ik = (Real)plis_inv_k_tab[ki];
+    pending = false;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      if (open_[i]) {
+        p[i] = (p[i] * lam[i]) * ik;
+        F[i] += p[i];
+        const bool brk = (p[i] <= F[i] * DiffTraits<Real>::tail) || ki >= DiffTraits<Real>::kmax;
+        if (!(u[i] > F[i]) || brk) {
+          open_[i] = false;
+          k[i] = ki;
+        }
+        pending |= open_[i];
+      }
+    }
+  }
+}
+
 // Per-thread copy of one subvolume's counts.  Small species counts stay in registers: the
 // selection loops below use compile-time indices only.
 template <int MAXS> struct Counts {
@@ -91,24 +201,72 @@ template <int MAXS> struct Deltas {
 // ------------------------------------------------------------------------------------------------
 // geometry
 // ------------------------------------------------------------------------------------------------
-__device__ __forceinline__ bool cell_of(const KArgs& A, uint32_t& c) {
+struct Cell {
+  uint32_t c;        // linear index
+  uint32_t x, y, z;  // lattice coordinates (lattice topology only)
+};
+
+__device__ __forceinline__ bool cell_of(const KArgs& A, uint32_t block, Cell& cl) {
   if (A.m.lattice) {
-    const uint32_t b = blockIdx.x, t = threadIdx.x;
+    const uint32_t b = block, t = threadIdx.x;
     if (t >= A.g.tx * A.g.ty * A.g.tz) return false;  // block rounded up to whole warps
     const uint32_t bx = b % A.g.ntx, br = b / A.g.ntx;
     const uint32_t by = br % A.g.nty, bz = br / A.g.nty;
     const uint32_t lx = t % A.g.tx, tr = t / A.g.tx;
     const uint32_t ly = tr % A.g.ty, lz = tr / A.g.ty;
-    const uint32_t x = bx * A.g.tx + lx, y = by * A.g.ty + ly, z = bz * A.g.tz + lz;
-    if (x >= A.m.X || y >= A.m.Y || z >= A.m.Z) return false;
-    c = x + A.m.X * (y + A.m.Y * z);
+    cl.x = bx * A.g.tx + lx;
+    cl.y = by * A.g.ty + ly;
+    cl.z = bz * A.g.tz + lz;
+    if (cl.x >= A.m.X || cl.y >= A.m.Y || cl.z >= A.m.Z) return false;
+    cl.c = cl.x + A.m.X * (cl.y + A.m.Y * cl.z);
     return true;
   }
-  c = blockIdx.x * blockDim.x + threadIdx.x;
-  return c < A.m.N;
+  cl.c = block * blockDim.x + threadIdx.x;
+  cl.x = cl.y = cl.z = 0;
+  return cl.c < A.m.N;
+}
+__device__ __forceinline__ bool cell_of(const KArgs& A, uint32_t& c) {
+  Cell cl;
+  const bool v = cell_of(A, blockIdx.x, cl);
+  c = cl.c;
+  return v;
 }
 
-// canonical neighbours: lattice rows -x,+x,-y,+y,-z,+z (absent ones skipped), else the table
+// Canonical neighbours of a subvolume and their own neighbour counts.  Lattice rows are
+// -x,+x,-y,+y,-z,+z (absent ones skipped), derived from the coordinates without divisions.
+struct Nbr {
+  uint32_t nb[6];
+  uint8_t nn[6];
+  int n;
+};
+
+__device__ __forceinline__ int axis_count(uint32_t v, uint32_t dim) { return (v > 0) + (v + 1 < dim); }
+
+__device__ __forceinline__ void nbr_info(const DevModel& m, const Cell& cl, Nbr& q) {
+  const uint32_t c = cl.c;
+  if (m.lattice) {
+    const uint32_t X = m.X, Y = m.Y, Z = m.Z, XY = m.X * m.Y;
+    const int ax = axis_count(cl.x, X), ay = axis_count(cl.y, Y), az = axis_count(cl.z, Z);
+    int n = 0;
+    if (cl.x > 0) { q.nb[n] = c - 1; q.nn[n++] = (uint8_t)(axis_count(cl.x - 1, X) + ay + az); }
+    if (cl.x + 1 < X) { q.nb[n] = c + 1; q.nn[n++] = (uint8_t)(axis_count(cl.x + 1, X) + ay + az); }
+    if (cl.y > 0) { q.nb[n] = c - X; q.nn[n++] = (uint8_t)(ax + axis_count(cl.y - 1, Y) + az); }
+    if (cl.y + 1 < Y) { q.nb[n] = c + X; q.nn[n++] = (uint8_t)(ax + axis_count(cl.y + 1, Y) + az); }
+    if (cl.z > 0) { q.nb[n] = c - XY; q.nn[n++] = (uint8_t)(ax + ay + axis_count(cl.z - 1, Z)); }
+    if (cl.z + 1 < Z) { q.nb[n] = c + XY; q.nn[n++] = (uint8_t)(ax + ay + axis_count(cl.z + 1, Z)); }
+    q.n = n;
+    for (int j = n; j < 6; ++j) { q.nb[j] = c; q.nn[j] = 0; }
+    return;
+  }
+  q.n = m.ncount[c];
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    q.nb[j] = m.canon[(size_t)c * 6 + j];
+    q.nn[j] = j < q.n ? m.ncount[q.nb[j]] : 0;
+  }
+}
+
+// canonical neighbours of a subvolume given only its index (rare paths: exact events)
 __device__ __forceinline__ int nbrs(const DevModel& m, uint32_t c, uint32_t nb[6]) {
   if (m.lattice) {
     const uint32_t X = m.X, Y = m.Y, Z = m.Z;
@@ -126,15 +284,6 @@ __device__ __forceinline__ int nbrs(const DevModel& m, uint32_t c, uint32_t nb[6
 #pragma unroll
   for (int j = 0; j < 6; ++j) nb[j] = m.canon[(size_t)c * 6 + j];
   return n;
-}
-
-__device__ __forceinline__ int nbr_count(const DevModel& m, uint32_t b) {
-  if (m.lattice) {
-    const uint32_t X = m.X, Y = m.Y, Z = m.Z;
-    const uint32_t x = b % X, y = (b / X) % Y, z = b / (X * Y);
-    return (x > 0) + (x + 1 < X) + (y > 0) + (y + 1 < Y) + (z > 0) + (z + 1 < Z);
-  }
-  return m.ncount[b];
 }
 
 // slot-th entry of the canonical 6-wide row of c (self padding beyond the neighbour count)
@@ -234,7 +383,7 @@ __device__ __forceinline__ void load_counts(const DevModel& m, const int32_t* X,
 // classification of one subvolume (compute_taus, tau.cu:197-252)
 // ------------------------------------------------------------------------------------------------
 template <typename Real, int MAXS>
-__device__ void classify_cell(const KArgs& A, uint32_t c, const Counts<MAXS>& x, const int32_t* Xe,
+__device__ void classify_cell(const KArgs& A, uint32_t c, const Nbr& q, const Counts<MAXS>& x, const int32_t* Xe,
                               double tau_cur, uint8_t flag_cur, uint64_t step, uint32_t attempt,
                               double ff, double& tau_out, int& flag_out) {
   const DevModel& m = A.m;
@@ -250,8 +399,7 @@ __device__ void classify_cell(const KArgs& A, uint32_t c, const Counts<MAXS>& x,
     }
   }
   const int comp = comp_of(m, c);
-  uint32_t nb[6];
-  const int n = nbrs(m, c, nb);
+  const int n = q.n;
   const int S = (int)m.S, R = (int)m.R;
   Real tau_ncr = RT<Real>::inf();
   for (int s = 0; s < S; ++s) {
@@ -289,11 +437,11 @@ __device__ void classify_cell(const KArgs& A, uint32_t c, const Counts<MAXS>& x,
     if (mode == 0) {
       if (xs >= nc) { mu = mu + d; s2 = s2 + d; }
       for (int j = 0; j < n; ++j) {
-        const uint32_t b = nb[j];
+        const uint32_t b = q.nb[j];
         const Real db = drate<Real>(m, comp_of(m, b), s) * (Real)Xe[(size_t)s * m.Npad + b];
-        const Real q = db / (Real)nbr_count(m, b);
-        mu = mu - q;
-        s2 = s2 + q;
+        const Real qd = db / (Real)q.nn[j];
+        mu = mu - qd;
+        s2 = s2 + qd;
       }
     } else {
       if (xs >= nc && n > 0) {
@@ -302,12 +450,12 @@ __device__ void classify_cell(const KArgs& A, uint32_t c, const Counts<MAXS>& x,
         s2 = s2 + dout;
       }
       for (int j = 0; j < n; ++j) {
-        const uint32_t b = nb[j];
+        const uint32_t b = q.nb[j];
         const int32_t xb = Xe[(size_t)s * m.Npad + b];
         if (xb >= nc) {
-          const Real q = drate<Real>(m, comp_of(m, b), s) * (Real)xb;
-          mu = mu + q;
-          s2 = s2 + q;
+          const Real qd = drate<Real>(m, comp_of(m, b), s) * (Real)xb;
+          mu = mu + qd;
+          s2 = s2 + qd;
         }
       }
     }
@@ -437,8 +585,13 @@ __device__ __forceinline__ long long warp_sum(long long v) {
 // ------------------------------------------------------------------------------------------------
 // k_leap (leap_step, leap.cu:3-65)
 // ------------------------------------------------------------------------------------------------
+// The leap is latency-bound on dependent FP64/integer chains: occupancy matters more than the few
+// registers it spills at this bound.
+#ifndef PLIS_LEAP_MIN_BLOCKS
+#define PLIS_LEAP_MIN_BLOCKS 4
+#endif
 template <typename Real, int MAXS>
-__global__ void __launch_bounds__(512) k_leap(KArgs A) {
+__global__ void __launch_bounds__(256, PLIS_LEAP_MIN_BLOCKS) k_leap(KArgs A) {
   Ctrl* K = A.b.ctrl;
   if (K->done) return;
   const DevModel& m = A.m;
@@ -453,8 +606,9 @@ __global__ void __launch_bounds__(512) k_leap(KArgs A) {
   __shared__ int s_big;
   if (threadIdx.x == 0) s_big = 0;
   __syncthreads();
-  uint32_t c = 0;
-  const bool valid = cell_of(A, c);
+  Cell cl;
+  const bool valid = cell_of(A, blockIdx.x, cl);
+  const uint32_t c = cl.c;
   long long ev = 0;
   int big = 0;
   if (valid) {
@@ -467,22 +621,53 @@ __global__ void __launch_bounds__(512) k_leap(KArgs A) {
     if (f == F_LEAP_CR || f == F_LEAP_NOCR) {  // leap.cu:9-10
       const int comp = comp_of(m, c);
       const int S = (int)m.S, R = (int)m.R;
-      for (int r = 0; r < R; ++r) {
-        const Real a = prop<Real>(m, x, r, comp);
-        const bool fire = (mode == 0) ? !crit_ref(m, x, r, nc) : ((a > (Real)0) && !crit_fix(m, x, r, a, nc));
-        if (!fire) continue;
-        plis_stream st = plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_react(r));
-        const long long k = RT<Real>::count(RT<Real>::poisson(&st, tl * a));
-        ev += k;
-        const int nn = m.n_net[r];
-        for (int i = 0; i < nn; ++i) {
-          const long long v = k * (long long)m.net_nu[r * 8 + i];
-          if (v >= kBigDraw || v <= -kBigDraw) big = 1;
-          dl.add(m.net_s[r * 8 + i], v);
+      for (int r0 = 0; r0 < R; r0 += 4) {
+        // reactions r0..r0+3: means >= 10 go through PTRS one by one, the rest in lockstep
+        Real u[4], lam[4];
+        bool act[4];
+        long long kk[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int r = r0 + i;
+          act[i] = false;
+          lam[i] = (Real)0;
+          u[i] = (Real)0;
+          kk[i] = 0;
+          if (r < R) {
+            const Real a = prop<Real>(m, x, r, comp);
+            const bool fire = (mode == 0) ? !crit_ref(m, x, r, nc) : ((a > (Real)0) && !crit_fix(m, x, r, a, nc));
+            lam[i] = fire ? tl * a : (Real)0;
+            if (lam[i] > (Real)0) {
+              plis_stream st = plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_react(r));
+              if (lam[i] < (Real)10) {
+                act[i] = true;
+                u[i] = DiffTraits<Real>::uni(&st);  // the inversion search's single uniform
+              } else {
+                kk[i] = RT<Real>::count(RT<Real>::poisson(&st, lam[i]));
+              }
+            }
+          }
+        }
+        long long ks[4];
+        batched_small_draws<Real>(u, lam, act, ks);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int r = r0 + i;
+          if (r >= R) continue;
+          const long long k = act[i] ? ks[i] : kk[i];
+          ev += k;
+          const int nn = m.n_net[r];
+          for (int q = 0; q < nn; ++q) {
+            const long long v = k * (long long)m.net_nu[r * 8 + q];
+            if (v >= kBigDraw || v <= -kBigDraw) big = 1;
+            dl.add(m.net_s[r * 8 + q], v);
+          }
         }
       }
-      uint32_t nb[6];
-      const int n = nbrs(m, c, nb);
+      Nbr q;
+      nbr_info(m, cl, q);
+      const int n = q.n;
+      const uint32_t* nb = q.nb;
       bool mark = false;
       for (int s = 0; s < S; ++s) {
         const int32_t xs = x.get(s);
@@ -490,10 +675,11 @@ __global__ void __launch_bounds__(512) k_leap(KArgs A) {
         if (mode == 0 && n > 0) mark = true;
         const Real lam = tl * (drate<Real>(m, comp, s) * (Real)xs);
         const Real em = RT<Real>::emlam(lam);  // one exp for the n draws of this species
+        long long kd[6];
+        diffusion_draws<Real>(A, c, s, n, lam, em, step, attempt, kd);
         long long out = 0;
         for (int j = 0; j < n; ++j) {
-          plis_stream st = plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_diff(s, j));
-          const long long k = RT<Real>::count(RT<Real>::poisson_shared(&st, lam, em));
+          const long long k = kd[j];
           if (k >= kBigJump) big = 1;
           if (k > 0) {
             atomicAdd(&Xt[(size_t)s * m.Npad + nb[j]], (int)k);
@@ -771,7 +957,7 @@ __global__ void __launch_bounds__(256) k_apply(KArgs A) {
 // k_classify + last-CTA control
 // ------------------------------------------------------------------------------------------------
 template <typename Real, int MAXS>
-__global__ void __launch_bounds__(512) k_classify(KArgs A) {
+__global__ void __launch_bounds__(256) k_classify(KArgs A) {
   Ctrl* K = A.b.ctrl;
   if (K->done) return;
   const DevModel& m = A.m;
@@ -791,8 +977,9 @@ __global__ void __launch_bounds__(512) k_classify(KArgs A) {
   __shared__ long long s_i[32];
   __shared__ bool s_last;
 
-  uint32_t c = 0;
-  const bool valid = cell_of(A, c);
+  Cell cl;
+  const bool valid = cell_of(A, blockIdx.x, cl);
+  const uint32_t c = cl.c;
   double tn = PLIS_INF_D;
   long long ti = 0x7FFFFFFFFFFFFFFFll;
   int fl = F_SSA_FF;
@@ -806,7 +993,9 @@ __global__ void __launch_bounds__(512) k_classify(KArgs A) {
         if (x.v[s] < 0) bad = 1;
         Xz[(size_t)s * m.Npad + c] = 0;
       }
-    classify_cell<Real>(A, c, x, Xe, tau_cur[c], flag_cur[c], step, attempt, ff, tn, fl);
+    Nbr q;
+    nbr_info(m, cl, q);
+    classify_cell<Real>(A, c, q, x, Xe, tau_cur[c], flag_cur[c], step, attempt, ff, tn, fl);
     tau_new[c] = tn;
     flag_new[c] = (uint8_t)fl;
     ti = c;

@@ -311,6 +311,50 @@ PLIS_HD double plis_lnfact(double k) {
 // ------------------------------------------------------------------------------------------------
 // Poisson, binary64
 // ------------------------------------------------------------------------------------------------
+// 1/k rounded to nearest, k = 0..200 (entry 0 unused): the inversion search multiplies by it
+// instead of dividing.  On the device it sits in constant memory; every active lane of a warp is at
+// the same k, so the read is a broadcast.
+#define PLIS_INV_K_VALUES \
+    0.0, 1.0, 0.5, 0.3333333333333333, 0.25, 0.2,\
+    0.16666666666666666, 0.14285714285714285, 0.125, 0.1111111111111111, 0.1, 0.09090909090909091,\
+    0.08333333333333333, 0.07692307692307693, 0.07142857142857142, 0.06666666666666667, 0.0625, 0.058823529411764705,\
+    0.05555555555555555, 0.05263157894736842, 0.05, 0.047619047619047616, 0.045454545454545456, 0.043478260869565216,\
+    0.041666666666666664, 0.04, 0.038461538461538464, 0.037037037037037035, 0.03571428571428571, 0.034482758620689655,\
+    0.03333333333333333, 0.03225806451612903, 0.03125, 0.030303030303030304, 0.029411764705882353, 0.02857142857142857,\
+    0.027777777777777776, 0.02702702702702703, 0.02631578947368421, 0.02564102564102564, 0.025, 0.024390243902439025,\
+    0.023809523809523808, 0.023255813953488372, 0.022727272727272728, 0.022222222222222223, 0.021739130434782608, 0.02127659574468085,\
+    0.020833333333333332, 0.02040816326530612, 0.02, 0.0196078431372549, 0.019230769230769232, 0.018867924528301886,\
+    0.018518518518518517, 0.01818181818181818, 0.017857142857142856, 0.017543859649122806, 0.017241379310344827, 0.01694915254237288,\
+    0.016666666666666666, 0.01639344262295082, 0.016129032258064516, 0.015873015873015872, 0.015625, 0.015384615384615385,\
+    0.015151515151515152, 0.014925373134328358, 0.014705882352941176, 0.014492753623188406, 0.014285714285714285, 0.014084507042253521,\
+    0.013888888888888888, 0.0136986301369863, 0.013513513513513514, 0.013333333333333334, 0.013157894736842105, 0.012987012987012988,\
+    0.01282051282051282, 0.012658227848101266, 0.0125, 0.012345679012345678, 0.012195121951219513, 0.012048192771084338,\
+    0.011904761904761904, 0.011764705882352941, 0.011627906976744186, 0.011494252873563218, 0.011363636363636364, 0.011235955056179775,\
+    0.011111111111111112, 0.01098901098901099, 0.010869565217391304, 0.010752688172043012, 0.010638297872340425, 0.010526315789473684,\
+    0.010416666666666666, 0.010309278350515464, 0.01020408163265306, 0.010101010101010102, 0.01, 0.009900990099009901,\
+    0.00980392156862745, 0.009708737864077669, 0.009615384615384616, 0.009523809523809525, 0.009433962264150943, 0.009345794392523364,\
+    0.009259259259259259, 0.009174311926605505, 0.00909090909090909, 0.009009009009009009, 0.008928571428571428, 0.008849557522123894,\
+    0.008771929824561403, 0.008695652173913044, 0.008620689655172414, 0.008547008547008548, 0.00847457627118644, 0.008403361344537815,\
+    0.008333333333333333, 0.008264462809917356, 0.00819672131147541, 0.008130081300813009, 0.008064516129032258, 0.008,\
+    0.007936507936507936, 0.007874015748031496, 0.0078125, 0.007751937984496124, 0.007692307692307693, 0.007633587786259542,\
+    0.007575757575757576, 0.007518796992481203, 0.007462686567164179, 0.007407407407407408, 0.007352941176470588, 0.0072992700729927005,\
+    0.007246376811594203, 0.007194244604316547, 0.007142857142857143, 0.0070921985815602835, 0.007042253521126761, 0.006993006993006993,\
+    0.006944444444444444, 0.006896551724137931, 0.00684931506849315, 0.006802721088435374, 0.006756756756756757, 0.006711409395973154,\
+    0.006666666666666667, 0.006622516556291391, 0.006578947368421052, 0.006535947712418301, 0.006493506493506494, 0.0064516129032258064,\
+    0.00641025641025641, 0.006369426751592357, 0.006329113924050633, 0.006289308176100629, 0.00625, 0.006211180124223602,\
+    0.006172839506172839, 0.006134969325153374, 0.006097560975609756, 0.006060606060606061, 0.006024096385542169, 0.005988023952095809,\
+    0.005952380952380952, 0.005917159763313609, 0.0058823529411764705, 0.005847953216374269, 0.005813953488372093, 0.005780346820809248,\
+    0.005747126436781609, 0.005714285714285714, 0.005681818181818182, 0.005649717514124294, 0.0056179775280898875, 0.00558659217877095,\
+    0.005555555555555556, 0.0055248618784530384, 0.005494505494505495, 0.00546448087431694, 0.005434782608695652, 0.005405405405405406,\
+    0.005376344086021506, 0.0053475935828877, 0.005319148936170213, 0.005291005291005291, 0.005263157894736842, 0.005235602094240838,\
+    0.005208333333333333, 0.0051813471502590676, 0.005154639175257732, 0.005128205128205128, 0.00510204081632653, 0.005076142131979695,\
+    0.005050505050505051, 0.005025125628140704, 0.005,
+#if defined(__CUDA_ARCH__)
+static __constant__ double plis_inv_k_tab[201] = {PLIS_INV_K_VALUES};
+#else
+static const double plis_inv_k_tab[201] = {PLIS_INV_K_VALUES};
+#endif
+
 #define PLIS_POISSON_BIG 1099511627776.0  // 2^40: returned for lambda >= 2^40 (counts overflow anyway)
 
 // Poisson(lam) for lam < 10 by inversion (sequential search from 0), given emlam = exp(-lam):
@@ -320,11 +364,13 @@ PLIS_HD double plis_poisson_small_d(plis_stream* st, double lam, double emlam) {
   double p = emlam;
   double F = p;
   double k = 0.0;
+  int ki = 0;
   while (u > F) {
     k += 1.0;
-    p = p * lam / k;
+    ki += 1;
+    p = (p * lam) * plis_inv_k_tab[ki];
     F += p;
-    if (p <= F * 8.673617379884035e-19 || k >= 200.0) break;  // tail below 2^-60: stop
+    if (p <= F * 8.673617379884035e-19 || ki >= 200) break;  // tail below 2^-60: stop
   }
   return k;
 }
@@ -334,17 +380,7 @@ PLIS_HD double plis_poisson_d(plis_stream* st, double lam) {
   if (lam >= PLIS_POISSON_BIG) return PLIS_POISSON_BIG;
   if (lam < 10.0) {
     // inversion by sequential search
-    double u = plis_uniform_d(st);
-    double p = plis_exp(-lam);
-    double F = p;
-    double k = 0.0;
-    while (u > F) {
-      k += 1.0;
-      p = p * lam / k;
-      F += p;
-      if (p <= F * 8.673617379884035e-19 || k >= 200.0) break;  // tail below 2^-60: stop
-    }
-    return k;
+    return plis_poisson_small_d(st, lam, plis_exp(-lam));
   }
   // PTRS, Hormann (1993)
   double slam = PLIS_SQRT(lam);
@@ -439,11 +475,13 @@ PLIS_HD double plis_poisson_small_f(plis_stream* st, float lam, float emlam) {
   float p = emlam;
   float F = p;
   float k = 0.0f;
+  int ki = 0;
   while (u > F) {
     k += 1.0f;
-    p = p * lam / k;
+    ki += 1;
+    p = (p * lam) * (float)plis_inv_k_tab[ki];
     F += p;
-    if (p <= F * 2.9802322e-08f || k >= 100.0f) break;  // tail below 2^-25
+    if (p <= F * 2.9802322e-08f || ki >= 100) break;  // tail below 2^-25
   }
   return (double)k;
 }
@@ -451,19 +489,7 @@ PLIS_HD double plis_poisson_small_f(plis_stream* st, float lam, float emlam) {
 // Returns the count as a double (exact integer), like plis_poisson_d.
 PLIS_HD double plis_poisson_f(plis_stream* st, float lam) {
   if (!(lam > 0.0f)) return 0.0;
-  if (lam < 10.0f) {
-    float u = plis_uniform_f(st);
-    float p = plis_expf(-lam);
-    float F = p;
-    float k = 0.0f;
-    while (u > F) {
-      k += 1.0f;
-      p = p * lam / k;
-      F += p;
-      if (p <= F * 2.9802322e-08f || k >= 100.0f) break;  // tail below 2^-25
-    }
-    return (double)k;
-  }
+  if (lam < 10.0f) return plis_poisson_small_f(st, lam, plis_expf(-lam));
   // lambda >= 10: the PTRS acceptance test compares ln-probabilities of size ~lambda*ln(lambda),
   // which binary32 cannot resolve (its spacing near 1e6 is 0.125), so it runs in binary64.
   return plis_poisson_d(st, (double)lam);
