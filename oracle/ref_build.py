@@ -4,6 +4,8 @@
 
 * refdump       the reference's header-only input parsers (PLISCuda/include/cpp/*.hpp) driven by
                 oracle/ref/refdump.cpp: g++ on the reference headers where they lie.
+* pliscuda_dropin the reference's main.cpp and parsers with pliscuda_b200/compat/run_simulation_shim.cpp
+                linked to libplis.so in place of driver.cu and its kernels.
 * pliscuda_test the reference's CUDA step (PLISCuda/src/*.cu + main.cpp) built with nvcc for sm_100a
   pliscuda      with -DTEST (fixed per-subvolume seeds, PLISCuda/src/init.cu:9-11) and without.
                 The reference makefile cannot be used as shipped (its -arch=sm_30 is gone from nvcc
@@ -57,10 +59,32 @@ def build_cuda(ref: str, test: bool) -> str:
     return out
 
 
+def build_dropin(ref: str) -> str:
+    """The reference's own main.cpp and parsers linked with pliscuda_b200/compat/run_simulation_shim.cpp
+    and libplis.so instead of driver.cu and the reference kernels: the literal drop-in."""
+    os.makedirs(OUT, exist_ok=True)
+    root = os.path.dirname(HERE)
+    out = os.path.join(OUT, "pliscuda_dropin")
+    obj_dir = os.path.join(OUT, "obj_dropin")
+    os.makedirs(obj_dir, exist_ok=True)
+    inc_cpp = os.path.join(ref, "PLISCuda", "include", "cpp")
+    main_o = os.path.join(obj_dir, "main.o")
+    _run(["nvcc", "-std=c++17", "-O2", "-arch=sm_100a", "-x", "cu", "-c",
+          os.path.join(ref, "PLISCuda", "src", "main.cpp"), "-o", main_o])
+    shim_o = os.path.join(obj_dir, "shim.o")
+    _run(["g++", "-std=c++17", "-O2", "-I", inc_cpp, "-I/usr/local/cuda/include", "-I", os.path.join(root, "include"),
+          "-c", os.path.join(root, "pliscuda_b200", "compat", "run_simulation_shim.cpp"), "-o", shim_o])
+    libdir = os.path.join(root, "pliscuda_b200")
+    _run(["nvcc", "-arch=sm_100a", main_o, shim_o, "-L" + libdir, "-lplis", "-Xlinker", "-rpath=$ORIGIN/../../pliscuda_b200",
+          "-o", out])
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
     ap.add_argument("--cuda", action="store_true", help="also build the reference CUDA binaries")
+    ap.add_argument("--dropin", action="store_true", help="also build main.cpp + the run_simulation shim")
     a = ap.parse_args(argv)
     if not os.path.isdir(a.reference):
         print("reference tree not present; nothing to build")
@@ -69,6 +93,8 @@ def main(argv=None):
     if a.cuda:
         print(build_cuda(a.reference, True))
         print(build_cuda(a.reference, False))
+    if a.dropin:
+        print(build_dropin(a.reference))
     return 0
 
 
