@@ -163,6 +163,19 @@ int plis_get_profile(plis_handle* h, plis_profile* out);
 /* Inspection: per-subvolume tau (binary64) and operation flags of the current state. */
 int plis_get_taus(plis_handle* h, double* tau, uint8_t* flags);
 
+/* Arg-min of a device array of n taus (first index on ties) into *d_min_tau / *d_argmin, enqueued
+ * on `stream` (a cudaStream_t, NULL for the default stream); the same global min-tau reduction the
+ * step does internally.  No counterpart in the reference: it exists for callers that cannot allocate
+ * device memory (a host whose own allocator owns the device memory, or a latency-critical loop in
+ * which cudaMalloc may synchronise the device).  It allocates nothing: inputs and outputs are the
+ * caller's device buffers, and its 16 KiB of per-CTA partials live in a fixed array inside the
+ * library, held on every device that loads the library until exit.  The first call on a device,
+ * made with that device current, looks up that array's device address; make it before any stream
+ * capture.  Calls share the array, so calls that overlap on the GPU race.  n must be in
+ * 1..PLIS_NOALLOC_MAX_TAUS, else PLIS_ERR_LIMIT. */
+#define PLIS_NOALLOC_MAX_TAUS 2147483647u
+int plis_tau_argmin_noalloc(const double* d_tau, uint64_t n, double* d_min_tau, int64_t* d_argmin, void* stream);
+
 /* Topology helpers (host only, no device needed).
  * plis_canonical_neighbours rewrites a 6-wide table so that each row lists its distinct non-self
  * neighbours first (lattice rows in the order -x,+x,-y,+y,-z,+z) followed by self padding; this is

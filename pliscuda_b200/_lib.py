@@ -83,6 +83,7 @@ def _load() -> ctypes.CDLL:
         "plis_get_stats": (i32, [vp, P(Stats)]),
         "plis_get_taus": (i32, [vp, vp, vp]),
         "plis_get_profile": (i32, [vp, P(Profile)]),
+        "plis_tau_argmin_noalloc": (i32, [vp, u64, vp, vp, vp]),
         "plis_canonical_neighbours": (i32, [u32, vp, vp, vp, vp]),
         "plis_config_load": (i32, [ctypes.c_char_p, P(vp)]),
         "plis_config_view_get": (i32, [vp, P(ConfigView)]),
