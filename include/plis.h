@@ -100,6 +100,7 @@ typedef struct plis_options {
   int32_t tile[3];            /* lattice brick per CTA (x, y, z), 0 = auto */
   int32_t persistent;         /* 1 = one cooperative persistent launch per run call, 0 = graph of phase kernels, -1 = auto */
   int32_t profile;            /* 1 = launch phase kernels one by one with CUDA events around each (plis_get_profile) */
+  int32_t stage_halo;         /* lattice leap: 1 = stage brick + halo in shared memory, 0 = global atomics (default) */
 } plis_options;
 
 /* Per-kernel device time accumulated while plis_options.profile is set (CUDA events recorded on the

@@ -77,6 +77,7 @@ void plis_options_init(plis_options* o) {
   o->max_rollbacks = 64;
   o->steps_per_launch = 0;
   o->persistent = -1;
+  o->stage_halo = 0;
 }
 
 int plis_create(const plis_model_desc* model, const plis_options* opts, plis_handle** out) {

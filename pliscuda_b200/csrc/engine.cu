@@ -187,6 +187,17 @@ int Engine::create(const Model& model, const plis_options& opt) {
   o.replica = opt.replica;
 
   launch_ = (opt.precision == PLIS_PREC_FP32) ? pick_f32(M.S) : pick_f64(M.S);
+  // shared-memory staging of the leap's brick + halo (lattices only, when the box fits)
+  g.staged = 0;
+  g.box_bytes = 0;
+  if (dm.lattice && opt.stage_halo) {
+    const size_t bytes = (size_t)(g.tx + 2) * (g.ty + 2) * (g.tz + 2) * M.S * sizeof(int32_t);
+    if (bytes <= 200u * 1024u) {
+      g.staged = 1;
+      g.box_bytes = (uint32_t)bytes;
+      if (bytes > 48u * 1024u) PLIS_CU(launch_.leap_smem((int)bytes));
+    }
+  }
   kernels_per_step_ = (opt.mode == PLIS_MODE_REFERENCE) ? 4 : 3;
   graph_steps_ = opt.steps_per_launch > 0 ? opt.steps_per_launch : 32;
   PLIS_CU(cudaDeviceSynchronize());

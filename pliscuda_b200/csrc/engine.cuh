@@ -95,6 +95,8 @@ struct Geo {
   uint32_t ntx, nty, ntz;  // bricks per dimension
   uint32_t nblocks;        // CTAs of the cell kernels
   uint32_t threads;        // threads per CTA
+  uint32_t staged;         // 1: the leap stages the brick + halo in shared memory
+  uint32_t box_bytes;      // dynamic shared memory of the staged leap
 };
 
 struct KArgs {

@@ -19,6 +19,7 @@ struct Launchers {
   void (*leap)(const KArgs&, dim3, dim3, cudaStream_t);
   void (*exact)(const KArgs&, dim3, dim3, cudaStream_t);
   void (*classify)(const KArgs&, dim3, dim3, cudaStream_t);
+  cudaError_t (*leap_smem)(int bytes);
 };
 
 class Engine {

@@ -237,6 +237,7 @@ __device__ __forceinline__ bool cell_of(const KArgs& A, uint32_t& c) {
 struct Nbr {
   uint32_t nb[6];
   uint8_t nn[6];
+  uint8_t dir[6];  // lattice direction of each slot: 0..5 = -x,+x,-y,+y,-z,+z
   int n;
 };
 
@@ -248,14 +249,14 @@ __device__ __forceinline__ void nbr_info(const DevModel& m, const Cell& cl, Nbr&
     const uint32_t X = m.X, Y = m.Y, Z = m.Z, XY = m.X * m.Y;
     const int ax = axis_count(cl.x, X), ay = axis_count(cl.y, Y), az = axis_count(cl.z, Z);
     int n = 0;
-    if (cl.x > 0) { q.nb[n] = c - 1; q.nn[n++] = (uint8_t)(axis_count(cl.x - 1, X) + ay + az); }
-    if (cl.x + 1 < X) { q.nb[n] = c + 1; q.nn[n++] = (uint8_t)(axis_count(cl.x + 1, X) + ay + az); }
-    if (cl.y > 0) { q.nb[n] = c - X; q.nn[n++] = (uint8_t)(ax + axis_count(cl.y - 1, Y) + az); }
-    if (cl.y + 1 < Y) { q.nb[n] = c + X; q.nn[n++] = (uint8_t)(ax + axis_count(cl.y + 1, Y) + az); }
-    if (cl.z > 0) { q.nb[n] = c - XY; q.nn[n++] = (uint8_t)(ax + ay + axis_count(cl.z - 1, Z)); }
-    if (cl.z + 1 < Z) { q.nb[n] = c + XY; q.nn[n++] = (uint8_t)(ax + ay + axis_count(cl.z + 1, Z)); }
+    if (cl.x > 0) { q.nb[n] = c - 1; q.dir[n] = 0; q.nn[n++] = (uint8_t)(axis_count(cl.x - 1, X) + ay + az); }
+    if (cl.x + 1 < X) { q.nb[n] = c + 1; q.dir[n] = 1; q.nn[n++] = (uint8_t)(axis_count(cl.x + 1, X) + ay + az); }
+    if (cl.y > 0) { q.nb[n] = c - X; q.dir[n] = 2; q.nn[n++] = (uint8_t)(ax + axis_count(cl.y - 1, Y) + az); }
+    if (cl.y + 1 < Y) { q.nb[n] = c + X; q.dir[n] = 3; q.nn[n++] = (uint8_t)(ax + axis_count(cl.y + 1, Y) + az); }
+    if (cl.z > 0) { q.nb[n] = c - XY; q.dir[n] = 4; q.nn[n++] = (uint8_t)(ax + ay + axis_count(cl.z - 1, Z)); }
+    if (cl.z + 1 < Z) { q.nb[n] = c + XY; q.dir[n] = 5; q.nn[n++] = (uint8_t)(ax + ay + axis_count(cl.z + 1, Z)); }
     q.n = n;
-    for (int j = n; j < 6; ++j) { q.nb[j] = c; q.nn[j] = 0; }
+    for (int j = n; j < 6; ++j) { q.nb[j] = c; q.nn[j] = 0; q.dir[j] = 0; }
     return;
   }
   q.n = m.ncount[c];
@@ -263,6 +264,7 @@ __device__ __forceinline__ void nbr_info(const DevModel& m, const Cell& cl, Nbr&
   for (int j = 0; j < 6; ++j) {
     q.nb[j] = m.canon[(size_t)c * 6 + j];
     q.nn[j] = j < q.n ? m.ncount[q.nb[j]] : 0;
+    q.dir[j] = 0;
   }
 }
 
@@ -590,27 +592,60 @@ __device__ __forceinline__ long long warp_sum(long long v) {
 #ifndef PLIS_LEAP_MIN_BLOCKS
 #define PLIS_LEAP_MIN_BLOCKS 4
 #endif
+// Shared-memory staging of one brick's leap: the brick plus a one-subvolume halo.  Every molecule a
+// subvolume of the brick keeps or sends is added into the box with shared-memory atomics; the box
+// is then flushed with one global reduction per touched subvolume, so global atomics only happen on
+// the brick's own subvolumes and its six faces.  Integer sums commute: results are unchanged.
+struct Box {
+  int32_t* acc;   // shared [S][bz][by][bx], or null when not staged (table topology / too large)
+  int bx, by, bz; // tx+2, ty+2, tz+2
+  int size;       // bx*by*bz
+};
+
+__device__ __forceinline__ int box_offset(const Box& b, int dir) {
+  switch (dir) {
+    case 0: return -1;
+    case 1: return 1;
+    case 2: return -b.bx;
+    case 3: return b.bx;
+    case 4: return -b.bx * b.by;
+    default: return b.bx * b.by;
+  }
+}
+
+struct LeapCtx {
+  const int32_t* Xc;
+  int32_t* Xt;
+  uint8_t* flag;
+  uint64_t step;
+  uint32_t attempt;
+};
+
+// Leap of one brick (or one 1-D block of a table topology) by the whole CTA; returns this thread's
+// events and guard flag.  leap_step, leap.cu:3-65.
 template <typename Real, int MAXS>
-__global__ void __launch_bounds__(256, PLIS_LEAP_MIN_BLOCKS) k_leap(KArgs A) {
-  Ctrl* K = A.b.ctrl;
-  if (K->done) return;
+__device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const LeapCtx& L, Real tl, const Box& box,
+                                          long long& ev, int& big) {
   const DevModel& m = A.m;
   const int mode = A.o.mode, nc = A.o.nc;
-  const int32_t* Xc = A.b.X[K->cur];
-  int32_t* Xt = A.b.X[K->tgt];
-  uint8_t* flag = A.b.flag[K->tf];
-  const uint64_t step = K->step + 1;
-  const uint32_t attempt = K->attempt;
-  const Real tl = (Real)K->tau_leap;
-  __shared__ long long s_ev[32];
-  __shared__ int s_big;
-  if (threadIdx.x == 0) s_big = 0;
-  __syncthreads();
+  const int32_t* Xc = L.Xc;
+  int32_t* Xt = L.Xt;
+  uint8_t* flag = L.flag;
+  const uint64_t step = L.step;
+  const uint32_t attempt = L.attempt;
   Cell cl;
-  const bool valid = cell_of(A, blockIdx.x, cl);
+  const bool valid = cell_of(A, tile, cl);
   const uint32_t c = cl.c;
-  long long ev = 0;
-  int big = 0;
+  int own = 0;
+  if (box.acc) {
+    for (int i = threadIdx.x; i < box.size * (int)m.S; i += blockDim.x) box.acc[i] = 0;
+    const uint32_t t = threadIdx.x;
+    const int lx = (int)(t % A.g.tx), ly = (int)((t / A.g.tx) % A.g.ty), lz = (int)(t / (A.g.tx * A.g.ty));
+    own = (lx + 1) + box.bx * ((ly + 1) + box.by * (lz + 1));
+    __syncthreads();
+  }
+  ev = 0;
+  big = 0;
   if (valid) {
     Counts<MAXS> x;
     load_counts(m, Xc, c, x);
@@ -667,7 +702,6 @@ __global__ void __launch_bounds__(256, PLIS_LEAP_MIN_BLOCKS) k_leap(KArgs A) {
       Nbr q;
       nbr_info(m, cl, q);
       const int n = q.n;
-      const uint32_t* nb = q.nb;
       bool mark = false;
       for (int s = 0; s < S; ++s) {
         const int32_t xs = x.get(s);
@@ -682,8 +716,9 @@ __global__ void __launch_bounds__(256, PLIS_LEAP_MIN_BLOCKS) k_leap(KArgs A) {
           const long long k = kd[j];
           if (k >= kBigJump) big = 1;
           if (k > 0) {
-            atomicAdd(&Xt[(size_t)s * m.Npad + nb[j]], (int)k);
-            if (mode == 1 && flag[nb[j]] == F_SSA_FF) flag[nb[j]] = F_SSA;
+            if (box.acc) atomicAdd_block(&box.acc[s * box.size + own + box_offset(box, q.dir[j])], (int)k);
+            else atomicAdd(&Xt[(size_t)s * m.Npad + q.nb[j]], (int)k);
+            if (mode == 1 && flag[q.nb[j]] == F_SSA_FF) flag[q.nb[j]] = F_SSA;
           }
           out += k;
         }
@@ -692,7 +727,7 @@ __global__ void __launch_bounds__(256, PLIS_LEAP_MIN_BLOCKS) k_leap(KArgs A) {
       }
       if (mark) {  // leap.cu:54-56: every receiver leaves fast-forward
         for (int j = 0; j < n; ++j)
-          if (flag[nb[j]] == F_SSA_FF) flag[nb[j]] = F_SSA;
+          if (flag[q.nb[j]] == F_SSA_FF) flag[q.nb[j]] = F_SSA;
       }
     }
 #pragma unroll
@@ -700,10 +735,71 @@ __global__ void __launch_bounds__(256, PLIS_LEAP_MIN_BLOCKS) k_leap(KArgs A) {
       if (s < (int)m.S) {
         const long long tv = (long long)x.v[s] + dl.v[s];
         if (tv >= kBigTile || tv <= -kBigTile) big = 1;
-        atomicAdd(&Xt[(size_t)s * m.Npad + c], (int)tv);
+        if (box.acc) atomicAdd_block(&box.acc[s * box.size + own], (int)tv);
+        else atomicAdd(&Xt[(size_t)s * m.Npad + c], (int)tv);
       }
     }
   }
+  if (box.acc) {  // flush the box: each subvolume's own entry, then the six halo faces
+    __syncthreads();
+    if (valid) {
+      for (int s = 0; s < (int)m.S; ++s) {
+        const int32_t v = box.acc[s * box.size + own];
+        if (v) atomicAdd(&Xt[(size_t)s * m.Npad + c], v);
+      }
+    }
+    const uint32_t tx = A.g.tx, ty = A.g.ty, tz = A.g.tz;
+    const uint32_t b = tile;
+    const uint32_t bxi = b % A.g.ntx, br = b / A.g.ntx;
+    const uint32_t byi = br % A.g.nty, bzi = br / A.g.nty;
+    const int x0 = (int)(bxi * tx), y0 = (int)(byi * ty), z0 = (int)(bzi * tz);
+    // face f: 0/1 = x-/x+ (ty*tz entries), 2/3 = y-/y+ (tx*tz), 4/5 = z-/z+ (tx*ty)
+    const int fsz[3] = {(int)(ty * tz), (int)(tx * tz), (int)(tx * ty)};
+    const int total = 2 * (fsz[0] + fsz[1] + fsz[2]);
+    for (int w = threadIdx.x; w < total; w += blockDim.x) {
+      int f = 0, i = w;
+      while (i >= fsz[f >> 1]) { i -= fsz[f >> 1]; ++f; }
+      int lx, ly, lz;  // box-relative coordinates (-1 .. t)
+      if (f < 2) { ly = i % (int)ty; lz = i / (int)ty; lx = (f == 0) ? -1 : (int)tx; }
+      else if (f < 4) { lx = i % (int)tx; lz = i / (int)tx; ly = (f == 2) ? -1 : (int)ty; }
+      else { lx = i % (int)tx; ly = i / (int)tx; lz = (f == 4) ? -1 : (int)tz; }
+      const int gx = x0 + lx, gy = y0 + ly, gz = z0 + lz;
+      if (gx < 0 || gy < 0 || gz < 0 || gx >= (int)m.X || gy >= (int)m.Y || gz >= (int)m.Z) continue;
+      const int p = (lx + 1) + box.bx * ((ly + 1) + box.by * (lz + 1));
+      const uint32_t g = (uint32_t)gx + m.X * ((uint32_t)gy + m.Y * (uint32_t)gz);
+      for (int s = 0; s < (int)m.S; ++s) {
+        const int32_t v = box.acc[s * box.size + p];
+        if (v) atomicAdd(&Xt[(size_t)s * m.Npad + g], v);
+      }
+    }
+  }
+}
+
+template <typename Real, int MAXS>
+__global__ void __launch_bounds__(256, PLIS_LEAP_MIN_BLOCKS) k_leap(KArgs A) {
+  Ctrl* K = A.b.ctrl;
+  if (K->done) return;
+  extern __shared__ int32_t s_box[];
+  __shared__ long long s_ev[32];
+  __shared__ int s_big;
+  if (threadIdx.x == 0) s_big = 0;
+  LeapCtx L;
+  L.Xc = A.b.X[K->cur];
+  L.Xt = A.b.X[K->tgt];
+  L.flag = A.b.flag[K->tf];
+  L.step = K->step + 1;
+  L.attempt = K->attempt;
+  const Real tl = (Real)K->tau_leap;
+  Box box;
+  box.acc = A.g.staged ? s_box : nullptr;
+  box.bx = (int)A.g.tx + 2;
+  box.by = (int)A.g.ty + 2;
+  box.bz = (int)A.g.tz + 2;
+  box.size = box.bx * box.by * box.bz;
+  __syncthreads();
+  long long ev;
+  int big;
+  leap_tile<Real, MAXS>(A, blockIdx.x, L, tl, box, ev, big);
   // events and guard flags of the CTA
   ev = warp_sum(ev);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -954,53 +1050,73 @@ __global__ void __launch_bounds__(256) k_apply(KArgs A) {
 #endif
 
 // ------------------------------------------------------------------------------------------------
-// k_classify + last-CTA control
+// classification phase + last-CTA control
 // ------------------------------------------------------------------------------------------------
-template <typename Real, int MAXS>
-__global__ void __launch_bounds__(256) k_classify(KArgs A) {
-  Ctrl* K = A.b.ctrl;
-  if (K->done) return;
-  const DevModel& m = A.m;
-  const uint32_t phase = K->phase;
-  const int32_t* Xe = A.b.X[phase == 0 ? K->cur : K->tgt];
-  int32_t* Xz = A.b.X[K->spare];
-  const uint32_t tf = K->tf;
-  const double* tau_cur = A.b.tau[tf];
-  double* tau_new = A.b.tau[tf ^ 1u];
-  const uint8_t* flag_cur = A.b.flag[tf];
-  uint8_t* flag_new = A.b.flag[tf ^ 1u];
-  const uint64_t step = phase == 0 ? 0 : K->step + 1;
-  const uint32_t attempt = phase == 0 ? 0 : K->attempt;
-  const double ff = K->dt;
+struct ClassifyCtx {
+  const int32_t* Xe;      // counts to classify (post-step, or the initial state)
+  int32_t* Xz;            // buffer the next leap reduces into: zeroed here
+  const double* tau_cur;
+  double* tau_new;
+  const uint8_t* flag_cur;
+  uint8_t* flag_new;
+  uint64_t step;
+  uint32_t attempt;
+  double ff;              // fast-forward decrement
+};
 
+__device__ __forceinline__ ClassifyCtx classify_ctx(const KArgs& A, const Ctrl* K) {
+  ClassifyCtx C;
+  const uint32_t phase = K->phase;
+  C.Xe = A.b.X[phase == 0 ? K->cur : K->tgt];
+  C.Xz = A.b.X[K->spare];
+  const uint32_t tf = K->tf;
+  C.tau_cur = A.b.tau[tf];
+  C.tau_new = A.b.tau[tf ^ 1u];
+  C.flag_cur = A.b.flag[tf];
+  C.flag_new = A.b.flag[tf ^ 1u];
+  C.step = phase == 0 ? 0 : K->step + 1;
+  C.attempt = phase == 0 ? 0 : K->attempt;
+  C.ff = K->dt;
+  return C;
+}
+
+// One thread's subvolume of one brick: negativity check, zeroing of the next target, classification.
+template <typename Real, int MAXS>
+__device__ __forceinline__ void classify_tile(const KArgs& A, uint32_t tile, const ClassifyCtx& C, double& tn,
+                                              long long& ti, int& fl, int& bad, bool& valid) {
+  const DevModel& m = A.m;
+  Cell cl;
+  valid = cell_of(A, tile, cl);
+  const uint32_t c = cl.c;
+  tn = PLIS_INF_D;
+  ti = 0x7FFFFFFFFFFFFFFFll;
+  fl = F_SSA_FF;
+  bad = 0;
+  if (!valid) return;
+  Counts<MAXS> x;
+  load_counts(m, C.Xe, c, x);
+#pragma unroll
+  for (int s = 0; s < MAXS; ++s)
+    if (s < (int)m.S) {
+      if (x.v[s] < 0) bad = 1;
+      C.Xz[(size_t)s * m.Npad + c] = 0;
+    }
+  Nbr q;
+  nbr_info(m, cl, q);
+  classify_cell<Real>(A, c, q, x, C.Xe, C.tau_cur[c], C.flag_cur[c], C.step, C.attempt, C.ff, tn, fl);
+  C.tau_new[c] = tn;
+  C.flag_new[c] = (uint8_t)fl;
+  ti = c;
+}
+
+// CTA reduction of one brick into slot `slot` (min tau with arg-min, #LEAP_CR, negative flag), then
+// the count of finished bricks; true in the CTA that finished last of `nslots`.
+__device__ __forceinline__ bool classify_slot(const KArgs& A, Ctrl* K, uint32_t slot, uint32_t nslots, double tn,
+                                              long long ti, bool is_cr, int bad) {
   __shared__ double s_t[32];
   __shared__ long long s_i[32];
   __shared__ bool s_last;
-
-  Cell cl;
-  const bool valid = cell_of(A, blockIdx.x, cl);
-  const uint32_t c = cl.c;
-  double tn = PLIS_INF_D;
-  long long ti = 0x7FFFFFFFFFFFFFFFll;
-  int fl = F_SSA_FF;
-  int bad = 0;
-  if (valid) {
-    Counts<MAXS> x;
-    load_counts(m, Xe, c, x);
-#pragma unroll
-    for (int s = 0; s < MAXS; ++s)
-      if (s < (int)m.S) {
-        if (x.v[s] < 0) bad = 1;
-        Xz[(size_t)s * m.Npad + c] = 0;
-      }
-    Nbr q;
-    nbr_info(m, cl, q);
-    classify_cell<Real>(A, c, q, x, Xe, tau_cur[c], flag_cur[c], step, attempt, ff, tn, fl);
-    tau_new[c] = tn;
-    flag_new[c] = (uint8_t)fl;
-    ti = c;
-  }
-  const int ncr = __syncthreads_count(valid && fl == F_LEAP_CR);
+  const int ncr = __syncthreads_count(is_cr);
   const int nbad = __syncthreads_or(bad);
   warp_min_pair(tn, ti);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -1011,26 +1127,34 @@ __global__ void __launch_bounds__(256) k_classify(KArgs A) {
     double bt = s_t[0];
     long long bi = s_i[0];
     for (int w = 1; w < nw; ++w) min_pair(bt, bi, s_t[w], s_i[w]);
-    A.b.slot_tau[blockIdx.x] = bt;
-    A.b.slot_idx[blockIdx.x] = bi;
-    A.b.slot_cr[blockIdx.x] = (uint32_t)ncr;
-    A.b.slot_bad[blockIdx.x] = nbad ? 1u : 0u;
+    A.b.slot_tau[slot] = bt;
+    A.b.slot_idx[slot] = bi;
+    A.b.slot_cr[slot] = (uint32_t)ncr;
+    A.b.slot_bad[slot] = nbad ? 1u : 0u;
     __threadfence();
     const uint32_t prev = atomicAdd(&K->blocks_done, 1u);
-    s_last = ((prev & 0x7FFFFFFFu) == gridDim.x - 1);
+    s_last = ((prev & 0x7FFFFFFFu) == nslots - 1);
   }
   __syncthreads();
-  if (!s_last) return;
+  return s_last;
+}
 
-  // ---- last CTA: grid-wide arg-min and the step decision ----
-  // every thread loads a strided share of the per-CTA slots (independent L2 loads in flight),
-  // then warp shuffles and one more pass over the warp results
+// The whole last CTA: reduce the `nslots` slots (independent L2 loads spread over the block), then
+// one thread takes the step decision (driver.cu:267-334): rollback or accept, time, the next plan.
+__device__ __forceinline__ void classify_control(const KArgs& A, Ctrl* K, uint32_t nslots) {
+  __shared__ double s_t[32];
+  __shared__ long long s_i[32];
+  __shared__ unsigned long long s_cr[32];
+  __shared__ uint32_t s_bad[32];
   __threadfence();
+  const uint32_t phase = K->phase;
+  const uint32_t tf = K->tf;
+  const uint8_t* flag_new = A.b.flag[tf ^ 1u];
   double gt = PLIS_INF_D;
   long long gi = 0x7FFFFFFFFFFFFFFFll;
   unsigned long long gcr = 0;
   uint32_t gbad = 0;
-  for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+  for (uint32_t b = threadIdx.x; b < nslots; b += blockDim.x) {
     min_pair(gt, gi, __ldcg(&A.b.slot_tau[b]), __ldcg(&A.b.slot_idx[b]));
     gcr += __ldcg(&A.b.slot_cr[b]);
     gbad |= __ldcg(&A.b.slot_bad[b]);
@@ -1038,12 +1162,10 @@ __global__ void __launch_bounds__(256) k_classify(KArgs A) {
   warp_min_pair(gt, gi);
   gcr = (unsigned long long)warp_sum((long long)gcr);
   gbad = __reduce_or_sync(0xffffffffu, gbad);
-  __shared__ unsigned long long s_cr[32];
-  __shared__ uint32_t s_bad[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   if (lane == 0) { s_t[wid] = gt; s_i[wid] = gi; s_cr[wid] = gcr; s_bad[wid] = gbad; }
   __syncthreads();
-  if (wid != 0) return;
-  {
+  if (wid == 0) {
     const int nw = (blockDim.x + 31) >> 5;
     gt = lane < nw ? s_t[lane] : PLIS_INF_D;
     gi = lane < nw ? s_i[lane] : 0x7FFFFFFFFFFFFFFFll;
@@ -1053,53 +1175,66 @@ __global__ void __launch_bounds__(256) k_classify(KArgs A) {
     gcr = (unsigned long long)warp_sum((long long)gcr);
     gbad = __reduce_or_sync(0xffffffffu, gbad);
   }
-  if (lane != 0) return;
-  const int mode = A.o.mode;
-  const uint32_t leap_bad = (__ldcg(&K->blocks_done) & 0x80000000u) ? 1u : 0u;
-  K->blocks_done = 0;
-  if (gi == 0x7FFFFFFFFFFFFFFFll) gi = -1;
-  if (phase == 0) {
-    K->tau_min = gt;
-    K->argmin = gi;
-    K->n_leap_cr = (uint32_t)gcr;
-    K->argmin_flag = gi >= 0 ? __ldcg(&flag_new[gi]) : F_SSA_FF;
-    K->tf = tf ^ 1u;
-    K->phase = 1;
-    K->done = 1;  // idle until a run call
-    return;
-  }
-  if (gbad || leap_bad) {  // check_state + revert (leap.cu:203-212, driver.cu:292-315)
-    K->attempt += 1;
-    if ((int)K->attempt > A.o.max_rollbacks) {
-      K->status = PLIS_ERR_STUCK;
-      K->stop_reason = PLIS_STOP_ERROR;
-      K->done = 1;
-      return;
+  if (threadIdx.x == 0) {
+    const int mode = A.o.mode;
+    const uint32_t leap_bad = (__ldcg(&K->blocks_done) & 0x80000000u) ? 1u : 0u;
+    K->blocks_done = 0;
+    if (gi == 0x7FFFFFFFFFFFFFFFll) gi = -1;
+    if (phase == 0) {
+      K->tau_min = gt;
+      K->argmin = gi;
+      K->n_leap_cr = (uint32_t)gcr;
+      K->argmin_flag = gi >= 0 ? __ldcg(&flag_new[gi]) : F_SSA_FF;
+      K->tf = tf ^ 1u;
+      K->phase = 1;
+      K->done = 1;  // idle until a run call
+    } else if (gbad || leap_bad) {  // check_state + revert (leap.cu:203-212, driver.cu:292-315)
+      K->attempt += 1;
+      if ((int)K->attempt > A.o.max_rollbacks) {
+        K->status = PLIS_ERR_STUCK;
+        K->stop_reason = PLIS_STOP_ERROR;
+        K->done = 1;
+      } else {
+        const uint32_t t = K->tgt;
+        K->tgt = K->spare;
+        K->spare = t;
+        set_attempt(K, mode);
+      }
+    } else {
+      // accept: swap state (driver.cu:320-323) by rotating buffer indices
+      K->t = K->t + K->dt;
+      K->step = K->step + 1;
+      K->events += K->ev_attempt;
+      K->exact_events += K->ex_attempt;
+      K->rollbacks += K->attempt;
+      K->last_tau = K->tau_min;
+      K->last_argmin = K->argmin;
+      const uint32_t oc = K->cur;
+      K->cur = K->tgt;
+      K->tgt = K->spare;
+      K->spare = oc;
+      K->tf = tf ^ 1u;
+      K->tau_min = gt;
+      K->argmin = gi;
+      K->n_leap_cr = (uint32_t)gcr;
+      K->argmin_flag = gi >= 0 ? __ldcg(&flag_new[gi]) : F_SSA_FF;
+      prepare_step(K, mode);
     }
-    const uint32_t t = K->tgt;
-    K->tgt = K->spare;
-    K->spare = t;
-    set_attempt(K, mode);
-    return;
   }
-  // accept: swap state (driver.cu:320-323) by rotating buffer indices
-  K->t = K->t + K->dt;
-  K->step = K->step + 1;
-  K->events += K->ev_attempt;
-  K->exact_events += K->ex_attempt;
-  K->rollbacks += K->attempt;
-  K->last_tau = K->tau_min;
-  K->last_argmin = K->argmin;
-  const uint32_t oc = K->cur;
-  K->cur = K->tgt;
-  K->tgt = K->spare;
-  K->spare = oc;
-  K->tf = tf ^ 1u;
-  K->tau_min = gt;
-  K->argmin = gi;
-  K->n_leap_cr = (uint32_t)gcr;
-  K->argmin_flag = gi >= 0 ? __ldcg(&flag_new[gi]) : F_SSA_FF;
-  prepare_step(K, mode);
+}
+
+template <typename Real, int MAXS>
+__global__ void __launch_bounds__(256) k_classify(KArgs A) {
+  Ctrl* K = A.b.ctrl;
+  if (K->done) return;
+  const ClassifyCtx C = classify_ctx(A, K);
+  double tn;
+  long long ti;
+  int fl, bad;
+  bool valid;
+  classify_tile<Real, MAXS>(A, blockIdx.x, C, tn, ti, fl, bad, valid);
+  if (classify_slot(A, K, blockIdx.x, gridDim.x, tn, ti, valid && fl == F_LEAP_CR, bad))
+    classify_control(A, K, gridDim.x);
 }
 
 #ifdef PLIS_ENGINE_HOST_TU
@@ -1112,21 +1247,24 @@ __global__ void k_fill_tau(double* t, uint8_t* f, uint32_t n) {
 // kernel launchers of each (precision, species capacity)
 template <typename Real, int MAXS>
 struct KernelSet {
-  static void leap(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) { k_leap<Real, MAXS><<<g, b, 0, s>>>(a); }
+  static void leap(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) { k_leap<Real, MAXS><<<g, b, a.g.box_bytes, s>>>(a); }
+  static cudaError_t leap_smem(int bytes) {
+    return cudaFuncSetAttribute(k_leap<Real, MAXS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  }
   static void exact(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) { k_exact<Real, MAXS><<<g, b, 0, s>>>(a); }
   static void classify(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) { k_classify<Real, MAXS><<<g, b, 0, s>>>(a); }
 };
 
 template <typename Real>
 Launchers pick_impl(uint32_t S) {
-  if (S <= 1) return {KernelSet<Real, 1>::leap, KernelSet<Real, 1>::exact, KernelSet<Real, 1>::classify};
-  if (S <= 2) return {KernelSet<Real, 2>::leap, KernelSet<Real, 2>::exact, KernelSet<Real, 2>::classify};
-  if (S <= 4) return {KernelSet<Real, 4>::leap, KernelSet<Real, 4>::exact, KernelSet<Real, 4>::classify};
-  if (S <= 8) return {KernelSet<Real, 8>::leap, KernelSet<Real, 8>::exact, KernelSet<Real, 8>::classify};
-  if (S <= 16) return {KernelSet<Real, 16>::leap, KernelSet<Real, 16>::exact, KernelSet<Real, 16>::classify};
-  if (S <= 32) return {KernelSet<Real, 32>::leap, KernelSet<Real, 32>::exact, KernelSet<Real, 32>::classify};
-  if (S <= 64) return {KernelSet<Real, 64>::leap, KernelSet<Real, 64>::exact, KernelSet<Real, 64>::classify};
-  return {KernelSet<Real, 256>::leap, KernelSet<Real, 256>::exact, KernelSet<Real, 256>::classify};
+  if (S <= 1) return {KernelSet<Real, 1>::leap, KernelSet<Real, 1>::exact, KernelSet<Real, 1>::classify, KernelSet<Real, 1>::leap_smem};
+  if (S <= 2) return {KernelSet<Real, 2>::leap, KernelSet<Real, 2>::exact, KernelSet<Real, 2>::classify, KernelSet<Real, 2>::leap_smem};
+  if (S <= 4) return {KernelSet<Real, 4>::leap, KernelSet<Real, 4>::exact, KernelSet<Real, 4>::classify, KernelSet<Real, 4>::leap_smem};
+  if (S <= 8) return {KernelSet<Real, 8>::leap, KernelSet<Real, 8>::exact, KernelSet<Real, 8>::classify, KernelSet<Real, 8>::leap_smem};
+  if (S <= 16) return {KernelSet<Real, 16>::leap, KernelSet<Real, 16>::exact, KernelSet<Real, 16>::classify, KernelSet<Real, 16>::leap_smem};
+  if (S <= 32) return {KernelSet<Real, 32>::leap, KernelSet<Real, 32>::exact, KernelSet<Real, 32>::classify, KernelSet<Real, 32>::leap_smem};
+  if (S <= 64) return {KernelSet<Real, 64>::leap, KernelSet<Real, 64>::exact, KernelSet<Real, 64>::classify, KernelSet<Real, 64>::leap_smem};
+  return {KernelSet<Real, 256>::leap, KernelSet<Real, 256>::exact, KernelSet<Real, 256>::classify, KernelSet<Real, 256>::leap_smem};
 }
 
 
