@@ -186,6 +186,51 @@ int plis_canonical_neighbours(uint32_t n, const uint32_t* table, const uint32_t 
                               uint32_t* canonical, uint32_t lattice_out[3]);
 
 /* ---------------------------------------------------------------------------------------------
+ * Batches: many independent replicas of one reaction network, each on its own reflective lattice
+ * (uneven sizes) with its own rate constants and its own random stream, advanced together by one
+ * persistent cooperative kernel.  The reference can only emulate this by concatenating disjoint
+ * topologies into one model, which couples them through its single global min-tau.  Replica r of a
+ * batch follows exactly the trajectory of plis_create with options.replica = replica_ids[r].
+ * ------------------------------------------------------------------------------------------- */
+typedef struct plis_batch_desc {
+  uint32_t n_replicas;        /* 1..4096 */
+  uint32_t n_species;         /* S <= 16 */
+  uint32_t n_reactions;       /* R */
+  const int32_t* reactants;   /* [S*R] species-major, shared by all replicas */
+  const int32_t* products;    /* [S*R] */
+  const uint32_t* lattice;    /* [n_replicas*3] X, Y, Z of each replica */
+  const double* reaction_rates;  /* [n_replicas*R] */
+  const double* diffusion_rates; /* [n_replicas*S] */
+  const uint32_t* replica_ids;   /* [n_replicas] stream key of each replica, NULL = 0..n-1 */
+} plis_batch_desc;
+
+typedef struct plis_batch_tuning {
+  int32_t tile[3];            /* brick shape of the bricks CTAs take from the work queue */
+  int32_t blocks_per_sm;      /* co-resident CTAs per SM of the persistent launch */
+  int32_t grid;               /* CTAs of the persistent launch */
+  double events_per_s;        /* measured by plis_batch_autotune (0 if not tuned) */
+} plis_batch_tuning;
+
+typedef struct plis_batch plis_batch;
+
+int plis_batch_create(const plis_batch_desc* desc, const plis_options* opts, plis_batch** out);
+int plis_batch_destroy(plis_batch* b);
+/* counts [S*N_r] species-major for replica r; resets that replica's time and statistics */
+int plis_batch_set_state(plis_batch* b, uint32_t replica, const uint32_t* counts);
+int plis_batch_get_state(plis_batch* b, uint32_t replica, uint32_t* counts);
+int plis_batch_get_taus(plis_batch* b, uint32_t replica, double* tau, uint8_t* flags);
+/* every replica until its time >= t_end (reference mode) / lands on t_end (corrected mode) */
+int plis_batch_run(plis_batch* b, double t_end);
+/* every replica at most n_steps accepted steps */
+int plis_batch_step(plis_batch* b, uint64_t n_steps);
+int plis_batch_get_stats(plis_batch* b, uint32_t replica, plis_stats* out);
+/* Time pilot_steps steps of the current state for each candidate brick shape, keep the fastest,
+ * restore the state.  The CTAs take bricks (and with them replicas) from a shared work queue, so
+ * the number of replicas per CTA adapts to their sizes at run time. */
+int plis_batch_autotune(plis_batch* b, uint64_t pilot_steps, plis_batch_tuning* out);
+int plis_batch_get_tuning(plis_batch* b, plis_batch_tuning* out);
+
+/* ---------------------------------------------------------------------------------------------
  * Input files in the reference's formats, read unchanged (Configuration.hpp:27-144,
  * Topology.hpp:98-191, State.hpp:112-217, Reactions.hpp:132-223, cpp_utils.hpp:29-56).
  * ------------------------------------------------------------------------------------------- */

@@ -54,6 +54,15 @@ class Stats(ctypes.Structure):
                 ("device_ms", f64), ("kernel_launches", u64)]
 
 
+class BatchDesc(ctypes.Structure):
+    _fields_ = [("n_replicas", u32), ("n_species", u32), ("n_reactions", u32), ("reactants", vp), ("products", vp),
+                ("lattice", vp), ("reaction_rates", vp), ("diffusion_rates", vp), ("replica_ids", vp)]
+
+
+class BatchTuning(ctypes.Structure):
+    _fields_ = [("tile", i32 * 3), ("blocks_per_sm", i32), ("grid", i32), ("events_per_s", f64)]
+
+
 class ConfigView(ctypes.Structure):
     _fields_ = [("model", ModelDesc), ("initial_state", vp), ("end_time", f64), ("log_freq", f64)]
 
@@ -85,6 +94,16 @@ def _load() -> ctypes.CDLL:
         "plis_get_taus": (i32, [vp, vp, vp]),
         "plis_get_profile": (i32, [vp, P(Profile)]),
         "plis_tau_argmin_noalloc": (i32, [vp, u64, vp, vp, vp]),
+        "plis_batch_create": (i32, [P(BatchDesc), P(Options), P(vp)]),
+        "plis_batch_destroy": (i32, [vp]),
+        "plis_batch_set_state": (i32, [vp, u32, vp]),
+        "plis_batch_get_state": (i32, [vp, u32, vp]),
+        "plis_batch_get_taus": (i32, [vp, u32, vp, vp]),
+        "plis_batch_run": (i32, [vp, f64]),
+        "plis_batch_step": (i32, [vp, u64]),
+        "plis_batch_get_stats": (i32, [vp, u32, P(Stats)]),
+        "plis_batch_autotune": (i32, [vp, u64, P(BatchTuning)]),
+        "plis_batch_get_tuning": (i32, [vp, P(BatchTuning)]),
         "plis_canonical_neighbours": (i32, [u32, vp, vp, vp, vp]),
         "plis_config_load": (i32, [ctypes.c_char_p, P(vp)]),
         "plis_config_view_get": (i32, [vp, P(ConfigView)]),

@@ -1,0 +1,358 @@
+// batch_kernels.cuh — many independent replicas advanced by one persistent cooperative kernel.
+//
+// A batch holds replicas of one reaction network with their own reflective lattice (uneven sizes),
+// their own rate constants (parameter sets) and their own random stream (replica id in the key).
+// Every replica is a segment of the concatenated state arrays and is cut into bricks.  One
+// cooperative launch loops over global iterations; in each, every replica that is not done takes
+// one step of the single-replica algorithm (engine_kernels.cuh):
+//
+//   plan      every CTA scans the replicas' control blocks (identical result in every CTA): prefix sums
+//             of the bricks still leaping / classifying, and whether any replica has exact events due
+//   leap      CTAs take bricks from an atomic work counter (dynamic balance over uneven replicas)
+//   ...       grid barrier; exact events and their deltas when due (two more barriers)
+//   classify  bricks again; the last brick of a replica to finish takes that replica's decision
+//             (rollback or accept, time, next plan): replicas never wait for each other
+//   barrier
+//
+// Grid barriers spin on a generation counter with an iteration limit: a barrier that gives up sets
+// an error word, every CTA leaves the loop, and the host reports PLIS_ERR_TIMEOUT.  The launch is
+// cooperative, so all CTAs are co-resident.
+#ifndef PLIS_BATCH_KERNELS_CUH_
+#define PLIS_BATCH_KERNELS_CUH_
+
+#include "batch.h"
+#include "engine_kernels.cuh"
+
+namespace plis {
+
+constexpr int kMaxBatchReplicas = 4096;
+
+struct RepDesc {
+  uint32_t X, Y, Z, N;
+  uint32_t coff;       // first subvolume of the replica in the concatenated arrays (multiple of 32)
+  uint32_t tile_off;   // first brick of the replica in the global brick numbering
+  uint32_t ntx, nty, ntz, ntiles;
+  uint32_t replica_id; // stream key
+};
+
+struct BatchArgs {
+  DevModel m;          // shared reaction tables; Npad = species stride of the concatenated arrays
+  DevOpts o;
+  Geo g;               // brick shape (tx, ty, tz, threads); per-replica brick counts in RepDesc
+  const KArgs* views;  // [nrep] the single-replica argument block of every replica (read-only)
+  const RepDesc* rep;
+  uint32_t nrep;
+  uint32_t rs, ss;     // rate-table strides per replica (R, S)
+  const void* rr;      // Real [nrep][R]
+  const void* dr;      // Real [nrep][S]
+  Ctrl* ctrl;          // [nrep]
+  int32_t* X[3];
+  double* tau[2];
+  uint8_t* flag[2];
+  int32_t* D;
+  double* slot_tau;    // per brick
+  long long* slot_idx;
+  uint32_t* slot_cr;
+  uint32_t* slot_bad;
+  unsigned* work;      // [4 phases][3 generations] brick / replica counters
+  unsigned* bar;       // grid barrier: [0] arrivals, [1] generation
+  int* err;            // 1 = a barrier timed out
+  unsigned long long spin_limit;
+  uint32_t max_iters;  // global iterations per launch
+};
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Grid-wide barrier of a cooperative launch (the arrive / spin pattern of a grid sync) whose spin
+// gives up after spin_limit polls, setting *err; returns false then.
+__device__ __forceinline__ bool grid_barrier(const BatchArgs& B) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned* count = B.bar;
+    volatile unsigned* gen = B.bar + 1;
+    const unsigned g = *gen;
+    __threadfence();
+    int ok = 1;
+    if (atomicAdd(count, 1u) + 1u == gridDim.x) {
+      atomicExch(count, 0u);
+      __threadfence();
+      atomicAdd((unsigned*)gen, 1u);
+    } else {
+      unsigned long long spins = 0;
+      while (ld_acquire_gpu(B.bar + 1) == g) {
+        if (++spins > B.spin_limit) {
+          ok = 0;
+          atomicExch(B.err, 1);
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+    s_ok = ok && *((volatile int*)B.err) == 0;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// next unit of a phase for this CTA: a work index in [0, total) or total when exhausted
+__device__ __forceinline__ unsigned grab(unsigned* counter, unsigned total) {
+  __shared__ unsigned s_w;
+  if (threadIdx.x == 0) s_w = atomicAdd(counter, 1u);
+  __syncthreads();
+  const unsigned w = s_w;
+  __syncthreads();
+  return w < total ? w : total;
+}
+
+// In-place inclusive prefix sums of a[0..n) and b[0..n) in shared memory by the whole CTA: each
+// thread sums a contiguous chunk, the chunk sums are scanned across warps, then written back.
+__device__ __forceinline__ void block_prefix2(uint32_t* a, uint32_t* b, uint32_t n) {
+  __shared__ uint32_t s_wa[32], s_wb[32];
+  const uint32_t nt = blockDim.x;
+  const uint32_t chunk = (n + nt - 1) / nt;
+  const uint32_t lo = threadIdx.x * chunk, hi = min(lo + chunk, n);
+  uint32_t sa = 0, sb = 0;
+  for (uint32_t i = lo; i < hi; ++i) { sa += a[i]; sb += b[i]; }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t ia = sa, ib = sb;  // inclusive warp scan
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t ta = __shfl_up_sync(0xffffffffu, ia, o), tb = __shfl_up_sync(0xffffffffu, ib, o);
+    if (lane >= o) { ia += ta; ib += tb; }
+  }
+  if (lane == 31) { s_wa[wid] = ia; s_wb[wid] = ib; }
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = (nt + 31) >> 5;
+    uint32_t va = lane < nw ? s_wa[lane] : 0u, vb = lane < nw ? s_wb[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t ta = __shfl_up_sync(0xffffffffu, va, o), tb = __shfl_up_sync(0xffffffffu, vb, o);
+      if (lane >= o) { va += ta; vb += tb; }
+    }
+    s_wa[lane] = va;
+    s_wb[lane] = vb;
+  }
+  __syncthreads();
+  uint32_t ra = ia - sa + (wid > 0 ? s_wa[wid - 1] : 0u);  // exclusive offset of this thread's chunk
+  uint32_t rb = ib - sb + (wid > 0 ? s_wb[wid - 1] : 0u);
+  for (uint32_t i = lo; i < hi; ++i) {
+    ra += a[i];
+    rb += b[i];
+    a[i] = ra;
+    b[i] = rb;
+  }
+  __syncthreads();
+}
+
+// replica owning work index w of an inclusive-exclusive prefix array p[0..n]
+__device__ __forceinline__ uint32_t find_replica(const uint32_t* p, uint32_t n, uint32_t w) {
+  uint32_t lo = 0, hi = n;  // p[lo] <= w < p[hi]
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (p[mid] <= w) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+template <typename Real, int MAXS>
+__global__ void __launch_bounds__(256, PLIS_LEAP_MIN_BLOCKS) k_batch(BatchArgs B) {
+  extern __shared__ int32_t s_box[];
+  __shared__ uint32_t s_lp[kMaxBatchReplicas + 1];  // bricks leaping, prefix over replicas
+  __shared__ uint32_t s_cp[kMaxBatchReplicas + 1];  // bricks classifying, prefix over replicas
+  __shared__ int s_exact, s_apply;
+  __shared__ long long s_ev[32];
+  __shared__ int s_big;
+  const uint32_t nrep = B.nrep;
+  Box box;
+  box.acc = B.g.staged ? s_box : nullptr;
+  box.bx = (int)B.g.tx + 2;
+  box.by = (int)B.g.ty + 2;
+  box.bz = (int)B.g.tz + 2;
+  box.size = box.bx * box.by * box.bz;
+
+  for (uint32_t it = 0; it < B.max_iters; ++it) {
+    const uint32_t gen = it % 3u;
+    // ---- plan (identical in every CTA) ----
+    if (threadIdx.x == 0) { s_exact = 0; s_apply = 0; }
+    __syncthreads();
+    for (uint32_t r = threadIdx.x; r < nrep; r += blockDim.x) {
+      const Ctrl* K = B.ctrl + r;
+      const int done = __ldcg(&K->done);
+      const uint32_t phase = __ldcg(&K->phase);
+      const uint32_t nt = B.rep[r].ntiles;
+      s_lp[r + 1] = (!done && phase == 1) ? nt : 0u;
+      s_cp[r + 1] = (!done) ? nt : 0u;
+      if (!done && phase == 1) {
+        const uint32_t ex = __ldcg(&K->exact);
+        if (ex) s_exact = 1;
+        if (ex & 1u) s_apply = 1;
+      }
+    }
+    if (threadIdx.x == 0) { s_lp[0] = 0; s_cp[0] = 0; }
+    __syncthreads();
+    block_prefix2(s_lp + 1, s_cp + 1, nrep);
+    const uint32_t n_leap = s_lp[nrep], n_class = s_cp[nrep];
+    const int any_exact = s_exact, any_apply = s_apply;
+    if (n_class == 0) break;
+
+    // ---- leap ----
+    if (n_leap > 0) {
+      while (true) {
+        const unsigned w = grab(B.work + 0 * 3 + gen, n_leap);
+        if (w >= n_leap) break;
+        const uint32_t r = find_replica(s_lp, nrep, w);
+        const KArgs& sA = B.views[r];
+        if (threadIdx.x == 0) s_big = 0;
+        __syncthreads();
+        Ctrl* K = sA.b.ctrl;
+        LeapCtx L;
+        L.Xc = sA.b.X[K->cur];
+        L.Xt = sA.b.X[K->tgt];
+        L.flag = sA.b.flag[K->tf];
+        L.step = K->step + 1;
+        L.attempt = K->attempt;
+        const Real tl = (Real)K->tau_leap;
+        long long ev;
+        int big;
+        leap_tile<Real, MAXS>(sA, w - s_lp[r], L, tl, box, ev, big);
+        ev = warp_sum(ev);
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        if (big) s_big = 1;
+        if (lane == 0) s_ev[wid] = ev;
+        __syncthreads();
+        if (wid == 0) {
+          const int nw = (blockDim.x + 31) >> 5;
+          long long v = lane < nw ? s_ev[lane] : 0;
+          v = warp_sum(v);
+          if (lane == 0) {
+            if (v) atomicAdd(&K->ev_attempt, (unsigned long long)v);
+            if (s_big) atomicOr(&K->blocks_done, 0x80000000u);
+          }
+        }
+        __syncthreads();
+      }
+      if (!grid_barrier(B)) return;
+    }
+
+    // ---- exact events (rare): one replica per CTA at a time ----
+    if (any_exact) {
+      while (true) {
+        const unsigned r = grab(B.work + 1 * 3 + gen, nrep);
+        if (r >= nrep) break;
+        const Ctrl* Kr = B.ctrl + r;
+        if (__ldcg(&Kr->done) || __ldcg(&Kr->phase) != 1u || __ldcg(&Kr->exact) == 0u) continue;
+        const KArgs& sA = B.views[r];
+        Ctrl* K = sA.b.ctrl;
+        const uint32_t ex = K->exact;
+        const int32_t* Xc = sA.b.X[K->cur];
+        int32_t* Xt = sA.b.X[K->tgt];
+        uint8_t* flag = sA.b.flag[K->tf];
+        const uint64_t step = K->step + 1;
+        const uint32_t attempt = K->attempt;
+        int fired = 0;
+        if (ex & 1u) {
+          for (uint32_t c = threadIdx.x; c < sA.m.N; c += blockDim.x) {
+            if (flag[c] == F_LEAP_CR) {
+              Counts<MAXS> x;
+              load_counts(sA.m, Xc, c, x);
+              fired += critical_event_ref<Real>(sA, c, x, Xt, step, attempt, sA.b.D, flag);
+            }
+          }
+        }
+        __syncthreads();
+        if ((ex & 2u) && threadIdx.x == 0) {
+          const uint32_t am = (uint32_t)K->argmin;
+          const uint8_t fa = flag[am];
+          Counts<MAXS> x;
+          load_counts(sA.m, Xc, am, x);
+          int32_t* dst = (ex & 1u) ? sA.b.D : Xt;
+          if (sA.o.mode == 0) {
+            if (fa == F_SSA || fa == F_SSA_FF) fired += argmin_event<Real>(sA, am, x, step, attempt, dst, flag, false);
+          } else if (fa == F_LEAP_CR) {
+            fired += argmin_event<Real>(sA, am, x, step, attempt, dst, flag, true);
+          } else if (fa == F_SSA || fa == F_SSA_FF) {
+            fired += argmin_event<Real>(sA, am, x, step, attempt, dst, flag, false);
+          }
+        }
+        if (fired) {
+          atomicAdd(&K->ev_attempt, (unsigned long long)fired);
+          atomicAdd(&K->ex_attempt, (unsigned long long)fired);
+        }
+        __syncthreads();
+      }
+      if (!grid_barrier(B)) return;
+      if (any_apply) {
+        while (true) {
+          const unsigned r = grab(B.work + 2 * 3 + gen, nrep);
+          if (r >= nrep) break;
+          const Ctrl* Kr = B.ctrl + r;
+          if (__ldcg(&Kr->done) || __ldcg(&Kr->phase) != 1u || !(__ldcg(&Kr->exact) & 1u)) continue;
+          const RepDesc& d = B.rep[r];
+          int32_t* Xt = B.X[__ldcg(&Kr->tgt)] + d.coff;
+          int32_t* Dr = B.D + d.coff;
+          for (uint32_t c = threadIdx.x; c < d.N; c += blockDim.x)
+            for (uint32_t s = 0; s < B.m.S; ++s) {
+              const size_t i = (size_t)s * B.m.Npad + c;
+              const int32_t v = Dr[i];
+              if (v) {
+                Xt[i] += v;
+                Dr[i] = 0;
+              }
+            }
+        }
+        if (!grid_barrier(B)) return;
+      }
+    }
+
+    // ---- classify + per-replica control ----
+    while (true) {
+      const unsigned w = grab(B.work + 3 * 3 + gen, n_class);
+      if (w >= n_class) break;
+      const uint32_t r = find_replica(s_cp, nrep, w);
+      const KArgs& sA = B.views[r];
+      Ctrl* K = sA.b.ctrl;
+      const ClassifyCtx C = classify_ctx(sA, K);
+      double tn;
+      long long ti;
+      int fl, bad;
+      bool valid;
+      const uint32_t tile = w - s_cp[r];
+      classify_tile<Real, MAXS>(sA, tile, C, tn, ti, fl, bad, valid);
+      if (classify_slot(sA, K, tile, sA.g.nblocks, tn, ti, valid && fl == F_LEAP_CR, bad))
+        classify_control(sA, K, sA.g.nblocks);
+      __syncthreads();
+    }
+    if (!grid_barrier(B)) return;
+    // counters of generation it+2 (== it-1) are no longer in use by any CTA
+    if (blockIdx.x == 0 && threadIdx.x < 4) B.work[threadIdx.x * 3 + (it + 2) % 3] = 0u;
+  }
+}
+
+template <typename Real, int MAXS>
+struct BatchKernelSet {
+  static void* kernel() { return (void*)&k_batch<Real, MAXS>; }
+  static cudaError_t set_smem(int bytes) {
+    return cudaFuncSetAttribute(k_batch<Real, MAXS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  }
+};
+
+template <typename Real>
+BatchLaunch batch_pick_impl(uint32_t S) {
+  if (S <= 1) return {BatchKernelSet<Real, 1>::kernel(), BatchKernelSet<Real, 1>::set_smem};
+  if (S <= 2) return {BatchKernelSet<Real, 2>::kernel(), BatchKernelSet<Real, 2>::set_smem};
+  if (S <= 4) return {BatchKernelSet<Real, 4>::kernel(), BatchKernelSet<Real, 4>::set_smem};
+  if (S <= 8) return {BatchKernelSet<Real, 8>::kernel(), BatchKernelSet<Real, 8>::set_smem};
+  return {BatchKernelSet<Real, 16>::kernel(), BatchKernelSet<Real, 16>::set_smem};
+}
+
+}  // namespace plis
+
+#endif

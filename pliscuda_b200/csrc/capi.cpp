@@ -4,6 +4,7 @@
 #include <string>
 
 #include "../../include/plis.h"
+#include "batch.h"
 #include "engine.h"
 #include "plis_model.h"
 
@@ -17,6 +18,10 @@ void set_error(const std::string& msg) { g_err = msg; }
 
 struct plis_handle {
   plis::Engine eng;
+};
+
+struct plis_batch {
+  plis::BatchEngine eng;
 };
 
 #define PLIS_GUARD_BEGIN try {
@@ -172,6 +177,103 @@ int plis_get_taus(plis_handle* h, double* tau, uint8_t* flags) {
   PLIS_GUARD_BEGIN
   if (!h) { g_err = "null argument"; return PLIS_ERR_INVALID; }
   return fail(h, h->eng.get_taus(tau, flags));
+  PLIS_GUARD_END
+}
+
+// ---------------------------------------------------------------------------------------------- batches
+static int bfail(plis_batch* b, int rc) {
+  if (rc != PLIS_OK) g_err = b->eng.error();
+  return rc;
+}
+
+int plis_batch_create(const plis_batch_desc* desc, const plis_options* opts, plis_batch** out) {
+  PLIS_GUARD_BEGIN
+  if (!desc || !out) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  *out = nullptr;
+  plis_options o;
+  plis_options_init(&o);
+  if (opts) {
+    if (opts->size != sizeof(plis_options)) { g_err = "plis_options.size mismatch (call plis_options_init)"; return PLIS_ERR_INVALID; }
+    o = *opts;
+  }
+  if (o.mode != PLIS_MODE_REFERENCE && o.mode != PLIS_MODE_CORRECTED) { g_err = "unknown mode"; return PLIS_ERR_INVALID; }
+  if (o.precision != PLIS_PREC_FP64 && o.precision != PLIS_PREC_FP32) { g_err = "unknown precision"; return PLIS_ERR_INVALID; }
+  if (o.critical_threshold < 0 || !(o.epsilon > 0.0) || o.max_rollbacks < 0 || o.max_rollbacks > 4000) {
+    g_err = "critical_threshold, epsilon or max_rollbacks out of range";
+    return PLIS_ERR_INVALID;
+  }
+  plis_batch* b = new plis_batch();
+  int rc = b->eng.create(*desc, o);
+  if (rc) {
+    g_err = b->eng.error();
+    delete b;
+    return rc;
+  }
+  *out = b;
+  return PLIS_OK;
+  PLIS_GUARD_END
+}
+
+int plis_batch_destroy(plis_batch* b) {
+  PLIS_GUARD_BEGIN
+  delete b;
+  return PLIS_OK;
+  PLIS_GUARD_END
+}
+
+int plis_batch_set_state(plis_batch* b, uint32_t replica, const uint32_t* counts) {
+  PLIS_GUARD_BEGIN
+  if (!b || !counts) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return bfail(b, b->eng.set_state(replica, counts));
+  PLIS_GUARD_END
+}
+
+int plis_batch_get_state(plis_batch* b, uint32_t replica, uint32_t* counts) {
+  PLIS_GUARD_BEGIN
+  if (!b || !counts) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return bfail(b, b->eng.get_state(replica, counts));
+  PLIS_GUARD_END
+}
+
+int plis_batch_get_taus(plis_batch* b, uint32_t replica, double* tau, uint8_t* flags) {
+  PLIS_GUARD_BEGIN
+  if (!b) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return bfail(b, b->eng.get_taus(replica, tau, flags));
+  PLIS_GUARD_END
+}
+
+int plis_batch_run(plis_batch* b, double t_end) {
+  PLIS_GUARD_BEGIN
+  if (!b) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return bfail(b, b->eng.run(t_end, ~0ull));
+  PLIS_GUARD_END
+}
+
+int plis_batch_step(plis_batch* b, uint64_t n) {
+  PLIS_GUARD_BEGIN
+  if (!b) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return bfail(b, b->eng.run(__builtin_inf(), n));
+  PLIS_GUARD_END
+}
+
+int plis_batch_get_stats(plis_batch* b, uint32_t replica, plis_stats* st) {
+  PLIS_GUARD_BEGIN
+  if (!b || !st) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return bfail(b, b->eng.stats(replica, st));
+  PLIS_GUARD_END
+}
+
+int plis_batch_autotune(plis_batch* b, uint64_t pilot_steps, plis_batch_tuning* out) {
+  PLIS_GUARD_BEGIN
+  if (!b) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return bfail(b, b->eng.autotune(pilot_steps, out));
+  PLIS_GUARD_END
+}
+
+int plis_batch_get_tuning(plis_batch* b, plis_batch_tuning* out) {
+  PLIS_GUARD_BEGIN
+  if (!b || !out) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return bfail(b, b->eng.tuning(out));
   PLIS_GUARD_END
 }
 

@@ -89,3 +89,23 @@ def test_null_arguments():
     assert _lib.lib.plis_set_state(None, None) == 1
     assert _lib.lib.plis_run(None, 1.0) == 1
     assert _lib.lib.plis_get_stats(None, None) == 1
+
+
+def _batch_kwargs(**over):
+    kw = dict(n_species=2, n_reactions=1, reactants=[1, 0], products=[0, 1], lattices=[[2, 2, 2], [3, 1, 1]],
+              reaction_rates=[1.0, 2.0], diffusion_rates=[0.1, 0.1, 0.2, 0.2])
+    kw.update(over)
+    return kw
+
+
+@pytest.mark.parametrize("over,status,msg", [
+    (dict(lattices=np.zeros((0, 3), np.uint32), reaction_rates=[], diffusion_rates=[]), 9, "n_replicas"),
+    (dict(reaction_rates=[1.0, -2.0]), 1, "finite and >= 0"),
+    (dict(lattices=[[2, 2, 2], [0, 1, 1]]), 1, "empty or too large lattice"),
+    (dict(n_species=17, reactants=[1] + [0] * 16, products=[0] * 17, diffusion_rates=[0.1] * 34), 9, "1..16 species"),
+])
+def test_invalid_batches_rejected_before_device(over, status, msg):
+    from pliscuda_b200.batch import Batch
+    with pytest.raises(plis.PlisError) as e:
+        Batch(**_batch_kwargs(**over))
+    assert e.value.status == status and msg in str(e.value)
