@@ -162,8 +162,12 @@ __device__ __forceinline__ uint32_t find_replica(const uint32_t* p, uint32_t n, 
   return lo;
 }
 
+// One kernel holds every phase, so it needs more registers than the leap alone.
+#ifndef PLIS_BATCH_MIN_BLOCKS
+#define PLIS_BATCH_MIN_BLOCKS 2
+#endif
 template <typename Real, int MAXS>
-__global__ void __launch_bounds__(256, PLIS_LEAP_MIN_BLOCKS) k_batch(BatchArgs B) {
+__global__ void __launch_bounds__(256, PLIS_BATCH_MIN_BLOCKS) k_batch(BatchArgs B) {
   extern __shared__ int32_t s_box[];
   __shared__ uint32_t s_lp[kMaxBatchReplicas + 1];  // bricks leaping, prefix over replicas
   __shared__ uint32_t s_cp[kMaxBatchReplicas + 1];  // bricks classifying, prefix over replicas
