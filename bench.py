@@ -28,6 +28,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import tempfile
 import statistics
 import subprocess
 import sys
@@ -50,6 +51,18 @@ def _peaks():
         return 6650.0, "fallback"
 
 
+# dram__bytes_read.sum + dram__bytes_write.sum per launch of the dominant kernel, from the committed
+# ncu capture of the same kernel on the same workload (profiles/k_leap_schlogl64.md: 2.49 MB read,
+# 0.22 MB written).  Keyed by (workload, semantics, precision, kernel); absent keys report null.
+NCU_TRAFFIC = {("schlogl64", "reference", "fp64", "leap"): (2.49e6 + 0.22e6, "profiles/k_leap_schlogl64.md")}
+
+WORKLOADS = {
+    "schlogl64": "Schlogl bistable model, 262144 subvolumes (64^3 reflective lattice), 1 species, 4 reactions",
+    "schlogl128": "Schlogl bistable model, 2097152 subvolumes (128^3 reflective lattice), 1 species, 4 reactions",
+    "small_ab": "A/B immigration-annihilation, 1000 subvolumes (10^3 reflective lattice), 2 species, 3 reactions",
+}
+
+
 def _workload(name):
     from pliscuda_b200 import workloads
     if name == "schlogl64":
@@ -70,7 +83,8 @@ class Clocks:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+        self.path = os.path.join(os.environ.get("PLIS_CLOCKS_DIR", tempfile.gettempdir()),
+                                 f"clocks_bench_{os.getpid()}.csv")
 
     def start(self):
         try:
@@ -183,6 +197,53 @@ def ncu_case(args):
     return 0
 
 
+def precision_report(args):
+    """FP32 form vs binary64 on the precision configuration: the seeded random 10-species,
+    20-reaction network (orders 0-2) on a 128^3 lattice.  The binary64 GPU step is bit-identical to
+    the FP64 host oracle, so its runs are the oracle's distribution.  The network is stiff (Cao tau
+    ~1e-10), so the report covers a short horizon: a binary64 pilot of --report-steps steps fixes
+    t_end, then both precisions run from the same state with independent seeds to exactly t_end
+    (corrected semantics, whose last step is cut at t_end).  Per species the change x(t_end) - x(0)
+    is compared over all subvolumes: relative error of its mean, that difference in standard errors
+    (z), and the KS distance of its distribution.  Also reports both precisions' throughput."""
+    import numpy as np
+    from scipy import stats as st_
+    from pliscuda_b200 import Simulation, workloads
+    side = args.report_side
+    model, state = workloads.random_network(side)
+    S, N = model.n_species, model.n_subvolumes
+    x0 = state.reshape(S, N).astype(np.int64)
+    with Simulation(model, mode="corrected", precision="fp64", seed=76) as sim:
+        sim.set_state(state)
+        t_end = sim.step(args.report_steps).time
+    res = {}
+    for prec in ("fp64", "fp32"):
+        with Simulation(model, mode="corrected", precision=prec, seed=77 if prec == "fp64" else 78) as sim:
+            sim.set_state(state)
+            st = sim.run(t_end)
+            x = sim.get_state().reshape(S, N).astype(np.int64)
+            res[prec] = {"delta": x - x0, "time": st.time, "events": st.events, "ms": st.device_ms,
+                         "steps": st.steps, "rollbacks": st.rollbacks}
+    d64, d32 = res["fp64"]["delta"], res["fp32"]["delta"]
+    per = []
+    for s in range(S):
+        m64, m32 = d64[s].mean(), d32[s].mean()
+        se = np.sqrt(d64[s].var() / N + d32[s].var() / N)
+        ks = float(st_.ks_2samp(d64[s], d32[s]).statistic) if d64[s].std() > 0 else 0.0
+        per.append({"species": s, "mean_delta_fp64": float(m64), "mean_delta_fp32": float(m32),
+                    "rel_error": float(abs(m32 - m64) / max(abs(m64), 1e-12)), "z": float((m32 - m64) / max(se, 1e-12)),
+                    "ks_delta": ks})
+    out = {"report": "precision", "workload": f"random network S=10 R=20 orders 0-2 on {side}^3, corrected semantics",
+           "t_end": t_end, "steps_fp64": res["fp64"]["steps"], "steps_fp32": res["fp32"]["steps"],
+           "rollbacks_fp64": res["fp64"]["rollbacks"], "rollbacks_fp32": res["fp32"]["rollbacks"],
+           "events_per_s_fp64": res["fp64"]["events"] / (res["fp64"]["ms"] * 1e-3),
+           "events_per_s_fp32": res["fp32"]["events"] / (res["fp32"]["ms"] * 1e-3),
+           "ms_per_step_fp64": res["fp64"]["ms"] / res["fp64"]["steps"],
+           "ms_per_step_fp32": res["fp32"]["ms"] / res["fp32"]["steps"], "per_species": per}
+    print(json.dumps(out))
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -196,30 +257,29 @@ def main(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--ncu-case", action="store_true", help="run only the fixed ncu capture case")
+    ap.add_argument("--precision-report", action="store_true", help="FP32 form vs binary64 on the precision config")
+    ap.add_argument("--report-side", type=int, default=128)
+    ap.add_argument("--report-steps", type=int, default=200)
     args = ap.parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
     if args.ncu_case:
         return ncu_case(args)
+    if args.precision_report:
+        return precision_report(args)
 
     import numpy as np
     import torch
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from pliscuda_b200 import Simulation, replicas
+    world, rank, local = replicas.rank_env()
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+    dist = replicas.init("nccl", local)
+    dev = replicas.rank_device(dist, local)
 
-    from pliscuda_b200 import Simulation
     model, state = _workload(args.workload)
-    seed = 1000 + rank
-    sim = Simulation(model, mode=args.mode, precision=args.precision, seed=seed, device=local)
+    ropt = replicas.replica_options(rank)
+    sim = Simulation(model, mode=args.mode, precision=args.precision, device=local, **ropt)
     sim.set_state(state)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")
 
@@ -251,19 +311,14 @@ def main(argv=None):
     ck = clocks.stop()
     if dist:
         dist.barrier()
-        v = torch.tensor([ms_tot, float(ev_tot), simt_tot], dtype=torch.float64, device=f"cuda:{local}")
-        mx = v.clone()
-        dist.all_reduce(mx[:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(v[1:2], op=dist.ReduceOp.SUM)
-        ms_all, ev_all = float(mx[0]), float(v[1])
-    else:
-        ms_all, ev_all = ms_tot, float(ev_tot)
+    job = replicas.combine(dist, dev, max_keys={"ms": ms_tot}, sum_keys={"events": float(ev_tot)})
+    ms_all, ev_all = job["ms"], job["events"]
     value = ev_all / (ms_all / 1e3)
     sim_time_per_sec = simt_tot / (ms_tot / 1e3)
 
     # per-kernel roofline from an event-instrumented replay of a slice of the same trajectory
     cur = sim.get_state()
-    with Simulation(model, mode=args.mode, precision=args.precision, seed=seed, device=local, profile=True) as ps:
+    with Simulation(model, mode=args.mode, precision=args.precision, device=local, profile=True, **ropt) as ps:
         ps.set_state(cur)
         ps.run(INTERVAL / 4)
         per = ps.kernel_profile()
@@ -274,6 +329,7 @@ def main(argv=None):
     achieved = algo_bytes[dom] / (ms_launch / 1e3) / 1e9
     peak, peak_kind = _peaks()
     shares = {k: round(v[0] / max(1e-12, sum(x[0] for x in per.values())), 4) for k, v in per.items()}
+    traffic = NCU_TRAFFIC.get((args.workload, args.mode, args.precision, dom), (None, None))
 
     # end to end through the C ABI with host buffers
     e2e = None
@@ -292,8 +348,9 @@ def main(argv=None):
             e_s += time.perf_counter() - w0
             e_ev += st.events
             hnp[:] = onp
-        e2e = {"value": e_ev / e_s, "unit": UNIT, "h2d_bytes_per_step": int(hnp.nbytes),
-               "d2h_bytes_per_step": int(onp.nbytes), "sim_time_per_sec": args.steps * INTERVAL / e_s}
+        ej = replicas.combine(dist, dev, max_keys={"s": e_s}, sum_keys={"events": float(e_ev)})
+        e2e = {"value": ej["events"] / ej["s"], "unit": UNIT, "h2d_bytes_per_step": int(hnp.nbytes) * world,
+               "d2h_bytes_per_step": int(onp.nbytes) * world, "sim_time_per_sec": args.steps * INTERVAL / e_s}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -305,8 +362,7 @@ def main(argv=None):
             "warmup": args.warmup, "ms_per_step": ms_all / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32",
             "data": "synthetic",
-            "config": {"workload": f"{args.workload}: Schlogl bistable model, {model.n_subvolumes} subvolumes "
-                                   f"(64^3 reflective lattice), 1 species, 4 reactions, {args.mode} semantics",
+            "config": {"workload": f"{args.workload}: {WORKLOADS[args.workload]}, {args.mode} semantics",
                        "step": f"one checkpoint interval of {INTERVAL} simulated time units",
                        "l2": "flushed between timed steps (512 MiB write)", "parallelism": f"replicas x{world}",
                        "precision": args.precision},
@@ -314,7 +370,7 @@ def main(argv=None):
             "leap_steps_per_sec": steps_tot / (ms_tot / 1e3),
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                         "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic[0], "traffic_source": traffic[1],
                          "algorithmic_bytes_per_launch": algo_bytes[dom], "ms_per_launch": ms_launch,
                          "kernel_share": shares},
             "e2e": e2e,
@@ -322,9 +378,7 @@ def main(argv=None):
             "clocks": ck,
         }
         print(json.dumps(line))
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finish(dist)
     return 0
 
 

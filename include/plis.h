@@ -18,7 +18,9 @@
  *                                                               (Topology.hpp:176-184)
  *   reaction_rates  [C*R], diffusion_rates [C*S] compartment-major (Configuration.hpp:123-143)
  *   compartment int32  [N] compartment of each subvolume       (cpp_utils.hpp:47-56)
- * Counts must stay below 2^31 (the reference stores them as int, driver.cu:55-59).
+ * Counts must stay below 2^30.  The reference stores them as int (driver.cu:55-59); one bit of
+ * headroom lets a step's summed int32 deltas be checked without overflow.  set_state rejects larger
+ * counts (PLIS_ERR_OVERFLOW), and a step that would reach 2^30 is rolled back with a halved tau.
  */
 #ifndef PLIS_H_
 #define PLIS_H_
@@ -41,7 +43,7 @@ typedef enum plis_status {
   PLIS_ERR_CUDA = 5,       /* CUDA runtime error (reference: gpuErrchk -> exit, cpp_utils.hpp:97-105) */
   PLIS_ERR_TIMEOUT = 6,    /* a bounded device-side wait gave up */
   PLIS_ERR_STUCK = 7,      /* more than max_rollbacks consecutive rollbacks in one step */
-  PLIS_ERR_OVERFLOW = 8,   /* a count would leave [0, 2^31) for a reason a rollback cannot fix */
+  PLIS_ERR_OVERFLOW = 8,   /* a count would leave [0, 2^30) (set_state input, or a step no rollback can fix) */
   PLIS_ERR_LIMIT = 9,      /* model exceeds a compiled limit (species, reactions, order, neighbours) */
   PLIS_ERR_NO_DEVICE = 10, /* no CUDA device (main.cpp:19-24) */
   PLIS_ERR_UNSUPPORTED = 11
@@ -157,6 +159,17 @@ int plis_set_time(plis_handle* h, double time);
 int plis_run(plis_handle* h, double t_end);
 int plis_step(plis_handle* h, uint64_t n_steps);
 int plis_get_stats(plis_handle* h, plis_stats* out);
+
+/* The reference's whole run_simulation (driver.cu:12-408) in one call: create a handle with opts
+ * (NULL = defaults), set counts, run until simulated time >= end_time, writing
+ * sim<unix time>_<time>.dat into out_dir (NULL or "" = the working directory) each time at least
+ * log_freq of simulated time has passed since the last snapshot (log_freq > 0; driver.cu:362-375)
+ * and once at the end (driver.cu:390-397), and, when verbose, print the reference's progress and
+ * final statistics lines to stdout (driver.cu:246, 380, 399-405).  A step with no possible event
+ * ends the run early as in the reference (driver.cu:269-272; stats.stop_reason ==
+ * PLIS_STOP_NO_EVENT).  *out (may be NULL) receives the final statistics. */
+int plis_run_simulation(const plis_model_desc* model, const uint32_t* counts, double end_time, double log_freq,
+                        const plis_options* opts, const char* out_dir, int verbose, plis_stats* out);
 
 /* Per-kernel timing of profiled run/step calls (plis_options.profile = 1); reset by plis_set_state. */
 int plis_get_profile(plis_handle* h, plis_profile* out);

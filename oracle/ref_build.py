@@ -9,7 +9,9 @@
 * pliscuda_test the reference's CUDA step (PLISCuda/src/*.cu + main.cpp) built with nvcc for sm_100a
   pliscuda      with -DTEST (fixed per-subvolume seeds, PLISCuda/src/init.cu:9-11) and without.
                 The reference makefile cannot be used as shipped (its -arch=sm_30 is gone from nvcc
-                12.9 and CCCL needs C++17); the flags below are the four changes recorded in DESIGN.md.
+                12.9 and CCCL needs C++17).  The build below keeps its -rdc=true and its release -O3 and
+                changes two flags: -arch=sm_100a for sm_30 and -std=c++17 for c++11; the TEST binary
+                adds -DTEST at -O3 (the makefile's test target uses -O2 -Wall).
 Outputs go only to oracle/_ref/ (git-ignored; it travels with the tree to the GPU box).
 Nothing from the reference is copied into the repository.
 """

@@ -2,7 +2,8 @@
 
     python pliscuda_b200/build.py [--force] [-v]
 
-Objects go to pliscuda_b200/_build/, the shared library to pliscuda_b200/libplis.so.  Every CUDA
+Objects go to pliscuda_b200/_build/, the shared library to pliscuda_b200/libplis.so, the
+`pliscuda <configuration file>` command to pliscuda_b200/pliscuda.  Every CUDA
 translation unit is compiled for sm_100a only, with -fmad=false so device floating point matches
 the host oracle bit for bit (explicit fma() calls are kept where the code wants them).
 """
@@ -19,6 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libplis.so")
+CLI = os.path.join(HERE, "pliscuda")
 ROOT = os.path.dirname(HERE)
 
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
@@ -30,7 +32,7 @@ CXX_FLAGS = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextr
              "-I" + os.path.join(CUDA_HOME, "include"), "-I" + os.path.join(ROOT, "include")]
 
 SOURCES = ["inst_f64.cu", "inst_f32.cu", "batch_f64.cu", "batch_f32.cu", "engine.cu", "batch.cu", "noalloc.cu",
-           "capi.cpp", "loader.cpp", "plis_model.cpp"]
+           "capi.cpp", "loader.cpp", "simulate.cpp", "plis_model.cpp"]
 HEADERS = ["engine_kernels.cuh", "batch_kernels.cuh", "batch.h", "engine.cuh", "engine.h", "plis_model.h",
            "plis_stream.h"]
 
@@ -78,12 +80,30 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+def build_cli(verbose: bool = False) -> str:
+    """The `pliscuda <configuration file>` command (csrc/cli.cpp) linked to libplis.so beside it."""
+    src = os.path.join(CSRC, "cli.cpp")
+    if os.path.exists(CLI) and os.path.getmtime(CLI) >= _newest([src, LIB, os.path.join(ROOT, "include", "plis.h")]):
+        return CLI
+    cmd = [os.environ.get("CXX", "g++")] + [f for f in CXX_FLAGS if f != "-fPIC"] + [
+        src, "-o", CLI + ".tmp", "-L" + HERE, "-lplis", "-Wl,-rpath,$ORIGIN",
+        "-L" + os.path.join(CUDA_HOME, "lib64"), "-lcudart_static", "-lpthread", "-ldl", "-lrt"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"building pliscuda failed:\n{r.stdout}\n{r.stderr}")
+    os.replace(CLI + ".tmp", CLI)
+    return CLI
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--force", action="store_true")
     ap.add_argument("-v", "--verbose", action="store_true")
     a = ap.parse_args(argv)
     print(build(force=a.force, verbose=a.verbose))
+    print(build_cli(verbose=a.verbose))
     return 0
 
 
