@@ -244,6 +244,77 @@ int plis_batch_autotune(plis_batch* b, uint64_t pilot_steps, plis_batch_tuning* 
 int plis_batch_get_tuning(plis_batch* b, plis_batch_tuning* out);
 
 /* ---------------------------------------------------------------------------------------------
+ * Learned tau proposals (no counterpart in the reference).  A proposer is an MLP 8 -> 64 -> 64 ->
+ * 64 -> 1 (ReLU; BF16 weights and activations, FP32 accumulation on the tensor cores) evaluated
+ * for every subvolume inside the classification.  Its features are log1p of the count of species
+ * 0, of the mean count of species 0 over the neighbours, of the propensities of reactions 0..3,
+ * log of the plain Cao leap bound tau_Cao, and log1p of the subvolume's total diffusion rate.  Its
+ * output y gives the proposal s * tau_Cao with s = exp(clamp(y, 0, log s_max)); flags and the
+ * critical times are decided against the proposal as against tau_Cao in the plain method.  The
+ * step leaps with the arg-min of the proposals; an attempt that has to be rolled back is retried
+ * with the plain Cao step (halved once per attempt), so every accepted step is either a proposal
+ * that kept all counts non-negative or a plain step.  Corrected mode only (PLIS_ERR_UNSUPPORTED
+ * otherwise); up to 4 species.  With s_max = 1 the trajectory is the plain method's, bit for bit.
+ *
+ * Training data are the simulator's own steps: plis_learner_record runs a plain handle step by
+ * step and records, for every stride-th subvolume (the offset rotates from step to step), the
+ * features of the state, its tau_Cao, the step taken from it and the label
+ * log(tau_safe / tau_Cao), where tau_safe = tau_step / max(rho, rho^2) and rho is the largest
+ * change of any propensity over the step relative to max(eps * a_j, c_j) (the Cao leap condition
+ * measured on the realised step), clamped to [log(1/16), log(64)].  plis_learner_train fits the
+ * MLP to a quantile of the label (pinball loss, Adam) with hand-written CUDA kernels.
+ * ------------------------------------------------------------------------------------------- */
+#define PLIS_PROPOSER_WEIGHTS 8977 /* 8961 parameters, then 8 feature means and 8 inverse deviations */
+
+typedef struct plis_train_params {
+  uint64_t iterations;     /* Adam steps, default 2000 */
+  uint32_t batch;          /* records per step, a multiple of 128, default 16384 */
+  float learning_rate;     /* default 1e-3 */
+  float quantile;          /* pinball-loss quantile of the label, default 0.25 */
+  uint64_t seed;           /* parameter initialisation and minibatch sampling, default 1 */
+} plis_train_params;
+
+typedef struct plis_train_report {
+  double loss_first;       /* mean pinball loss of the first and the last step's minibatch */
+  double loss_last;
+  uint64_t records;        /* records trained on */
+  uint64_t iterations;
+  double device_ms;        /* device time of the training (CUDA events) */
+} plis_train_report;
+
+/* A recorded subvolume-step, as plis_learner_get_records / set_records move them (64 bytes). */
+typedef struct plis_trace_record {
+  float features[8];       /* raw (unnormalised) features */
+  float tau_cao;
+  float tau_step;
+  float label;             /* NaN: unusable (no leap bound) */
+  uint32_t subvolume;
+  int32_t counts[4];       /* species 0..3 at the recorded state */
+} plis_trace_record;
+
+typedef struct plis_learner plis_learner;
+
+void plis_train_params_init(plis_train_params* p);
+int plis_learner_create(uint64_t capacity, int device, plis_learner** out);
+int plis_learner_destroy(plis_learner* learner);
+/* n_steps plain steps of h (corrected mode, <= 4 species), recording every stride-th subvolume */
+int plis_learner_record(plis_learner* learner, plis_handle* h, uint64_t n_steps, uint32_t stride);
+int plis_learner_count(const plis_learner* learner, uint64_t* n_records);
+int plis_learner_get_records(plis_learner* learner, uint64_t first, uint64_t n, plis_trace_record* out);
+int plis_learner_set_records(plis_learner* learner, const plis_trace_record* records, uint64_t n);
+/* feature statistics of the records, then p->iterations Adam steps from a fresh initialisation */
+int plis_learner_train(plis_learner* learner, const plis_train_params* p, plis_train_report* out);
+/* mean pinball loss and its gradient over all records (current weights and feature statistics) */
+int plis_learner_gradient(plis_learner* learner, float quantile, float* grad, double* loss);
+/* the MLP output y for n raw feature rows [n*8], through the same tensor-core inference code */
+int plis_learner_predict(plis_learner* learner, const float* features, uint64_t n, float* y);
+int plis_learner_get_weights(plis_learner* learner, float* weights);       /* [PLIS_PROPOSER_WEIGHTS] */
+int plis_learner_set_weights(plis_learner* learner, const float* weights);
+/* Attach a proposer (weights as plis_learner_get_weights returns them) to h with clamp s_max >= 1,
+ * or detach it (weights NULL or s_max <= 0).  The current state is classified again. */
+int plis_set_proposer(plis_handle* h, const float* weights, double s_max);
+
+/* ---------------------------------------------------------------------------------------------
  * Input files in the reference's formats, read unchanged (Configuration.hpp:27-144,
  * Topology.hpp:98-191, State.hpp:112-217, Reactions.hpp:132-223, cpp_utils.hpp:29-56).
  * ------------------------------------------------------------------------------------------- */

@@ -198,6 +198,18 @@ class Simulation:
         _check(_lib.lib.plis_get_stats(self._h, ctypes.byref(st)))
         return st
 
+    def set_proposer(self, weights: Optional[np.ndarray], s_max: float = 0.0) -> None:
+        """Attach a learned tau proposer (weights from pliscuda_b200.learned.Learner.weights(), clamp
+        s_max >= 1; corrected mode) or detach it (weights None).  The current state is classified
+        again; time and statistics are kept."""
+        if weights is None or s_max <= 0:
+            _check(_lib.lib.plis_set_proposer(self._h, None, 0.0))
+            return
+        w = np.ascontiguousarray(weights, dtype=np.float32).reshape(-1)
+        if w.size != _lib.PROPOSER_WEIGHTS:
+            raise InvalidArgument(1, f"proposer weights must hold {_lib.PROPOSER_WEIGHTS} floats, got {w.size}")
+        _check(_lib.lib.plis_set_proposer(self._h, _c(w), float(s_max)))
+
     def kernel_profile(self) -> dict:
         """{kernel: (total ms, launches)} of profiled calls (profile=True)."""
         p = _lib.Profile()

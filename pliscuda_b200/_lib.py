@@ -63,6 +63,24 @@ class BatchTuning(ctypes.Structure):
     _fields_ = [("tile", i32 * 3), ("blocks_per_sm", i32), ("grid", i32), ("events_per_s", f64)]
 
 
+class TrainParams(ctypes.Structure):
+    _fields_ = [("iterations", u64), ("batch", u32), ("learning_rate", ctypes.c_float), ("quantile", ctypes.c_float),
+                ("seed", u64)]
+
+
+class TrainReport(ctypes.Structure):
+    _fields_ = [("loss_first", f64), ("loss_last", f64), ("records", u64), ("iterations", u64), ("device_ms", f64)]
+
+
+PROPOSER_WEIGHTS = 8977
+# plis_trace_record (64 bytes)
+import numpy as _np  # noqa: E402
+
+TRACE_DTYPE = _np.dtype([("features", "<f4", (8,)), ("tau_cao", "<f4"), ("tau_step", "<f4"), ("label", "<f4"),
+                         ("subvolume", "<u4"), ("counts", "<i4", (4,))])
+assert TRACE_DTYPE.itemsize == 64
+
+
 class ConfigView(ctypes.Structure):
     _fields_ = [("model", ModelDesc), ("initial_state", vp), ("end_time", f64), ("log_freq", f64)]
 
@@ -113,6 +131,20 @@ def _load() -> ctypes.CDLL:
         "plis_parse_reactions": (i32, [ctypes.c_char_p, P(u32), P(u32), P(vp), P(vp)]),
         "plis_free": (None, [vp]),
         "plis_write_snapshot": (i32, [ctypes.c_char_p, vp, u32, u32, f64]),
+        "plis_run_simulation": (i32, [P(ModelDesc), vp, f64, f64, P(Options), ctypes.c_char_p, i32, P(Stats)]),
+        "plis_train_params_init": (None, [P(TrainParams)]),
+        "plis_learner_create": (i32, [u64, i32, P(vp)]),
+        "plis_learner_destroy": (i32, [vp]),
+        "plis_learner_record": (i32, [vp, vp, u64, u32]),
+        "plis_learner_count": (i32, [vp, P(u64)]),
+        "plis_learner_get_records": (i32, [vp, u64, u64, vp]),
+        "plis_learner_set_records": (i32, [vp, vp, u64]),
+        "plis_learner_train": (i32, [vp, P(TrainParams), P(TrainReport)]),
+        "plis_learner_gradient": (i32, [vp, ctypes.c_float, vp, P(f64)]),
+        "plis_learner_predict": (i32, [vp, vp, u64, vp]),
+        "plis_learner_get_weights": (i32, [vp, vp]),
+        "plis_learner_set_weights": (i32, [vp, vp]),
+        "plis_set_proposer": (i32, [vp, vp, f64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

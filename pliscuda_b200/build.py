@@ -32,9 +32,10 @@ CXX_FLAGS = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextr
              "-I" + os.path.join(CUDA_HOME, "include"), "-I" + os.path.join(ROOT, "include")]
 
 SOURCES = ["inst_f64.cu", "inst_f32.cu", "batch_f64.cu", "batch_f32.cu", "engine.cu", "batch.cu", "noalloc.cu",
+           "learned.cu",
            "capi.cpp", "loader.cpp", "simulate.cpp", "plis_model.cpp"]
-HEADERS = ["engine_kernels.cuh", "batch_kernels.cuh", "batch.h", "engine.cuh", "engine.h", "plis_model.h",
-           "plis_stream.h"]
+HEADERS = ["engine_kernels.cuh", "batch_kernels.cuh", "batch.h", "engine.cuh", "engine.h", "learned.h",
+           "plis_model.h", "plis_stream.h"]
 
 
 def _newest(paths):

@@ -6,6 +6,7 @@
 #include "../../include/plis.h"
 #include "batch.h"
 #include "engine.h"
+#include "learned.h"
 #include "plis_model.h"
 
 namespace {
@@ -22,6 +23,10 @@ struct plis_handle {
 
 struct plis_batch {
   plis::BatchEngine eng;
+};
+
+struct plis_learner {
+  plis::Learner l;
 };
 
 #define PLIS_GUARD_BEGIN try {
@@ -177,6 +182,119 @@ int plis_get_taus(plis_handle* h, double* tau, uint8_t* flags) {
   PLIS_GUARD_BEGIN
   if (!h) { g_err = "null argument"; return PLIS_ERR_INVALID; }
   return fail(h, h->eng.get_taus(tau, flags));
+  PLIS_GUARD_END
+}
+
+// ---------------------------------------------------------------------------------------------- learned tau
+static int lfail(plis_learner* L, int rc) {
+  if (rc != PLIS_OK) g_err = L->l.error();
+  return rc;
+}
+
+void plis_train_params_init(plis_train_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof *p);
+  p->iterations = 2000;
+  p->batch = 16384;
+  p->learning_rate = 1e-3f;
+  p->quantile = 0.25f;
+  p->seed = 1;
+}
+
+int plis_learner_create(uint64_t capacity, int device, plis_learner** out) {
+  PLIS_GUARD_BEGIN
+  if (!out) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  *out = nullptr;
+  if (capacity == 0 || capacity > (1ull << 31)) { g_err = "capacity must be in 1..2^31 records"; return PLIS_ERR_INVALID; }
+  plis_learner* L = new plis_learner();
+  int rc = L->l.create(capacity, device);
+  if (rc) {
+    g_err = L->l.error();
+    delete L;
+    return rc;
+  }
+  *out = L;
+  return PLIS_OK;
+  PLIS_GUARD_END
+}
+
+int plis_learner_destroy(plis_learner* L) {
+  PLIS_GUARD_BEGIN
+  delete L;
+  return PLIS_OK;
+  PLIS_GUARD_END
+}
+
+int plis_learner_record(plis_learner* L, plis_handle* h, uint64_t n_steps, uint32_t stride) {
+  PLIS_GUARD_BEGIN
+  if (!L || !h) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return lfail(L, L->l.record(h->eng, n_steps, stride));
+  PLIS_GUARD_END
+}
+
+int plis_learner_count(const plis_learner* L, uint64_t* n) {
+  PLIS_GUARD_BEGIN
+  if (!L || !n) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return L->l.count(n);
+  PLIS_GUARD_END
+}
+
+int plis_learner_get_records(plis_learner* L, uint64_t first, uint64_t n, plis_trace_record* out) {
+  PLIS_GUARD_BEGIN
+  if (!L || (!out && n)) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return lfail(L, L->l.get_records(first, n, out));
+  PLIS_GUARD_END
+}
+
+int plis_learner_set_records(plis_learner* L, const plis_trace_record* recs, uint64_t n) {
+  PLIS_GUARD_BEGIN
+  if (!L || (!recs && n)) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return lfail(L, L->l.set_records(recs, n));
+  PLIS_GUARD_END
+}
+
+int plis_learner_train(plis_learner* L, const plis_train_params* p, plis_train_report* out) {
+  PLIS_GUARD_BEGIN
+  if (!L) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  plis_train_params q;
+  plis_train_params_init(&q);
+  if (p) q = *p;
+  return lfail(L, L->l.train(q, out));
+  PLIS_GUARD_END
+}
+
+int plis_learner_gradient(plis_learner* L, float quantile, float* grad, double* loss) {
+  PLIS_GUARD_BEGIN
+  if (!L || !grad) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return lfail(L, L->l.gradient(grad, loss, quantile));
+  PLIS_GUARD_END
+}
+
+int plis_learner_predict(plis_learner* L, const float* features, uint64_t n, float* y) {
+  PLIS_GUARD_BEGIN
+  if (!L || ((!features || !y) && n)) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return lfail(L, L->l.predict(features, n, y));
+  PLIS_GUARD_END
+}
+
+int plis_learner_get_weights(plis_learner* L, float* w) {
+  PLIS_GUARD_BEGIN
+  if (!L || !w) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return lfail(L, L->l.get_weights(w));
+  PLIS_GUARD_END
+}
+
+int plis_learner_set_weights(plis_learner* L, const float* w) {
+  PLIS_GUARD_BEGIN
+  if (!L || !w) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return lfail(L, L->l.set_weights(w));
+  PLIS_GUARD_END
+}
+
+int plis_set_proposer(plis_handle* h, const float* weights, double s_max) {
+  PLIS_GUARD_BEGIN
+  if (!h) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return fail(h, h->eng.set_proposer(weights, s_max));
   PLIS_GUARD_END
 }
 

@@ -204,13 +204,19 @@ int Engine::create(const Model& model, const plis_options& opt) {
   return PLIS_OK;
 }
 
+void Engine::launch_classify() {
+  const dim3 gc(args_.g.nblocks), bc(args_.g.threads);
+  if (use_learned_) llaunch_.classify(args_, gc, bc, stream_);
+  else launch_.classify(args_, gc, bc, stream_);
+}
+
 void Engine::enqueue_step() {
   const dim3 gc(args_.g.nblocks), bc(args_.g.threads);
   const dim3 gx((args_.m.N + 255) / 256), bx(256);
   launch_.leap(args_, gc, bc, stream_);
   launch_.exact(args_, gx, bx, stream_);
   if (opt_.mode == PLIS_MODE_REFERENCE) k_apply<<<gx, bx, 0, stream_>>>(args_);
-  launch_.classify(args_, gc, bc, stream_);
+  launch_classify();
 }
 
 // Profiled step: the same four launches with CUDA events between them, accumulated per kernel.
@@ -226,7 +232,7 @@ int Engine::enqueue_step_profiled() {
   PLIS_CU(cudaEventRecord(pev_[2], stream_));
   if (opt_.mode == PLIS_MODE_REFERENCE) k_apply<<<gx, bx, 0, stream_>>>(args_);
   PLIS_CU(cudaEventRecord(pev_[3], stream_));
-  launch_.classify(args_, gc, bc, stream_);
+  launch_classify();
   PLIS_CU(cudaEventRecord(pev_[4], stream_));
   PLIS_CU(cudaEventSynchronize(pev_[4]));
   const int kind[4] = {PLIS_KERNEL_LEAP, PLIS_KERNEL_EXACT, PLIS_KERNEL_APPLY, PLIS_KERNEL_CLASSIFY};
@@ -293,13 +299,85 @@ int Engine::set_state(const uint32_t* counts) {
   k.t_end = 0.0;
   *h_ctrl_ = k;
   PLIS_CU(cudaMemcpyAsync(args_.b.ctrl, h_ctrl_, sizeof(Ctrl), cudaMemcpyHostToDevice, stream_));
-  launch_.classify(args_, dim3(args_.g.nblocks), dim3(args_.g.threads), stream_);
+  launch_classify();
   launches_ += 3;
   PLIS_CU(cudaGetLastError());
   int rc = read_ctrl();
   if (rc) return rc;
   device_ms_ = 0.0;
   std::memset(&prof_, 0, sizeof prof_);
+  state_set_ = true;
+  return PLIS_OK;
+}
+
+// Classify the current state again (after the classification kernels changed): phase 0 at the
+// current step, no fast-forward decrement; time, step and statistics are kept.
+int Engine::reclassify() {
+  int rc = read_ctrl();
+  if (rc) return rc;
+  if (h_ctrl_->status != PLIS_OK) return PLIS_OK;
+  h_ctrl_->phase = 0;
+  h_ctrl_->dt = 0.0;
+  h_ctrl_->done = 0;
+  PLIS_CU(cudaMemcpyAsync(args_.b.ctrl, h_ctrl_, sizeof(Ctrl), cudaMemcpyHostToDevice, stream_));
+  launch_classify();
+  launches_ += 1;
+  PLIS_CU(cudaGetLastError());
+  return read_ctrl();
+}
+
+int Engine::set_proposer(const float* weights, double s_max) {
+  const bool on = weights != nullptr && s_max > 0.0;
+  if (on) {
+    if (opt_.mode != PLIS_MODE_CORRECTED) {
+      err_ = "learned tau proposals need corrected mode";
+      return PLIS_ERR_UNSUPPORTED;
+    }
+    if (s_max < 1.0) { err_ = "s_max must be >= 1"; return PLIS_ERR_INVALID; }
+    llaunch_ = learned_pick(opt_.precision, model_.S);
+    if (!llaunch_.classify) { err_ = "learned tau proposals support up to 4 species"; return PLIS_ERR_LIMIT; }
+    int rc;
+    if (!d_lp_) {
+      if ((rc = dmalloc((void**)&d_lp_, sizeof(LearnedParams)))) return rc;
+      if ((rc = dmalloc((void**)&d_lw_, PLIS_PROPOSER_WEIGHTS * sizeof(float)))) return rc;
+      if ((rc = dmalloc((void**)&d_slot_plain_, (size_t)args_.g.nblocks * sizeof(double)))) return rc;
+    }
+    PLIS_CU(cudaMemcpyAsync(d_lw_, weights, PLIS_PROPOSER_WEIGHTS * sizeof(float), cudaMemcpyHostToDevice, stream_));
+    learned_pack(d_lw_, s_max, d_lp_, stream_);
+    PLIS_CU(cudaGetLastError());
+    args_.b.lp = d_lp_;
+    args_.b.slot_tau_plain = d_slot_plain_;
+  } else {
+    args_.b.lp = nullptr;
+    args_.b.slot_tau_plain = nullptr;
+  }
+  use_learned_ = on;
+  if (graph_exec_) {  // the graph holds the kernel arguments by value
+    cudaGraphExecDestroy(graph_exec_);
+    graph_exec_ = nullptr;
+  }
+  return state_set_ ? reclassify() : PLIS_OK;
+}
+
+int Engine::trace_features(TraceRec* out, uint32_t offset, uint32_t stride, uint32_t count) {
+  LearnedLaunch l = learned_pick(opt_.precision, model_.S);
+  if (!l.features) { err_ = "trace recording supports up to 4 species"; return PLIS_ERR_LIMIT; }
+  if (!state_set_) { err_ = "no state set"; return PLIS_ERR_INVALID; }
+  if (count == 0) return PLIS_OK;
+  l.features(args_, out, offset, stride, count, stream_);
+  launches_ += 1;
+  PLIS_CU(cudaGetLastError());
+  return PLIS_OK;
+}
+
+int Engine::trace_label(TraceRec* recs, uint32_t count, double tau_step) {
+  LearnedLaunch l = learned_pick(opt_.precision, model_.S);
+  if (!l.label) { err_ = "trace recording supports up to 4 species"; return PLIS_ERR_LIMIT; }
+  if (count == 0) return PLIS_OK;
+  l.label(args_, recs, count, tau_step, stream_);
+  launches_ += 1;
+  PLIS_CU(cudaGetLastError());
+  PLIS_CU(cudaStreamSynchronize(stream_));
   return PLIS_OK;
 }
 

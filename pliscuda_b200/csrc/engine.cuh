@@ -39,6 +39,12 @@ struct Ctrl {
   uint32_t pad_;
   unsigned long long events, exact_events, rollbacks;
   unsigned long long ev_attempt, ex_attempt;
+  // learned tau proposals (corrected mode): attempt 0 leaps with the arg-min of the proposed taus,
+  // every later attempt with the plain Cao step halved once per attempt
+  double tau_min_plain;  // min of the plain taus of the current state
+  double tau_step_plain; // the same clamped onto t_end
+  uint32_t learned;      // 1: tau_min is the min of proposed taus
+  uint32_t pad2_;
 };
 
 struct DevModel {
@@ -77,6 +83,8 @@ struct DevBufs {
   long long* slot_idx;
   uint32_t* slot_cr;
   uint32_t* slot_bad;
+  double* slot_tau_plain;  // learned classification: per-CTA min of the plain taus (else null)
+  const struct LearnedParams* lp;  // learned classification: the proposer's packed weights
   Ctrl* ctrl;
 };
 

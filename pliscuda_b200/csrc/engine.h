@@ -10,6 +10,7 @@
 
 #include "../../include/plis.h"
 #include "engine.cuh"
+#include "learned.h"
 #include "plis_model.h"
 
 namespace plis {
@@ -34,6 +35,13 @@ class Engine {
   int advance(double t_end, uint64_t n_steps);
   int stats(plis_stats* st);
   int profile(plis_profile* p);
+  // learned tau proposals (learned.cu): attach (weights != null, s_max >= 1) or detach a proposer
+  int set_proposer(const float* weights, double s_max);
+  // trace recording: features of every stride-th subvolume of the current state from offset, and
+  // the labels of those records once a step has been taken
+  int trace_features(TraceRec* out, uint32_t offset, uint32_t stride, uint32_t count);
+  int trace_label(TraceRec* recs, uint32_t count, double tau_step);
+  int device() const { return opt_.device; }
   const std::string& error() const { return err_; }
   const Model& model() const { return model_; }
 
@@ -42,8 +50,10 @@ class Engine {
   int dmalloc(void** p, size_t bytes);
   template <typename T> int upload(const std::vector<T>& v, const T** out);
   void enqueue_step();
+  void launch_classify();
   int build_graph();
   int read_ctrl();
+  int reclassify();
 
   Model model_;
   plis_options opt_{};
@@ -62,6 +72,12 @@ class Engine {
   plis_profile prof_{};
   cudaEvent_t pev_[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   int enqueue_step_profiled();
+  bool state_set_ = false;
+  bool use_learned_ = false;
+  LearnedLaunch llaunch_{};
+  LearnedParams* d_lp_ = nullptr;
+  float* d_lw_ = nullptr;
+  double* d_slot_plain_ = nullptr;
 };
 
 }  // namespace plis

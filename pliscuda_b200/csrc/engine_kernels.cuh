@@ -384,22 +384,31 @@ __device__ __forceinline__ void load_counts(const DevModel& m, const int32_t* X,
 // ------------------------------------------------------------------------------------------------
 // classification of one subvolume (compute_taus, tau.cu:197-252)
 // ------------------------------------------------------------------------------------------------
-template <typename Real, int MAXS>
-__device__ void classify_cell(const KArgs& A, uint32_t c, const Nbr& q, const Counts<MAXS>& x, const int32_t* Xe,
-                              double tau_cur, uint8_t flag_cur, uint64_t step, uint32_t attempt,
-                              double ff, double& tau_out, int& flag_out) {
-  const DevModel& m = A.m;
-  const int mode = A.o.mode;
-  const int nc = A.o.nc;
+// Fast-forward of an SSA_FF subvolume (tau.cu:214-217): true when the subvolume keeps its flag and
+// its tau is decremented by the time advanced.
+__device__ __forceinline__ bool classify_ff(int mode, double tau_cur, uint8_t flag_cur, uint64_t step, double ff,
+                                            double& tau_out, int& flag_out) {
   if (step > 0 && flag_cur == F_SSA_FF && !plis_isinf_d(tau_cur)) {
     if (mode == 0) {
-      if (ff > 0.0 && ff != tau_cur) { tau_out = tau_cur - ff; flag_out = F_SSA_FF; return; }  // tau.cu:214-217
+      if (ff > 0.0 && ff != tau_cur) { tau_out = tau_cur - ff; flag_out = F_SSA_FF; return true; }
     } else if (tau_cur > ff) {
       tau_out = tau_cur - ff;
       flag_out = F_SSA_FF;
-      return;
+      return true;
     }
   }
+  return false;
+}
+
+// The deterministic part of compute_taus (tau.cu:68-195): the Cao leap bound tau_ncr over the
+// species that enter it, and the rate whose exponential time is tau_cr (critical channels; in
+// corrected mode, all channels of a subvolume without a leap bound).
+template <typename Real, int MAXS>
+__device__ __forceinline__ void cell_tau_parts(const KArgs& A, uint32_t c, const Nbr& q, const Counts<MAXS>& x,
+                                               const int32_t* Xe, Real& tau_ncr_out, Real& rate_cr_out) {
+  const DevModel& m = A.m;
+  const int mode = A.o.mode;
+  const int nc = A.o.nc;
   const int comp = comp_of(m, c);
   const int n = q.n;
   const int S = (int)m.S, R = (int)m.R;
@@ -488,14 +497,20 @@ __device__ void classify_cell(const KArgs& A, uint32_t c, const Nbr& q, const Co
     for (int r = 0; r < R; ++r) rsum = rsum + prop<Real>(m, x, r, comp);
     for (int s = 0; s < S; ++s) dsum = dsum + (Real)n * (drate<Real>(m, comp, s) * (Real)x.get(s));
   }
-  double tcr;
-  if (rsum == (Real)0 && dsum == (Real)0) {
-    tcr = PLIS_INF_D;
-  } else {
-    plis_stream st = plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_TAU, step, attempt, 0);
-    tcr = plis_exponential_d(&st, (double)(rsum + dsum));
-  }
-  const double tn = (double)tau_ncr;
+  tau_ncr_out = tau_ncr;
+  rate_cr_out = (rsum == (Real)0 && dsum == (Real)0) ? (Real)0 : rsum + dsum;
+}
+
+// tau_cr: exponential time of the critical rate (inf when it is zero), tau.cu:193.
+template <typename Real>
+__device__ __forceinline__ double cell_tau_cr(const KArgs& A, uint32_t c, uint64_t step, uint32_t attempt, Real rate) {
+  if (rate == (Real)0) return PLIS_INF_D;
+  plis_stream st = plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_TAU, step, attempt, 0);
+  return plis_exponential_d(&st, (double)rate);
+}
+
+// Flag and tau of a subvolume from its leap bound and its critical time (tau.cu:224-250).
+__device__ __forceinline__ void cell_decide(double tn, double tcr, double& tau_out, int& flag_out) {
   if (plis_isinf_d(tn)) {
     flag_out = F_SSA_FF;
     tau_out = tcr;
@@ -509,11 +524,33 @@ __device__ void classify_cell(const KArgs& A, uint32_t c, const Nbr& q, const Co
 }
 
 // ------------------------------------------------------------------------------------------------
+// classification of one subvolume (compute_taus, tau.cu:197-252)
+// ------------------------------------------------------------------------------------------------
+template <typename Real, int MAXS>
+__device__ void classify_cell(const KArgs& A, uint32_t c, const Nbr& q, const Counts<MAXS>& x, const int32_t* Xe,
+                              double tau_cur, uint8_t flag_cur, uint64_t step, uint32_t attempt,
+                              double ff, double& tau_out, int& flag_out) {
+  if (classify_ff(A.o.mode, tau_cur, flag_cur, step, ff, tau_out, flag_out)) return;
+  Real tau_ncr, rate;
+  cell_tau_parts<Real>(A, c, q, x, Xe, tau_ncr, rate);
+  const double tcr = cell_tau_cr<Real>(A, c, step, attempt, rate);
+  cell_decide((double)tau_ncr, tcr, tau_out, flag_out);
+}
+
+// ------------------------------------------------------------------------------------------------
 // control (runs in one thread of the last CTA of k_classify, or in k_prepare)
 // ------------------------------------------------------------------------------------------------
 __device__ __forceinline__ void set_attempt(Ctrl* K, int mode) {
   double scale = 1.0;
   for (uint32_t i = 0; i < K->attempt; ++i) scale *= 0.5;
+  if (K->learned && K->attempt > 0) {  // a proposal was rolled back: plain Cao step, halved per attempt
+    K->tau_leap = K->tau_step_plain * scale;
+    K->dt = K->tau_leap;
+    K->exact = 0;
+    K->ev_attempt = 0;
+    K->ex_attempt = 0;
+    return;
+  }
   if (mode == 0) {  // the reference re-leaps with the un-halved tau but advances time by the halved one
     K->tau_leap = K->tau_min;
     K->dt = K->tau_min * scale;
@@ -547,6 +584,10 @@ __device__ __forceinline__ void prepare_step(Ctrl* K, int mode) {
   }
   K->tau_step = K->tau_min;
   if (mode == 1 && K->t_end - K->t < K->tau_step) K->tau_step = K->t_end - K->t;
+  if (K->learned) {
+    K->tau_step_plain = K->tau_min_plain;
+    if (K->t_end - K->t < K->tau_step_plain) K->tau_step_plain = K->t_end - K->t;
+  }
   K->attempt = 0;
   set_attempt(K, mode);
 }
@@ -578,6 +619,12 @@ __device__ __forceinline__ void warp_min_pair(double& t, long long& i) {
     min_pair(t, i, t2, i2);
   }
 }
+__device__ __forceinline__ double warp_min_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
 __device__ __forceinline__ long long warp_sum(long long v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -1074,7 +1121,7 @@ __device__ __forceinline__ ClassifyCtx classify_ctx(const KArgs& A, const Ctrl* 
   C.tau_new = A.b.tau[tf ^ 1u];
   C.flag_cur = A.b.flag[tf];
   C.flag_new = A.b.flag[tf ^ 1u];
-  C.step = phase == 0 ? 0 : K->step + 1;
+  C.step = phase == 0 ? K->step : K->step + 1;  // phase 0 at step 0 after set_state, or a re-classification
   C.attempt = phase == 0 ? 0 : K->attempt;
   C.ff = K->dt;
   return C;
@@ -1146,6 +1193,7 @@ __device__ __forceinline__ void classify_control(const KArgs& A, Ctrl* K, uint32
   __shared__ long long s_i[32];
   __shared__ unsigned long long s_cr[32];
   __shared__ uint32_t s_bad[32];
+  __shared__ double s_p[32];
   __threadfence();
   const uint32_t phase = K->phase;
   const uint32_t tf = K->tf;
@@ -1154,16 +1202,20 @@ __device__ __forceinline__ void classify_control(const KArgs& A, Ctrl* K, uint32
   long long gi = 0x7FFFFFFFFFFFFFFFll;
   unsigned long long gcr = 0;
   uint32_t gbad = 0;
+  double gp = PLIS_INF_D;  // learned classification: min of the plain taus
+  const double* sp = A.b.slot_tau_plain;
   for (uint32_t b = threadIdx.x; b < nslots; b += blockDim.x) {
     min_pair(gt, gi, __ldcg(&A.b.slot_tau[b]), __ldcg(&A.b.slot_idx[b]));
     gcr += __ldcg(&A.b.slot_cr[b]);
     gbad |= __ldcg(&A.b.slot_bad[b]);
+    if (sp) gp = fmin(gp, __ldcg(&sp[b]));
   }
   warp_min_pair(gt, gi);
   gcr = (unsigned long long)warp_sum((long long)gcr);
   gbad = __reduce_or_sync(0xffffffffu, gbad);
+  if (sp) gp = warp_min_d(gp);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  if (lane == 0) { s_t[wid] = gt; s_i[wid] = gi; s_cr[wid] = gcr; s_bad[wid] = gbad; }
+  if (lane == 0) { s_t[wid] = gt; s_i[wid] = gi; s_cr[wid] = gcr; s_bad[wid] = gbad; s_p[wid] = gp; }
   __syncthreads();
   if (wid == 0) {
     const int nw = (blockDim.x + 31) >> 5;
@@ -1171,17 +1223,21 @@ __device__ __forceinline__ void classify_control(const KArgs& A, Ctrl* K, uint32
     gi = lane < nw ? s_i[lane] : 0x7FFFFFFFFFFFFFFFll;
     gcr = lane < nw ? s_cr[lane] : 0ull;
     gbad = lane < nw ? s_bad[lane] : 0u;
+    gp = lane < nw ? s_p[lane] : PLIS_INF_D;
     warp_min_pair(gt, gi);
     gcr = (unsigned long long)warp_sum((long long)gcr);
     gbad = __reduce_or_sync(0xffffffffu, gbad);
+    if (sp) gp = warp_min_d(gp);
   }
   if (threadIdx.x == 0) {
     const int mode = A.o.mode;
     const uint32_t leap_bad = (__ldcg(&K->blocks_done) & 0x80000000u) ? 1u : 0u;
     K->blocks_done = 0;
     if (gi == 0x7FFFFFFFFFFFFFFFll) gi = -1;
+    K->learned = sp ? 1u : 0u;
     if (phase == 0) {
       K->tau_min = gt;
+      K->tau_min_plain = gp;
       K->argmin = gi;
       K->n_leap_cr = (uint32_t)gcr;
       K->argmin_flag = gi >= 0 ? __ldcg(&flag_new[gi]) : F_SSA_FF;
@@ -1215,6 +1271,7 @@ __device__ __forceinline__ void classify_control(const KArgs& A, Ctrl* K, uint32
       K->spare = oc;
       K->tf = tf ^ 1u;
       K->tau_min = gt;
+      K->tau_min_plain = gp;
       K->argmin = gi;
       K->n_leap_cr = (uint32_t)gcr;
       K->argmin_flag = gi >= 0 ? __ldcg(&flag_new[gi]) : F_SSA_FF;

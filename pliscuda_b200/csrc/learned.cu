@@ -1,0 +1,928 @@
+// learned.cu — learned tau proposals on the device.
+//
+//  * cell_features: the proposer's 8 inputs of one subvolume, computed from the same state and the
+//    same plain leap bound the classification computes.
+//  * warp_mlp: the MLP 8 -> 64 -> 64 -> 64 -> 1 for the 32 subvolumes of a warp on the tensor cores
+//    (mma.sync m16n8k16, BF16 operands, FP32 accumulators).  The accumulator fragment of one layer
+//    is, after bias + ReLU + BF16 rounding, exactly the A fragment of the next layer, so hidden
+//    activations never leave registers; B fragments are pre-packed per lane (16 KB per layer, read
+//    through L1).
+//  * k_classify_learned: the classification with proposals, a second (plain) min-tau reduction
+//    for the rollback fallback, and the usual last-CTA control.
+//  * k_trace_features / k_trace_label: recording of (features, label) pairs from plain steps.
+//  * k_train / k_adam / feature statistics / k_pack: training in FP32 (one CTA = 128 records, the
+//    forward and backward pass of the whole MLP in shared memory, per-CTA gradients reduced in a
+//    fixed order by the Adam kernel, so training is deterministic), then packing of the BF16
+//    fragments the inference reads.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "engine_kernels.cuh"
+#include "learned.h"
+
+namespace plis {
+
+// ------------------------------------------------------------------------------------------------
+// features
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ Cell cell_from_index(const DevModel& m, uint32_t c) {
+  Cell cl;
+  cl.c = c;
+  if (m.lattice) {
+    cl.x = c % m.X;
+    cl.y = (c / m.X) % m.Y;
+    cl.z = c / (m.X * m.Y);
+  } else {
+    cl.x = cl.y = cl.z = 0;
+  }
+  return cl;
+}
+
+// log1p(x0), log1p(mean neighbour x0), log1p(a_0..a_3), log(tau_Cao), log1p(total diffusion rate)
+template <typename Real, int MAXS>
+__device__ __forceinline__ void cell_features(const KArgs& A, uint32_t c, const Nbr& q, const Counts<MAXS>& x,
+                                              const int32_t* Xe, Real tau_ncr, float f[kFeat]) {
+  const DevModel& m = A.m;
+  const int comp = comp_of(m, c);
+  const float x0 = (float)x.get(0);
+  float ns = 0.f;
+  for (int j = 0; j < q.n; ++j) ns += (float)Xe[q.nb[j]];
+  f[0] = log1pf(x0);
+  f[1] = log1pf(q.n > 0 ? ns / (float)q.n : x0);
+#pragma unroll
+  for (int r = 0; r < 4; ++r) f[2 + r] = r < (int)m.R ? log1pf((float)prop<Real>(m, x, r, comp)) : 0.f;
+  f[6] = logf(fminf(fmaxf((float)tau_ncr, 1e-30f), 1e30f));
+  float dt = 0.f;
+  for (int s = 0; s < (int)m.S; ++s) dt += (float)q.n * ((float)drate<Real>(m, comp, s) * (float)x.get(s));
+  f[7] = log1pf(dt);
+}
+
+// ------------------------------------------------------------------------------------------------
+// warp-level tensor-core MLP
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);  // .x (lo) in the low 16 bits
+  return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+// D = A * B + D, A 16x16 row-major BF16, B 16x8 column-major BF16, D 16x8 FP32
+__device__ __forceinline__ void mma16816(float d[4], const uint32_t a[4], uint2 b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b.x), "r"(b.y));
+}
+
+// Accumulators of the 8 n-tiles of a 64-wide layer -> bias, ReLU, BF16 -> A fragments of the 4
+// k-tiles of the next layer (k-tile kk = n-tiles 2kk and 2kk+1).
+__device__ __forceinline__ void bias_relu_pack(const float c[8][4], const float* __restrict__ bias, int t,
+                                               uint32_t a[4][4]) {
+#pragma unroll
+  for (int kk = 0; kk < 4; ++kk) {
+    const int j0 = 2 * kk, j1 = 2 * kk + 1;
+    const float b00 = __ldg(&bias[8 * j0 + 2 * t]), b01 = __ldg(&bias[8 * j0 + 2 * t + 1]);
+    const float b10 = __ldg(&bias[8 * j1 + 2 * t]), b11 = __ldg(&bias[8 * j1 + 2 * t + 1]);
+    a[kk][0] = pack_bf16x2(fmaxf(c[j0][0] + b00, 0.f), fmaxf(c[j0][1] + b01, 0.f));
+    a[kk][1] = pack_bf16x2(fmaxf(c[j0][2] + b00, 0.f), fmaxf(c[j0][3] + b01, 0.f));
+    a[kk][2] = pack_bf16x2(fmaxf(c[j1][0] + b10, 0.f), fmaxf(c[j1][1] + b11, 0.f));
+    a[kk][3] = pack_bf16x2(fmaxf(c[j1][2] + b10, 0.f), fmaxf(c[j1][3] + b11, 0.f));
+  }
+}
+
+// y of this lane's row from its 8 normalised features.  Every lane of the warp must call it
+// (converged): lane l is row l; rows 0..15 and 16..31 are two m16 tiles done one after the other.
+__device__ float warp_mlp(const LearnedParams* __restrict__ P, const float f[kFeat]) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const uint32_t p0 = pack_bf16x2(f[0], f[1]), p1 = pack_bf16x2(f[2], f[3]);
+  const uint32_t p2 = pack_bf16x2(f[4], f[5]), p3 = pack_bf16x2(f[6], f[7]);
+  float mine = 0.f;
+#pragma unroll 1
+  for (int mt = 0; mt < 2; ++mt) {
+    uint32_t a[4][4];
+    {  // layer-1 A fragment: features 2t, 2t+1 of rows g and g+8 of this tile; K 8..15 are zero
+      const int s0 = 16 * mt + g, s1 = s0 + 8;
+      const uint32_t u0 = __shfl_sync(FULL, p0, s0), u1 = __shfl_sync(FULL, p1, s0);
+      const uint32_t u2 = __shfl_sync(FULL, p2, s0), u3 = __shfl_sync(FULL, p3, s0);
+      const uint32_t v0 = __shfl_sync(FULL, p0, s1), v1 = __shfl_sync(FULL, p1, s1);
+      const uint32_t v2 = __shfl_sync(FULL, p2, s1), v3 = __shfl_sync(FULL, p3, s1);
+      a[0][0] = t == 0 ? u0 : t == 1 ? u1 : t == 2 ? u2 : u3;
+      a[0][1] = t == 0 ? v0 : t == 1 ? v1 : t == 2 ? v2 : v3;
+      a[0][2] = 0u;
+      a[0][3] = 0u;
+    }
+    float c[8][4];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      c[j][0] = c[j][1] = c[j][2] = c[j][3] = 0.f;
+      mma16816(c[j], a[0], __ldg(&P->w1f[j * 32 + lane]));
+    }
+    bias_relu_pack(c, P->b1, t, a);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      c[j][0] = c[j][1] = c[j][2] = c[j][3] = 0.f;
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk) mma16816(c[j], a[kk], __ldg(&P->w2f[(kk * 8 + j) * 32 + lane]));
+    }
+    bias_relu_pack(c, P->b2, t, a);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      c[j][0] = c[j][1] = c[j][2] = c[j][3] = 0.f;
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk) mma16816(c[j], a[kk], __ldg(&P->w3f[(kk * 8 + j) * 32 + lane]));
+    }
+    // output layer in FP32: rows g (c0, c1) and g + 8 (c2, c3), columns 8j + 2t, 8j + 2t + 1
+    float y0 = 0.f, y1 = 0.f;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int col = 8 * j + 2 * t;
+      const float b0 = __ldg(&P->b3[col]), b1 = __ldg(&P->b3[col + 1]);
+      const float w0 = __ldg(&P->w4[col]), w1 = __ldg(&P->w4[col + 1]);
+      y0 = y0 + fmaxf(c[j][0] + b0, 0.f) * w0 + fmaxf(c[j][1] + b1, 0.f) * w1;
+      y1 = y1 + fmaxf(c[j][2] + b0, 0.f) * w0 + fmaxf(c[j][3] + b1, 0.f) * w1;
+    }
+    y0 += __shfl_xor_sync(FULL, y0, 1);
+    y0 += __shfl_xor_sync(FULL, y0, 2);
+    y1 += __shfl_xor_sync(FULL, y1, 1);
+    y1 += __shfl_xor_sync(FULL, y1, 2);
+    const int r = lane - 16 * mt;
+    const int src = 4 * (r & 7);
+    const float z0 = __shfl_sync(FULL, y0, src), z1 = __shfl_sync(FULL, y1, src);
+    if (r >= 0 && r < 16) mine = (r < 8 ? z0 : z1) + P->b4;
+  }
+  return mine;
+}
+
+__device__ __forceinline__ void normalise(const LearnedParams* __restrict__ P, float f[kFeat]) {
+#pragma unroll
+  for (int k = 0; k < kFeat; ++k) f[k] = (f[k] - __ldg(&P->fmean[k])) * __ldg(&P->finv[k]);
+}
+
+// ------------------------------------------------------------------------------------------------
+// classification with proposals
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ bool classify_slot_learned(const KArgs& A, Ctrl* K, uint32_t slot, uint32_t nslots,
+                                                      double tn, long long ti, double tp, bool is_cr, int bad) {
+  __shared__ double s_t[32];
+  __shared__ long long s_i[32];
+  __shared__ double s_p[32];
+  __shared__ bool s_last;
+  const int ncr = __syncthreads_count(is_cr);
+  const int nbad = __syncthreads_or(bad);
+  warp_min_pair(tn, ti);
+  tp = warp_min_d(tp);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) { s_t[wid] = tn; s_i[wid] = ti; s_p[wid] = tp; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    double bt = s_t[0], bp = s_p[0];
+    long long bi = s_i[0];
+    for (int w = 1; w < nw; ++w) {
+      min_pair(bt, bi, s_t[w], s_i[w]);
+      bp = fmin(bp, s_p[w]);
+    }
+    A.b.slot_tau[slot] = bt;
+    A.b.slot_idx[slot] = bi;
+    A.b.slot_tau_plain[slot] = bp;
+    A.b.slot_cr[slot] = (uint32_t)ncr;
+    A.b.slot_bad[slot] = nbad ? 1u : 0u;
+    __threadfence();
+    const uint32_t prev = atomicAdd(&K->blocks_done, 1u);
+    s_last = ((prev & 0x7FFFFFFFu) == nslots - 1);
+  }
+  __syncthreads();
+  return s_last;
+}
+
+template <typename Real, int MAXS>
+__global__ void __launch_bounds__(256, 2) k_classify_learned(KArgs A) {
+  Ctrl* K = A.b.ctrl;
+  if (K->done) return;
+  const ClassifyCtx C = classify_ctx(A, K);
+  const LearnedParams* P = A.b.lp;
+  const DevModel& m = A.m;
+  Cell cl;
+  const bool valid = cell_of(A, blockIdx.x, cl);
+  const uint32_t c = cl.c;
+  double tn = PLIS_INF_D, tp = PLIS_INF_D;
+  long long ti = 0x7FFFFFFFFFFFFFFFll;
+  int fl = F_SSA_FF, bad = 0;
+  bool ff = false;
+  Real tau_ncr = RT<Real>::inf(), rate = (Real)0;
+  float f[kFeat];
+#pragma unroll
+  for (int k = 0; k < kFeat; ++k) f[k] = 0.f;
+  if (valid) {
+    Counts<MAXS> x;
+    load_counts(m, C.Xe, c, x);
+#pragma unroll
+    for (int s = 0; s < MAXS; ++s)
+      if (s < (int)m.S) {
+        if (x.v[s] < 0) bad = 1;
+        C.Xz[(size_t)s * m.Npad + c] = 0;
+      }
+    Nbr q;
+    nbr_info(m, cl, q);
+    ff = classify_ff(A.o.mode, C.tau_cur[c], C.flag_cur[c], C.step, C.ff, tn, fl);
+    if (!ff) {
+      cell_tau_parts<Real>(A, c, q, x, C.Xe, tau_ncr, rate);
+      if (!plis_isinf_d((double)tau_ncr)) {
+        cell_features<Real>(A, c, q, x, C.Xe, tau_ncr, f);
+        normalise(P, f);
+      }
+    }
+  }
+  __syncwarp();
+  const float y = warp_mlp(P, f);
+  if (valid) {
+    if (ff) {
+      tp = tn;
+    } else {
+      const double tcr = cell_tau_cr<Real>(A, c, C.step, C.attempt, rate);
+      const double tnd = (double)tau_ncr;
+      int fp;
+      cell_decide(tnd, tcr, tp, fp);
+      const float ls = fminf(fmaxf(y, 0.f), P->log_smax);
+      const double sc = ls > 0.f ? (double)expf(ls) : 1.0;
+      cell_decide(plis_isinf_d(tnd) ? tnd : tnd * sc, tcr, tn, fl);
+    }
+    C.tau_new[c] = tn;
+    C.flag_new[c] = (uint8_t)fl;
+    ti = c;
+  }
+  if (classify_slot_learned(A, K, blockIdx.x, gridDim.x, tn, ti, tp, valid && fl == F_LEAP_CR, bad))
+    classify_control(A, K, gridDim.x);
+}
+
+// ------------------------------------------------------------------------------------------------
+// trace recording
+// ------------------------------------------------------------------------------------------------
+template <typename Real, int MAXS>
+__global__ void k_trace_features(KArgs A, TraceRec* out, uint32_t offset, uint32_t stride, uint32_t count) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const DevModel& m = A.m;
+  const int32_t* Xe = A.b.X[A.b.ctrl->cur];
+  const uint32_t c = offset + i * stride;
+  const Cell cl = cell_from_index(m, c);
+  Counts<MAXS> x;
+  load_counts(m, Xe, c, x);
+  Nbr q;
+  nbr_info(m, cl, q);
+  Real tn, rate;
+  cell_tau_parts<Real>(A, c, q, x, Xe, tn, rate);
+  TraceRec r;
+  cell_features<Real>(A, c, q, x, Xe, tn, r.f);
+  r.tau_cao = (float)tn;
+  r.tau_step = 0.f;
+  r.label = PLIS_NAN_F;
+  r.cell = c;
+#pragma unroll
+  for (int s = 0; s < 4; ++s) r.x[s] = s < (int)m.S ? x.get(s) : 0;
+  out[i] = r;
+}
+
+// label of each record from the state the step reached: the Cao leap condition on the realised step
+template <typename Real, int MAXS>
+__global__ void k_trace_label(KArgs A, TraceRec* recs, uint32_t count, double tau_step) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const DevModel& m = A.m;
+  TraceRec r = recs[i];
+  const uint32_t c = r.cell;
+  const int comp = comp_of(m, c);
+  Counts<MAXS> x0, x1;
+#pragma unroll
+  for (int s = 0; s < MAXS; ++s) x0.v[s] = (s < (int)m.S && s < 4) ? r.x[s] : 0;
+  load_counts(m, A.b.X[A.b.ctrl->cur], c, x1);
+  const Cell cl = cell_from_index(m, c);
+  Nbr q;
+  nbr_info(m, cl, q);
+  const float eps = (float)A.o.eps;
+  const Real* rr = (const Real*)m.rr;
+  float rho = 0.f;
+  for (int j = 0; j < (int)m.R; ++j) {
+    const float a0 = (float)prop<Real>(m, x0, j, comp), a1 = (float)prop<Real>(m, x1, j, comp);
+    const float cj = (float)rr[(size_t)comp * m.R + j];
+    if ((a0 > 0.f || a1 > 0.f) && cj > 0.f) rho = fmaxf(rho, fabsf(a1 - a0) / fmaxf(eps * a0, cj));
+  }
+  for (int s = 0; s < (int)m.S; ++s) {
+    const float d = (float)q.n * (float)drate<Real>(m, comp, s);
+    if (d > 0.f) {
+      const float a0 = d * (float)x0.get(s), a1 = d * (float)x1.get(s);
+      rho = fmaxf(rho, fabsf(a1 - a0) / fmaxf(eps * a0, d));
+    }
+  }
+  r.tau_step = (float)tau_step;
+  const float lmax = 4.158883083f, lmin = -2.772588722f;  // log 64, log 1/16
+  if (!(r.tau_cao > 0.f) || isinf(r.tau_cao) || !(tau_step > 0.0)) {
+    r.label = PLIS_NAN_F;
+  } else if (rho <= 0.f) {
+    r.label = lmax;
+  } else {
+    const double safe = tau_step / fmax((double)rho, (double)rho * (double)rho);
+    r.label = fminf(fmaxf((float)log(safe / (double)r.tau_cao), lmin), lmax);
+  }
+  recs[i] = r;
+}
+
+template <typename Real, int MAXS>
+struct LearnedSet {
+  static void classify(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) {
+    k_classify_learned<Real, MAXS><<<g, b, 0, s>>>(a);
+  }
+  static void features(const KArgs& a, TraceRec* out, uint32_t offset, uint32_t stride, uint32_t count,
+                       cudaStream_t s) {
+    k_trace_features<Real, MAXS><<<(count + 127) / 128, 128, 0, s>>>(a, out, offset, stride, count);
+  }
+  static void label(const KArgs& a, TraceRec* recs, uint32_t count, double tau_step, cudaStream_t s) {
+    k_trace_label<Real, MAXS><<<(count + 127) / 128, 128, 0, s>>>(a, recs, count, tau_step);
+  }
+};
+
+template <typename Real>
+static LearnedLaunch learned_pick_impl(uint32_t S) {
+  if (S <= 1) return {LearnedSet<Real, 1>::classify, LearnedSet<Real, 1>::features, LearnedSet<Real, 1>::label};
+  if (S <= 2) return {LearnedSet<Real, 2>::classify, LearnedSet<Real, 2>::features, LearnedSet<Real, 2>::label};
+  if (S <= 4) return {LearnedSet<Real, 4>::classify, LearnedSet<Real, 4>::features, LearnedSet<Real, 4>::label};
+  return {nullptr, nullptr, nullptr};
+}
+
+LearnedLaunch learned_pick(int precision, uint32_t S) {
+  return precision == PLIS_PREC_FP32 ? learned_pick_impl<float>(S) : learned_pick_impl<double>(S);
+}
+
+// ------------------------------------------------------------------------------------------------
+// packing, inference for tests
+// ------------------------------------------------------------------------------------------------
+__global__ void k_pack(const float* __restrict__ w, float log_smax, LearnedParams* __restrict__ P) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = i & 31, g = lane >> 2, t = lane & 3;
+  if (i < 8 * 32) {
+    const int n = 8 * (i >> 5) + g, k = 2 * t;  // K rows 8..15 are the zero padding
+    P->w1f[i] = make_uint2(pack_bf16x2(w[kOffW1 + k * kHid + n], w[kOffW1 + (k + 1) * kHid + n]), 0u);
+  } else if (i < 8 * 32 + 2 * 32 * 32) {
+    const int ii = i - 8 * 32;
+    const int layer = ii >> 10, fr = (ii & 1023) >> 5;  // fragment kk * 8 + j
+    const int kk = fr >> 3, j = fr & 7;
+    const float* W = w + (layer == 0 ? kOffW2 : kOffW3);
+    const int n = 8 * j + g, k = 16 * kk + 2 * t;
+    const uint2 v = make_uint2(pack_bf16x2(W[k * kHid + n], W[(k + 1) * kHid + n]),
+                               pack_bf16x2(W[(k + 8) * kHid + n], W[(k + 9) * kHid + n]));
+    if (layer == 0) P->w2f[ii & 1023] = v;
+    else P->w3f[ii & 1023] = v;
+  }
+  if (i < kHid) {
+    P->b1[i] = w[kOffB1 + i];
+    P->b2[i] = w[kOffB2 + i];
+    P->b3[i] = w[kOffB3 + i];
+    P->w4[i] = w[kOffW4 + i];
+  }
+  if (i < kFeat) {
+    P->fmean[i] = w[kNParams + i];
+    P->finv[i] = w[kNParams + kFeat + i];
+  }
+  if (i == 0) {
+    P->b4 = w[kOffB4];
+    P->log_smax = log_smax;
+  }
+}
+
+void learned_pack(const float* w, double s_max, LearnedParams* out, cudaStream_t s) {
+  const float ls = s_max > 1.0 ? (float)std::log(s_max) : 0.f;
+  k_pack<<<(8 * 32 + 2 * 32 * 32 + 255) / 256, 256, 0, s>>>(w, ls, out);
+}
+
+__global__ void k_predict(const LearnedParams* __restrict__ P, const float* __restrict__ feats, uint64_t n,
+                          float* __restrict__ y) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  float f[kFeat];
+#pragma unroll
+  for (int k = 0; k < kFeat; ++k) f[k] = i < n ? feats[i * kFeat + k] : 0.f;
+  if (i < n) normalise(P, f);
+  const float v = warp_mlp(P, f);  // whole warps: the grid covers n rounded up to 128
+  if (i < n) y[i] = v;
+}
+
+// ------------------------------------------------------------------------------------------------
+// training
+// ------------------------------------------------------------------------------------------------
+constexpr int kTB = 128;          // records per training CTA
+constexpr int kLd = kTB + 1;      // row pitch of the activation tiles (bank-conflict-free columns)
+constexpr size_t kTrainSmem = (size_t)(kNParams + (kFeat + 3 * kHid) * kLd + kTB + 32) * sizeof(float);
+constexpr int kStatN = 2 * kFeat + 2;  // sums of f, f^2, label, count
+
+// dW[k][j] = sum_u A[k][u] G[j][u] for a 64x64 layer: each thread a 4x8 tile
+__device__ __forceinline__ void grad_tile(const float* A, const float* G, float* out, int t) {
+  const int k0 = (t >> 3) * 4, j0 = (t & 7) * 8;
+  float acc[4][8];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int l = 0; l < 8; ++l) acc[i][l] = 0.f;
+  for (int u = 0; u < kTB; ++u) {
+    float a[4], g[8];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a[i] = A[(k0 + i) * kLd + u];
+#pragma unroll
+    for (int l = 0; l < 8; ++l) g[l] = G[(j0 + l) * kLd + u];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int l = 0; l < 8; ++l) acc[i][l] = acc[i][l] + a[i] * g[l];
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int l = 0; l < 8; ++l) out[(k0 + i) * kHid + j0 + l] = acc[i][l];
+}
+
+// column t: H[k] <- (sum_j G[j] W[k][j]) * (H[k] > 0)
+__device__ __forceinline__ void backprop_layer(const float* G, float* H, const float* W, int t) {
+  float acc[kHid];
+#pragma unroll
+  for (int k = 0; k < kHid; ++k) acc[k] = 0.f;
+  for (int j = 0; j < kHid; ++j) {
+    const float gj = G[j * kLd + t];
+#pragma unroll
+    for (int k = 0; k < kHid; ++k) acc[k] = acc[k] + gj * W[k * kHid + j];
+  }
+#pragma unroll
+  for (int k = 0; k < kHid; ++k) {
+    const float h = H[k * kLd + t];
+    H[k * kLd + t] = h > 0.f ? acc[k] : 0.f;
+  }
+}
+
+// column t: H[j] <- relu(b[j] + sum_k In[k] W[k][j])
+__device__ __forceinline__ void forward_layer(const float* In, float* H, const float* W, const float* b, int t) {
+  float acc[kHid];
+#pragma unroll
+  for (int j = 0; j < kHid; ++j) acc[j] = b[j];
+  for (int k = 0; k < kHid; ++k) {
+    const float h = In[k * kLd + t];
+#pragma unroll
+    for (int j = 0; j < kHid; ++j) acc[j] = acc[j] + h * W[k * kHid + j];
+  }
+#pragma unroll
+  for (int j = 0; j < kHid; ++j) H[j * kLd + t] = fmaxf(acc[j], 0.f);
+}
+
+// One CTA: forward and backward pass of 128 records; writes its summed gradient (already scaled by
+// inv_batch) and its summed loss.  fixed: record blockIdx*128 + t; else Philox-sampled records.
+__global__ void __launch_bounds__(kTB) k_train(const TraceRec* __restrict__ recs, uint64_t n,
+                                                const float* __restrict__ W, float* __restrict__ partial,
+                                                float* __restrict__ loss_out, uint64_t iter, uint32_t seed_lo,
+                                                uint32_t seed_hi, float quantile, int fixed, float inv_batch) {
+  extern __shared__ float sm[];
+  float* sW = sm;
+  float* F = sW + kNParams;
+  float* H1 = F + kFeat * kLd;
+  float* H2 = H1 + kHid * kLd;
+  float* H3 = H2 + kHid * kLd;
+  float* dy = H3 + kHid * kLd;
+  float* red = dy + kTB;
+  const int t = threadIdx.x;
+  for (int i = t; i < kNParams; i += kTB) sW[i] = W[i];
+  uint64_t idx;
+  bool use;
+  if (fixed) {
+    idx = (uint64_t)blockIdx.x * kTB + t;
+    use = idx < n;
+  } else {
+    plis_u32x4 ctr = {(uint32_t)(blockIdx.x * kTB + t), (uint32_t)iter, (uint32_t)(iter >> 32), 0x7A11u};
+    const plis_u32x4 r = plis_philox4x32_10(ctr, seed_lo, seed_hi);
+    idx = (((uint64_t)r.x << 32) | r.y) % n;
+    use = true;
+  }
+  float f[kFeat], label = 0.f;
+  if (use) {
+    const TraceRec& r = recs[idx];
+    label = r.label;
+    use = !isnan(label);
+#pragma unroll
+    for (int k = 0; k < kFeat; ++k) f[k] = (r.f[k] - W[kNParams + k]) * W[kNParams + kFeat + k];
+  }
+  if (!use) {
+#pragma unroll
+    for (int k = 0; k < kFeat; ++k) f[k] = 0.f;
+  }
+#pragma unroll
+  for (int k = 0; k < kFeat; ++k) F[k * kLd + t] = f[k];
+  __syncthreads();
+  // forward
+  for (int j = 0; j < kHid; ++j) {
+    float s = sW[kOffB1 + j];
+#pragma unroll
+    for (int k = 0; k < kFeat; ++k) s = s + f[k] * sW[kOffW1 + k * kHid + j];
+    H1[j * kLd + t] = fmaxf(s, 0.f);
+  }
+  forward_layer(H1, H2, sW + kOffW2, sW + kOffB2, t);
+  forward_layer(H2, H3, sW + kOffW3, sW + kOffB3, t);
+  float y = sW[kOffB4];
+  for (int j = 0; j < kHid; ++j) y = y + H3[j * kLd + t] * sW[kOffW4 + j];
+  float loss = 0.f, g = 0.f;
+  if (use) {
+    const float res = label - y;
+    loss = res >= 0.f ? quantile * res : (quantile - 1.f) * res;
+    g = res > 0.f ? -quantile : (res < 0.f ? 1.f - quantile : 0.f);
+  }
+  dy[t] = g * inv_batch;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
+  if ((t & 31) == 0) red[t >> 5] = loss;
+  __syncthreads();
+  if (t == 0) loss_out[blockIdx.x] = red[0] + red[1] + red[2] + red[3];
+  float* P = partial + (size_t)blockIdx.x * kNParams;
+  // output layer
+  if (t < kHid) {
+    float s = 0.f;
+    for (int u = 0; u < kTB; ++u) s = s + H3[t * kLd + u] * dy[u];
+    P[kOffW4 + t] = s;
+  } else if (t == kHid) {
+    float s = 0.f;
+    for (int u = 0; u < kTB; ++u) s = s + dy[u];
+    P[kOffB4] = s;
+  }
+  __syncthreads();
+  {  // G3 = dy * w4 * relu'(H3), in place
+    const float d = dy[t];
+    for (int j = 0; j < kHid; ++j) {
+      const float h = H3[j * kLd + t];
+      H3[j * kLd + t] = h > 0.f ? d * sW[kOffW4 + j] : 0.f;
+    }
+  }
+  __syncthreads();
+  grad_tile(H2, H3, P + kOffW3, t);
+  if (t < kHid) {
+    float s = 0.f;
+    for (int u = 0; u < kTB; ++u) s = s + H3[t * kLd + u];
+    P[kOffB3 + t] = s;
+  }
+  __syncthreads();
+  backprop_layer(H3, H2, sW + kOffW3, t);  // G2 in place of H2
+  __syncthreads();
+  grad_tile(H1, H2, P + kOffW2, t);
+  if (t < kHid) {
+    float s = 0.f;
+    for (int u = 0; u < kTB; ++u) s = s + H2[t * kLd + u];
+    P[kOffB2 + t] = s;
+  }
+  __syncthreads();
+  backprop_layer(H2, H1, sW + kOffW2, t);  // G1 in place of H1
+  __syncthreads();
+  for (int e = t; e < kFeat * kHid; e += kTB) {
+    const int k = e / kHid, j = e % kHid;
+    float s = 0.f;
+    for (int u = 0; u < kTB; ++u) s = s + F[k * kLd + u] * H1[j * kLd + u];
+    P[kOffW1 + e] = s;
+  }
+  if (t < kHid) {
+    float s = 0.f;
+    for (int u = 0; u < kTB; ++u) s = s + H1[t * kLd + u];
+    P[kOffB1 + t] = s;
+  }
+}
+
+// gradient = sum over CTAs (fixed order); Adam step when lr > 0, else the gradient into out
+__global__ void k_adam(float* __restrict__ W, float* __restrict__ m, float* __restrict__ v,
+                       const float* __restrict__ partial, uint32_t nblk, float lr, float bc1, float bc2,
+                       float* __restrict__ out) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= kNParams) return;
+  float g = 0.f;
+  for (uint32_t b = 0; b < nblk; ++b) g = g + partial[(size_t)b * kNParams + p];
+  if (out) {
+    out[p] = g;
+    return;
+  }
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  const float mm = b1 * m[p] + (1.f - b1) * g;
+  const float vv = b2 * v[p] + (1.f - b2) * g * g;
+  m[p] = mm;
+  v[p] = vv;
+  W[p] = W[p] - lr * (mm / bc1) / (sqrtf(vv / bc2) + eps);
+}
+
+// per-CTA sums of the usable records' features, squares, labels and count
+__global__ void k_feat_partial(const TraceRec* __restrict__ recs, uint64_t n, double* __restrict__ part) {
+  __shared__ double s[kStatN][8];
+  double acc[kStatN];
+#pragma unroll
+  for (int k = 0; k < kStatN; ++k) acc[k] = 0.0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const TraceRec& r = recs[i];
+    if (isnan(r.label)) continue;
+#pragma unroll
+    for (int k = 0; k < kFeat; ++k) {
+      acc[k] += (double)r.f[k];
+      acc[kFeat + k] += (double)r.f[k] * (double)r.f[k];
+    }
+    acc[2 * kFeat] += (double)r.label;
+    acc[2 * kFeat + 1] += 1.0;
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < kStatN; ++k) {
+    double v = acc[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) s[k][wid] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < kStatN) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += s[threadIdx.x][w];
+    part[(size_t)blockIdx.x * kStatN + threadIdx.x] = v;
+  }
+}
+
+// means and inverse deviations into the weights buffer, the label mean into out[0], count out[1]
+__global__ void k_feat_final(const double* __restrict__ part, int nblk, float* __restrict__ w, double* __restrict__ out) {
+  __shared__ double tot[kStatN];
+  if (threadIdx.x < kStatN) {
+    double v = 0.0;
+    for (int b = 0; b < nblk; ++b) v += part[(size_t)b * kStatN + threadIdx.x];
+    tot[threadIdx.x] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < kFeat) {
+    const int k = threadIdx.x;
+    const double cnt = tot[2 * kFeat + 1];
+    const double mean = cnt > 0 ? tot[k] / cnt : 0.0;
+    const double var = cnt > 0 ? tot[kFeat + k] / cnt - mean * mean : 1.0;
+    const double sd = sqrt(var > 1e-6 ? var : 1e-6);
+    w[kNParams + k] = (float)mean;
+    w[kNParams + kFeat + k] = (float)(1.0 / sd);
+  }
+  if (threadIdx.x == 0) {
+    const double cnt = tot[2 * kFeat + 1];
+    out[0] = cnt > 0 ? tot[2 * kFeat] / cnt : 0.0;
+    out[1] = cnt;
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// host: Learner
+// ------------------------------------------------------------------------------------------------
+#define PLIS_LCU(call)                                                                   \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess) {                                                             \
+      err_ = std::string(#call) + ": " + cudaGetErrorString(e_);                          \
+      return e_ == cudaErrorMemoryAllocation ? PLIS_ERR_OOM : PLIS_ERR_CUDA;             \
+    }                                                                                    \
+  } while (0)
+
+constexpr int kStatBlocks = 256;
+
+Learner::~Learner() {
+  if (device_ >= 0) cudaSetDevice(device_);
+  for (void* p : allocs_) cudaFree(p);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+int Learner::dmalloc(void** p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+  if (e != cudaSuccess) {
+    err_ = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? PLIS_ERR_OOM : PLIS_ERR_CUDA;
+  }
+  allocs_.push_back(*p);
+  return PLIS_OK;
+}
+
+// He-uniform initialisation from a Philox stream, zero biases, identity feature statistics
+static void init_weights(std::vector<float>& w, uint64_t seed) {
+  w.assign(kNWeights, 0.f);
+  uint32_t ctr = 0;
+  auto uni = [&](void) {
+    plis_u32x4 c = {ctr++, 0x1417u, 0u, 0u};
+    const plis_u32x4 r = plis_philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    return ((double)(r.x >> 8) + 0.5) / 16777216.0;  // (0, 1)
+  };
+  auto fill = [&](int off, int fan_in, int count) {
+    const double a = std::sqrt(6.0 / fan_in);
+    for (int i = 0; i < count; ++i) w[off + i] = (float)((2.0 * uni() - 1.0) * a);
+  };
+  fill(kOffW1, kFeat, kFeat * kHid);
+  fill(kOffW2, kHid, kHid * kHid);
+  fill(kOffW3, kHid, kHid * kHid);
+  fill(kOffW4, kHid, kHid);
+  for (int k = 0; k < kFeat; ++k) w[kNParams + kFeat + k] = 1.f;
+}
+
+int Learner::create(uint64_t capacity, int device) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    err_ = "No CUDA-capable device detected.";
+    device_ = -1;
+    return PLIS_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= ndev) {
+    err_ = "device ordinal out of range";
+    device_ = -1;
+    return PLIS_ERR_INVALID;
+  }
+  device_ = device;
+  PLIS_LCU(cudaSetDevice(device));
+  PLIS_LCU(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  capacity_ = capacity;
+  int rc;
+  if ((rc = dmalloc((void**)&recs_, capacity * sizeof(TraceRec)))) return rc;
+  if ((rc = dmalloc((void**)&w_, kNWeights * sizeof(float)))) return rc;
+  if ((rc = dmalloc((void**)&m_, kNParams * sizeof(float)))) return rc;
+  if ((rc = dmalloc((void**)&v_, kNParams * sizeof(float)))) return rc;
+  if ((rc = dmalloc((void**)&stats_, (kStatBlocks * kStatN + 2) * sizeof(double)))) return rc;
+  if ((rc = dmalloc((void**)&packed_, sizeof(LearnedParams)))) return rc;
+  std::vector<float> w;
+  init_weights(w, 1);
+  PLIS_LCU(cudaMemcpy(w_, w.data(), kNWeights * sizeof(float), cudaMemcpyHostToDevice));
+  PLIS_LCU(cudaFuncSetAttribute(k_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrainSmem));
+  return PLIS_OK;
+}
+
+int Learner::ensure_train_buffers(uint32_t blocks) {
+  if (blocks <= partial_blocks_) return PLIS_OK;
+  int rc;
+  if ((rc = dmalloc((void**)&partial_, (size_t)blocks * kNParams * sizeof(float)))) return rc;
+  if ((rc = dmalloc((void**)&loss_, (size_t)blocks * sizeof(float)))) return rc;
+  partial_blocks_ = blocks;
+  return PLIS_OK;
+}
+
+int Learner::record(Engine& e, uint64_t n_steps, uint32_t stride) {
+  if (stride == 0) { err_ = "stride must be positive"; return PLIS_ERR_INVALID; }
+  PLIS_LCU(cudaSetDevice(device_));
+  const uint32_t N = e.model().N;
+  for (uint64_t k = 0; k < n_steps; ++k) {
+    const uint32_t offset = (uint32_t)(k % stride) % N;
+    const uint32_t cnt = (N - offset + stride - 1) / stride;
+    if (count_ + cnt > capacity_) break;
+    int rc = e.trace_features(recs_ + count_, offset, stride, cnt);
+    if (rc) { err_ = e.error(); return rc; }
+    plis_stats a, b;
+    e.stats(&a);
+    rc = e.advance(PLIS_INF_D, 1);
+    if (rc) { err_ = e.error(); return rc; }
+    e.stats(&b);
+    if (b.steps == a.steps) break;  // nothing can fire any more
+    rc = e.trace_label(recs_ + count_, cnt, b.time - a.time);
+    if (rc) { err_ = e.error(); return rc; }
+    count_ += cnt;
+  }
+  return PLIS_OK;
+}
+
+int Learner::get_records(uint64_t first, uint64_t n, void* out) {
+  if (first + n > count_) { err_ = "record range out of bounds"; return PLIS_ERR_INVALID; }
+  PLIS_LCU(cudaSetDevice(device_));
+  PLIS_LCU(cudaMemcpy(out, recs_ + first, n * sizeof(TraceRec), cudaMemcpyDeviceToHost));
+  return PLIS_OK;
+}
+
+int Learner::set_records(const void* recs, uint64_t n) {
+  if (n > capacity_) { err_ = "more records than the capacity"; return PLIS_ERR_INVALID; }
+  PLIS_LCU(cudaSetDevice(device_));
+  if (n) PLIS_LCU(cudaMemcpy(recs_, recs, n * sizeof(TraceRec), cudaMemcpyHostToDevice));
+  count_ = n;
+  return PLIS_OK;
+}
+
+int Learner::feature_stats() {
+  k_feat_partial<<<kStatBlocks, 256, 0, stream_>>>(recs_, count_, stats_);
+  k_feat_final<<<1, 32, 0, stream_>>>(stats_, kStatBlocks, w_, stats_ + kStatBlocks * kStatN);
+  PLIS_LCU(cudaGetLastError());
+  return PLIS_OK;
+}
+
+int Learner::train(const plis_train_params& p, plis_train_report* out) {
+  if (count_ == 0) { err_ = "no records"; return PLIS_ERR_INVALID; }
+  if (p.batch == 0 || p.batch % kTB) { err_ = "batch must be a positive multiple of 128"; return PLIS_ERR_INVALID; }
+  if (!(p.quantile > 0.f && p.quantile < 1.f)) { err_ = "quantile must be in (0, 1)"; return PLIS_ERR_INVALID; }
+  PLIS_LCU(cudaSetDevice(device_));
+  const uint32_t nblk = p.batch / kTB;
+  int rc = ensure_train_buffers(nblk);
+  if (rc) return rc;
+  // fresh parameters, then the statistics of these records
+  std::vector<float> w;
+  init_weights(w, p.seed);
+  PLIS_LCU(cudaMemcpyAsync(w_, w.data(), kNParams * sizeof(float), cudaMemcpyHostToDevice, stream_));
+  if ((rc = feature_stats())) return rc;
+  double st[2];
+  PLIS_LCU(cudaMemcpyAsync(st, stats_ + kStatBlocks * kStatN, sizeof st, cudaMemcpyDeviceToHost, stream_));
+  PLIS_LCU(cudaStreamSynchronize(stream_));
+  if (st[1] < 1.0) { err_ = "no usable records (every label is NaN)"; return PLIS_ERR_INVALID; }
+  const float b4 = (float)st[0];
+  PLIS_LCU(cudaMemcpyAsync(w_ + kOffB4, &b4, sizeof b4, cudaMemcpyHostToDevice, stream_));
+  PLIS_LCU(cudaMemsetAsync(m_, 0, kNParams * sizeof(float), stream_));
+  PLIS_LCU(cudaMemsetAsync(v_, 0, kNParams * sizeof(float), stream_));
+  cudaEvent_t e0, e1;
+  PLIS_LCU(cudaEventCreate(&e0));
+  PLIS_LCU(cudaEventCreate(&e1));
+  PLIS_LCU(cudaEventRecord(e0, stream_));
+  std::vector<float> lossbuf(nblk);
+  double loss_first = 0.0, loss_last = 0.0;
+  const float inv_b = 1.f / (float)p.batch;
+  double b1t = 1.0, b2t = 1.0;
+  for (uint64_t it = 0; it < p.iterations; ++it) {
+    k_train<<<nblk, kTB, kTrainSmem, stream_>>>(recs_, count_, w_, partial_, loss_, it, (uint32_t)p.seed,
+                                                 (uint32_t)(p.seed >> 32), p.quantile, 0, inv_b);
+    b1t *= 0.9;
+    b2t *= 0.999;
+    k_adam<<<(kNParams + 255) / 256, 256, 0, stream_>>>(w_, m_, v_, partial_, nblk, p.learning_rate,
+                                                         (float)(1.0 - b1t), (float)(1.0 - b2t), nullptr);
+    if (it == 0 || it + 1 == p.iterations) {
+      PLIS_LCU(cudaMemcpyAsync(lossbuf.data(), loss_, nblk * sizeof(float), cudaMemcpyDeviceToHost, stream_));
+      PLIS_LCU(cudaStreamSynchronize(stream_));
+      double s = 0.0;
+      for (float v : lossbuf) s += v;
+      (it == 0 ? loss_first : loss_last) = s / p.batch;
+      if (it == 0) loss_last = loss_first;
+    }
+  }
+  PLIS_LCU(cudaEventRecord(e1, stream_));
+  PLIS_LCU(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  PLIS_LCU(cudaGetLastError());
+  adam_t_ = p.iterations;
+  if (out) {
+    out->loss_first = loss_first;
+    out->loss_last = loss_last;
+    out->records = count_;
+    out->iterations = p.iterations;
+    out->device_ms = ms;
+  }
+  return PLIS_OK;
+}
+
+int Learner::gradient(float* grad, double* loss, float quantile) {
+  if (count_ == 0) { err_ = "no records"; return PLIS_ERR_INVALID; }
+  PLIS_LCU(cudaSetDevice(device_));
+  const uint32_t nblk = (uint32_t)((count_ + kTB - 1) / kTB);
+  int rc = ensure_train_buffers(nblk);
+  if (rc) return rc;
+  float* d_g = nullptr;
+  PLIS_LCU(cudaMalloc(&d_g, kNParams * sizeof(float)));
+  k_train<<<nblk, kTB, kTrainSmem, stream_>>>(recs_, count_, w_, partial_, loss_, 0, 0, 0, quantile, 1,
+                                               1.f / (float)count_);
+  k_adam<<<(kNParams + 255) / 256, 256, 0, stream_>>>(w_, m_, v_, partial_, nblk, 0.f, 1.f, 1.f, d_g);
+  std::vector<float> lossbuf(nblk);
+  cudaError_t e = cudaMemcpyAsync(grad, d_g, kNParams * sizeof(float), cudaMemcpyDeviceToHost, stream_);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(lossbuf.data(), loss_, nblk * sizeof(float), cudaMemcpyDeviceToHost, stream_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+  cudaFree(d_g);
+  if (e != cudaSuccess) { err_ = cudaGetErrorString(e); return PLIS_ERR_CUDA; }
+  double s = 0.0;
+  for (float v : lossbuf) s += v;
+  if (loss) *loss = s / (double)count_;
+  return PLIS_OK;
+}
+
+int Learner::predict(const float* features, uint64_t n, float* y) {
+  PLIS_LCU(cudaSetDevice(device_));
+  if (n == 0) return PLIS_OK;
+  float *d_f = nullptr, *d_y = nullptr;
+  PLIS_LCU(cudaMalloc(&d_f, n * kFeat * sizeof(float)));
+  cudaError_t e = cudaMalloc(&d_y, n * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_f, features, n * kFeat * sizeof(float), cudaMemcpyHostToDevice, stream_);
+  if (e == cudaSuccess) {
+    learned_pack(w_, 1.0, packed_, stream_);
+    k_predict<<<(unsigned)((n + 127) / 128), 128, 0, stream_>>>(packed_, d_f, n, d_y);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(y, d_y, n * sizeof(float), cudaMemcpyDeviceToHost, stream_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+  cudaFree(d_f);
+  if (d_y) cudaFree(d_y);
+  if (e != cudaSuccess) { err_ = cudaGetErrorString(e); return PLIS_ERR_CUDA; }
+  return PLIS_OK;
+}
+
+int Learner::get_weights(float* w) {
+  PLIS_LCU(cudaSetDevice(device_));
+  PLIS_LCU(cudaMemcpyAsync(w, w_, kNWeights * sizeof(float), cudaMemcpyDeviceToHost, stream_));
+  PLIS_LCU(cudaStreamSynchronize(stream_));
+  return PLIS_OK;
+}
+
+int Learner::set_weights(const float* w) {
+  PLIS_LCU(cudaSetDevice(device_));
+  PLIS_LCU(cudaMemcpyAsync(w_, w, kNWeights * sizeof(float), cudaMemcpyHostToDevice, stream_));
+  PLIS_LCU(cudaStreamSynchronize(stream_));
+  return PLIS_OK;
+}
+
+}  // namespace plis

@@ -1,0 +1,169 @@
+"""Learned tau proposals: trace recording, training and deployment (plis_learner_* and
+plis_set_proposer in include/plis.h).
+
+    from pliscuda_b200 import Simulation, workloads
+    from pliscuda_b200.learned import Learner, calibrate
+
+    model, state = workloads.schlogl(64)
+    with Simulation(model, mode="corrected", seed=1) as sim, Learner(12_000_000) as L:
+        sim.set_state(state)
+        L.record(sim, n_steps=40)          # 40 plain steps x 262,144 subvolumes = 1.05e7 records
+        L.train(iterations=2000)
+        weights = L.weights()
+    s_max, table = calibrate(model, state, weights)   # largest clamp that keeps KS <= bound
+    with Simulation(big_model, mode="corrected") as sim:
+        sim.set_state(big_state)
+        sim.set_proposer(weights, s_max)
+        sim.run(20.0)
+
+The plain method is the judge of a proposer's error: calibrate() runs the plain method and the
+proposer side by side to the same checkpoints and keeps the largest clamp s_max of a ladder whose
+marginal distributions stay within the KS bound; with none, s_max = 1 (the plain method).
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Dict, Iterable, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import Model, Simulation, _c, _check, _lib
+
+TRACE_DTYPE = _lib.TRACE_DTYPE
+N_WEIGHTS = _lib.PROPOSER_WEIGHTS
+N_PARAMS = 8961
+
+
+class Learner:
+    """Trace buffer of up to `capacity` records and an MLP proposer on one device."""
+
+    def __init__(self, capacity: int, device: int = 0):
+        self._h = ctypes.c_void_p()
+        _check(_lib.lib.plis_learner_create(int(capacity), int(device), ctypes.byref(self._h)))
+
+    def close(self) -> None:
+        if self._h:
+            _lib.lib.plis_learner_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def record(self, sim: Simulation, n_steps: int, stride: int = 1) -> int:
+        """n_steps plain steps of sim (corrected mode), recording every stride-th subvolume of each
+        state; returns the number of records added (stops early when the buffer is full)."""
+        before = self.count
+        _check(_lib.lib.plis_learner_record(self._h, sim._h, int(n_steps), int(stride)))
+        return self.count - before
+
+    @property
+    def count(self) -> int:
+        n = ctypes.c_uint64()
+        _check(_lib.lib.plis_learner_count(self._h, ctypes.byref(n)))
+        return int(n.value)
+
+    def records(self, first: int = 0, n: Optional[int] = None) -> np.ndarray:
+        if n is None:
+            n = self.count - first
+        out = np.empty(n, dtype=TRACE_DTYPE)
+        _check(_lib.lib.plis_learner_get_records(self._h, int(first), int(n), _c(out)))
+        return out
+
+    def set_records(self, recs: np.ndarray) -> None:
+        r = np.ascontiguousarray(recs, dtype=TRACE_DTYPE)
+        _check(_lib.lib.plis_learner_set_records(self._h, _c(r), int(r.size)))
+
+    def train(self, iterations: int = 2000, batch: int = 16384, learning_rate: float = 1e-3,
+              quantile: float = 0.25, seed: int = 1) -> Dict[str, float]:
+        p = _lib.TrainParams()
+        _lib.lib.plis_train_params_init(ctypes.byref(p))
+        p.iterations, p.batch, p.learning_rate, p.quantile, p.seed = iterations, batch, learning_rate, quantile, seed
+        rep = _lib.TrainReport()
+        _check(_lib.lib.plis_learner_train(self._h, ctypes.byref(p), ctypes.byref(rep)))
+        return {"loss_first": rep.loss_first, "loss_last": rep.loss_last, "records": int(rep.records),
+                "iterations": int(rep.iterations), "device_ms": rep.device_ms}
+
+    def gradient(self, quantile: float = 0.25) -> Tuple[np.ndarray, float]:
+        """Mean pinball loss over all records and its gradient w.r.t. the 8961 parameters."""
+        g = np.empty(N_PARAMS, np.float32)
+        loss = ctypes.c_double()
+        _check(_lib.lib.plis_learner_gradient(self._h, float(quantile), _c(g), ctypes.byref(loss)))
+        return g, float(loss.value)
+
+    def predict(self, features: np.ndarray) -> np.ndarray:
+        f = np.ascontiguousarray(features, dtype=np.float32).reshape(-1, 8)
+        y = np.empty(f.shape[0], np.float32)
+        _check(_lib.lib.plis_learner_predict(self._h, _c(f), int(f.shape[0]), _c(y)))
+        return y
+
+    def weights(self) -> np.ndarray:
+        w = np.empty(N_WEIGHTS, np.float32)
+        _check(_lib.lib.plis_learner_get_weights(self._h, _c(w)))
+        return w
+
+    def set_weights(self, w: np.ndarray) -> None:
+        a = np.ascontiguousarray(w, dtype=np.float32).reshape(-1)
+        if a.size != N_WEIGHTS:
+            raise ValueError(f"expected {N_WEIGHTS} floats")
+        _check(_lib.lib.plis_learner_set_weights(self._h, _c(a)))
+
+
+def ks_distance(a: np.ndarray, b: np.ndarray) -> float:
+    """Two-sample Kolmogorov-Smirnov distance of integer samples."""
+    a = np.sort(np.asarray(a).ravel())
+    b = np.sort(np.asarray(b).ravel())
+    v = np.union1d(a, b)
+    fa = np.searchsorted(a, v, side="right") / a.size
+    fb = np.searchsorted(b, v, side="right") / b.size
+    return float(np.max(np.abs(fa - fb)))
+
+
+def compare(model: Model, state: np.ndarray, weights: np.ndarray, s_max: float, checkpoints: Sequence[float], *,
+            precision: str = "fp64", seeds: Tuple[int, int] = (101, 202), device: int = 0) -> Dict:
+    """Plain method and proposer (corrected mode, independent seeds) from the same state to each
+    checkpoint.  Per checkpoint: the largest KS distance over species of the pooled subvolume
+    counts.  Totals: steps, events, rollbacks and device time of each run."""
+    S, N = model.n_species, model.n_subvolumes
+    snaps = {}
+    totals = {}
+    for name, seed in (("plain", seeds[0]), ("learned", seeds[1])):
+        with Simulation(model, mode="corrected", precision=precision, seed=seed, device=device) as sim:
+            sim.set_state(state)
+            if name == "learned":
+                sim.set_proposer(weights, s_max)
+            out = []
+            for t in checkpoints:
+                sim.run(float(t))
+                out.append(sim.get_state().reshape(S, N).copy())
+            st = sim.stats()
+            totals[name] = {"steps": int(st.steps), "events": int(st.events), "rollbacks": int(st.rollbacks),
+                            "device_ms": float(st.device_ms), "time": float(st.time)}
+            snaps[name] = out
+    ks = []
+    for k in range(len(checkpoints)):
+        ks.append(max(ks_distance(snaps["plain"][k][s], snaps["learned"][k][s]) for s in range(S)))
+    return {"s_max": float(s_max), "checkpoints": [float(t) for t in checkpoints], "ks": ks, "ks_max": max(ks),
+            "plain": totals["plain"], "learned": totals["learned"]}
+
+
+def calibrate(model: Model, state: np.ndarray, weights: np.ndarray, *, ladder: Iterable[float] = (16, 8, 4, 2),
+              checkpoints: Sequence[float] = (1.0, 2.0, 3.0, 4.0, 5.0), bound: float = 0.02, margin: float = 0.75,
+              precision: str = "fp64", device: int = 0) -> Tuple[float, list]:
+    """Largest clamp of the ladder whose proposals keep the KS distance to the plain method within
+    margin * bound at every checkpoint; 1.0 (the plain method) when none does."""
+    table = []
+    for s in sorted(ladder, reverse=True):
+        rep = compare(model, state, weights, s, checkpoints, precision=precision, device=device)
+        table.append(rep)
+        if rep["ks_max"] <= margin * bound:
+            return float(s), table
+    return 1.0, table

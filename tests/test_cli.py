@@ -99,10 +99,11 @@ def test_cli_matches_the_library_bit_for_bit(tmp_path):
         for x, t in snaps:
             target = min(sim.stats().time + 0.25, 1.0)
             st = sim.run(target)
-            assert np.float32(st.time) == np.float32(t)
+            assert "%f" % float(np.float32(st.time)) == "%f" % t  # the .dat header prints time with %f
             assert np.array_equal(sim.get_state().reshape(x.shape).astype(np.int64), x)
     times = [t for _, t in snaps]
-    assert all(b - a >= 0.25 - 1e-6 for a, b in zip(times, times[1:]))
+    inner = times[:-1]  # the final snapshot closes the run at end time, whatever the gap
+    assert all(b - a >= 0.25 - 1e-6 for a, b in zip(inner, inner[1:]))
     assert times[-1] >= 1.0
 
 
