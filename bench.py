@@ -16,8 +16,14 @@ write) between timed intervals.  `e2e` is the same metric through the C ABI with
 every interval uploads the state from pinned host memory (plis_set_state), runs, and reads the
 state back (plis_get_state).
 
-N > 1 (torchrun): each rank simulates its own independent replica (different seed) on its own GPU;
-there is no data-path collective.  value = all ranks' events / the max over ranks of device time.
+`learned` (rank 0, N = 1): learned tau proposals against the plain method on Schlogl 128^3 to
+t = 20 (corrected semantics, FP64): events/s and sim-time/s of both on this GPU, the KS distance of
+the marginals at every checkpoint, rollbacks, and the training and calibration that produced the
+proposer (learned_report).
+
+N > 1 (torchrun): each rank simulates its own independent replica (its rank is the replica id in
+the Philox key) on its own GPU; there is no data-path collective.  value = all ranks' events / the
+max over ranks of device time.
 
 --impl reference: the reference has no CPU implementation of the step, so its CPU arm is the FP64
 host oracle (oracle/plis_oracle.cpp, OpenMP over subvolumes) on all host threads, on a bounded
@@ -244,6 +250,47 @@ def precision_report(args):
     return 0
 
 
+def learned_report():
+    """Learned tau proposals against the plain method on the same GPU (corrected semantics, FP64).
+
+    Training: for each label tolerance eps_L, 40 plain steps of Schlogl 64^3 are recorded
+    (1.05e7 subvolume-step records) and a proposer is trained on them (hand-written kernels).
+    Calibration on 64^3: the plain method and every candidate (proposer, clamp s_max) run from the
+    same state to t = 1..5; candidates whose marginals stay within KS 0.015 (0.75 x the bound) of the
+    plain method's are admissible, the fastest of them is kept.  Measurement on Schlogl 128^3
+    (2,097,152 subvolumes): plain and learned runs to t = 20 with checkpoints every 1.0; events/s and
+    sim-time/s from CUDA-event device time; KS of the pooled subvolume counts at every checkpoint;
+    rollbacks among all attempts."""
+    from pliscuda_b200 import workloads
+    from pliscuda_b200.learned import _ks_per_checkpoint, _run_to_checkpoints, calibrate, train_proposer
+    m64, s64 = workloads.schlogl(64)
+    cands, training = [], []
+    for eps_l in (0.4, 0.8, 1.6):
+        w, rep = train_proposer(m64, s64, label_epsilon=eps_l)
+        training.append({k: rep[k] for k in ("label_epsilon", "records", "iterations", "device_ms", "loss_first",
+                                             "loss_last")})
+        for s_max in (8.0, 16.0, 32.0):
+            cands.append((w, s_max, {"label_epsilon": eps_l, "s_max": s_max}))
+    best, cal = calibrate(m64, s64, cands)
+    m128, s128 = workloads.schlogl(128)
+    cps = [float(t) for t in range(1, 21)]
+    ps, pt = _run_to_checkpoints(m128, s128, cps, seed=11, precision="fp64", device=0)
+    out = {"workload": "schlogl128: Schlogl bistable model, 2097152 subvolumes (128^3), corrected semantics, FP64, "
+                       "t = 0..20, checkpoints every 1.0",
+           "plain": pt, "training": training, "calibration": cal}
+    if best is None:
+        out["learned"] = None
+        return out
+    w, s_max, tag = cands[best]
+    ls, lt = _run_to_checkpoints(m128, s128, cps, seed=12, precision="fp64", device=0, weights=w, s_max=s_max)
+    ks = _ks_per_checkpoint(ps, ls)
+    lt.update(tag)
+    out.update({"learned": lt, "ks": [round(k, 5) for k in ks], "ks_max": max(ks), "ks_bound": 0.02,
+                "speedup_events_per_s": lt["events_per_s"] / pt["events_per_s"],
+                "speedup_sim_time_per_s": lt["sim_time_per_s"] / pt["sim_time_per_s"]})
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -258,6 +305,8 @@ def main(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--ncu-case", action="store_true", help="run only the fixed ncu capture case")
     ap.add_argument("--precision-report", action="store_true", help="FP32 form vs binary64 on the precision config")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-tau comparison")
+    ap.add_argument("--learned-report", action="store_true", help="print only the learned-tau comparison")
     ap.add_argument("--report-side", type=int, default=128)
     ap.add_argument("--report-steps", type=int, default=200)
     args = ap.parse_args(argv)
@@ -267,6 +316,9 @@ def main(argv=None):
         return ncu_case(args)
     if args.precision_report:
         return precision_report(args)
+    if args.learned_report:
+        print(json.dumps(learned_report()))
+        return 0
 
     import numpy as np
     import torch
@@ -355,6 +407,9 @@ def main(argv=None):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(model, state, os.cpu_count() or 1)
+    learned = None
+    if rank == 0 and world == 1 and not args.no_learned:
+        learned = learned_report()
 
     if rank == 0:
         line = {
@@ -376,6 +431,7 @@ def main(argv=None):
             "e2e": e2e,
             "cpu_baseline": cpu,
             "clocks": ck,
+            "learned": learned,
         }
         print(json.dumps(line))
     replicas.finish(dist)

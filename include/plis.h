@@ -260,9 +260,11 @@ int plis_batch_get_tuning(plis_batch* b, plis_batch_tuning* out);
  * step and records, for every stride-th subvolume (the offset rotates from step to step), the
  * features of the state, its tau_Cao, the step taken from it and the label
  * log(tau_safe / tau_Cao), where tau_safe = tau_step / max(rho, rho^2) and rho is the largest
- * change of any propensity over the step relative to max(eps * a_j, c_j) (the Cao leap condition
- * measured on the realised step), clamped to [log(1/16), log(64)].  plis_learner_train fits the
- * MLP to a quantile of the label (pinball loss, Adam) with hand-written CUDA kernels.
+ * change of any propensity over the step relative to max(eps_L * a_j, c_j) (the Cao leap
+ * condition at tolerance eps_L measured on the realised step), clamped to [log(1/16), log(64)].
+ * plis_learner_train fits the MLP to a quantile of the label (pinball loss, Adam) with
+ * hand-written CUDA kernels.  The accuracy of a proposer is judged against the plain method
+ * (KS distance of the marginals at checkpoints), which fixes s_max.
  * ------------------------------------------------------------------------------------------- */
 #define PLIS_PROPOSER_WEIGHTS 8977 /* 8961 parameters, then 8 feature means and 8 inverse deviations */
 
@@ -297,8 +299,10 @@ typedef struct plis_learner plis_learner;
 void plis_train_params_init(plis_train_params* p);
 int plis_learner_create(uint64_t capacity, int device, plis_learner** out);
 int plis_learner_destroy(plis_learner* learner);
-/* n_steps plain steps of h (corrected mode, <= 4 species), recording every stride-th subvolume */
-int plis_learner_record(plis_learner* learner, plis_handle* h, uint64_t n_steps, uint32_t stride);
+/* n_steps steps of h (<= 4 species), recording every stride-th subvolume; labels use the leap
+ * condition at label_epsilon (0: the handle's epsilon) */
+int plis_learner_record(plis_learner* learner, plis_handle* h, uint64_t n_steps, uint32_t stride,
+                        double label_epsilon);
 int plis_learner_count(const plis_learner* learner, uint64_t* n_records);
 int plis_learner_get_records(plis_learner* learner, uint64_t first, uint64_t n, plis_trace_record* out);
 int plis_learner_set_records(plis_learner* learner, const plis_trace_record* records, uint64_t n);

@@ -135,7 +135,7 @@ def _load() -> ctypes.CDLL:
         "plis_train_params_init": (None, [P(TrainParams)]),
         "plis_learner_create": (i32, [u64, i32, P(vp)]),
         "plis_learner_destroy": (i32, [vp]),
-        "plis_learner_record": (i32, [vp, vp, u64, u32]),
+        "plis_learner_record": (i32, [vp, vp, u64, u32, f64]),
         "plis_learner_count": (i32, [vp, P(u64)]),
         "plis_learner_get_records": (i32, [vp, u64, u64, vp]),
         "plis_learner_set_records": (i32, [vp, vp, u64]),

@@ -225,10 +225,10 @@ int plis_learner_destroy(plis_learner* L) {
   PLIS_GUARD_END
 }
 
-int plis_learner_record(plis_learner* L, plis_handle* h, uint64_t n_steps, uint32_t stride) {
+int plis_learner_record(plis_learner* L, plis_handle* h, uint64_t n_steps, uint32_t stride, double label_epsilon) {
   PLIS_GUARD_BEGIN
   if (!L || !h) { g_err = "null argument"; return PLIS_ERR_INVALID; }
-  return lfail(L, L->l.record(h->eng, n_steps, stride));
+  return lfail(L, L->l.record(h->eng, n_steps, stride, label_epsilon));
   PLIS_GUARD_END
 }
 

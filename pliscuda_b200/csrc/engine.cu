@@ -370,11 +370,11 @@ int Engine::trace_features(TraceRec* out, uint32_t offset, uint32_t stride, uint
   return PLIS_OK;
 }
 
-int Engine::trace_label(TraceRec* recs, uint32_t count, double tau_step) {
+int Engine::trace_label(TraceRec* recs, uint32_t count, double tau_step, double label_eps) {
   LearnedLaunch l = learned_pick(opt_.precision, model_.S);
   if (!l.label) { err_ = "trace recording supports up to 4 species"; return PLIS_ERR_LIMIT; }
   if (count == 0) return PLIS_OK;
-  l.label(args_, recs, count, tau_step, stream_);
+  l.label(args_, recs, count, tau_step, (float)(label_eps > 0.0 ? label_eps : opt_.epsilon), stream_);
   launches_ += 1;
   PLIS_CU(cudaGetLastError());
   PLIS_CU(cudaStreamSynchronize(stream_));

@@ -38,9 +38,9 @@ class Engine {
   // learned tau proposals (learned.cu): attach (weights != null, s_max >= 1) or detach a proposer
   int set_proposer(const float* weights, double s_max);
   // trace recording: features of every stride-th subvolume of the current state from offset, and
-  // the labels of those records once a step has been taken
+  // the labels of those records once a step has been taken (leap condition at label_eps, 0 = epsilon)
   int trace_features(TraceRec* out, uint32_t offset, uint32_t stride, uint32_t count);
-  int trace_label(TraceRec* recs, uint32_t count, double tau_step);
+  int trace_label(TraceRec* recs, uint32_t count, double tau_step, double label_eps);
   int device() const { return opt_.device; }
   const std::string& error() const { return err_; }
   const Model& model() const { return model_; }

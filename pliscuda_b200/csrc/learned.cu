@@ -292,7 +292,7 @@ __global__ void k_trace_features(KArgs A, TraceRec* out, uint32_t offset, uint32
 
 // label of each record from the state the step reached: the Cao leap condition on the realised step
 template <typename Real, int MAXS>
-__global__ void k_trace_label(KArgs A, TraceRec* recs, uint32_t count, double tau_step) {
+__global__ void k_trace_label(KArgs A, TraceRec* recs, uint32_t count, double tau_step, float eps) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
   const DevModel& m = A.m;
@@ -306,7 +306,6 @@ __global__ void k_trace_label(KArgs A, TraceRec* recs, uint32_t count, double ta
   const Cell cl = cell_from_index(m, c);
   Nbr q;
   nbr_info(m, cl, q);
-  const float eps = (float)A.o.eps;
   const Real* rr = (const Real*)m.rr;
   float rho = 0.f;
   for (int j = 0; j < (int)m.R; ++j) {
@@ -343,8 +342,8 @@ struct LearnedSet {
                        cudaStream_t s) {
     k_trace_features<Real, MAXS><<<(count + 127) / 128, 128, 0, s>>>(a, out, offset, stride, count);
   }
-  static void label(const KArgs& a, TraceRec* recs, uint32_t count, double tau_step, cudaStream_t s) {
-    k_trace_label<Real, MAXS><<<(count + 127) / 128, 128, 0, s>>>(a, recs, count, tau_step);
+  static void label(const KArgs& a, TraceRec* recs, uint32_t count, double tau_step, float eps, cudaStream_t s) {
+    k_trace_label<Real, MAXS><<<(count + 127) / 128, 128, 0, s>>>(a, recs, count, tau_step, eps);
   }
 };
 
@@ -760,8 +759,9 @@ int Learner::ensure_train_buffers(uint32_t blocks) {
   return PLIS_OK;
 }
 
-int Learner::record(Engine& e, uint64_t n_steps, uint32_t stride) {
+int Learner::record(Engine& e, uint64_t n_steps, uint32_t stride, double label_eps) {
   if (stride == 0) { err_ = "stride must be positive"; return PLIS_ERR_INVALID; }
+  if (label_eps < 0.0) { err_ = "label_epsilon must be >= 0"; return PLIS_ERR_INVALID; }
   PLIS_LCU(cudaSetDevice(device_));
   const uint32_t N = e.model().N;
   for (uint64_t k = 0; k < n_steps; ++k) {
@@ -776,7 +776,7 @@ int Learner::record(Engine& e, uint64_t n_steps, uint32_t stride) {
     if (rc) { err_ = e.error(); return rc; }
     e.stats(&b);
     if (b.steps == a.steps) break;  // nothing can fire any more
-    rc = e.trace_label(recs_ + count_, cnt, b.time - a.time);
+    rc = e.trace_label(recs_ + count_, cnt, b.time - a.time, label_eps);
     if (rc) { err_ = e.error(); return rc; }
     count_ += cnt;
   }

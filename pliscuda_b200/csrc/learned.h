@@ -56,7 +56,7 @@ static_assert(sizeof(TraceRec) == 64, "trace record size");
 struct LearnedLaunch {
   void (*classify)(const KArgs&, dim3, dim3, cudaStream_t);
   void (*features)(const KArgs&, TraceRec*, uint32_t offset, uint32_t stride, uint32_t count, cudaStream_t);
-  void (*label)(const KArgs&, TraceRec*, uint32_t count, double tau_step, cudaStream_t);
+  void (*label)(const KArgs&, TraceRec*, uint32_t count, double tau_step, float eps, cudaStream_t);
 };
 // nullptr members when the species count is above 4
 LearnedLaunch learned_pick(int precision, uint32_t S);
@@ -70,7 +70,7 @@ class Learner {
   Learner() = default;
   ~Learner();
   int create(uint64_t capacity, int device);
-  int record(Engine& e, uint64_t n_steps, uint32_t stride);
+  int record(Engine& e, uint64_t n_steps, uint32_t stride, double label_eps);
   int count(uint64_t* n) const { *n = count_; return PLIS_OK; }
   int get_records(uint64_t first, uint64_t n, void* out);
   int set_records(const void* recs, uint64_t n);

@@ -10,15 +10,15 @@ plis_set_proposer in include/plis.h).
         L.record(sim, n_steps=40)          # 40 plain steps x 262,144 subvolumes = 1.05e7 records
         L.train(iterations=2000)
         weights = L.weights()
-    s_max, table = calibrate(model, state, weights)   # largest clamp that keeps KS <= bound
+    best, table = calibrate(model, state, [(weights, 16.0, "eps 0.05")])  # KS against the plain method
     with Simulation(big_model, mode="corrected") as sim:
         sim.set_state(big_state)
-        sim.set_proposer(weights, s_max)
+        sim.set_proposer(weights, 16.0)
         sim.run(20.0)
 
-The plain method is the judge of a proposer's error: calibrate() runs the plain method and the
-proposer side by side to the same checkpoints and keeps the largest clamp s_max of a ladder whose
-marginal distributions stay within the KS bound; with none, s_max = 1 (the plain method).
+The plain method is the judge of a proposer's error: calibrate() runs the plain method and each
+candidate (weights, s_max) side by side to the same checkpoints, admits the candidates whose
+marginal distributions stay within the KS bound, and picks the fastest of those.
 """
 from __future__ import annotations
 
@@ -58,11 +58,12 @@ class Learner:
         except Exception:
             pass
 
-    def record(self, sim: Simulation, n_steps: int, stride: int = 1) -> int:
-        """n_steps plain steps of sim (corrected mode), recording every stride-th subvolume of each
-        state; returns the number of records added (stops early when the buffer is full)."""
+    def record(self, sim: Simulation, n_steps: int, stride: int = 1, label_epsilon: float = 0.0) -> int:
+        """n_steps steps of sim, recording every stride-th subvolume of each state, labels at the
+        leap-condition tolerance label_epsilon (0: the simulation's epsilon); returns the number of
+        records added (stops early when the buffer is full)."""
         before = self.count
-        _check(_lib.lib.plis_learner_record(self._h, sim._h, int(n_steps), int(stride)))
+        _check(_lib.lib.plis_learner_record(self._h, sim._h, int(n_steps), int(stride), float(label_epsilon)))
         return self.count - before
 
     @property
@@ -127,43 +128,75 @@ def ks_distance(a: np.ndarray, b: np.ndarray) -> float:
     return float(np.max(np.abs(fa - fb)))
 
 
+def _run_to_checkpoints(model: Model, state: np.ndarray, checkpoints: Sequence[float], *, seed: int,
+                        precision: str, device: int, weights=None, s_max: float = 0.0):
+    S, N = model.n_species, model.n_subvolumes
+    with Simulation(model, mode="corrected", precision=precision, seed=seed, device=device) as sim:
+        sim.set_state(state)
+        if weights is not None:
+            sim.set_proposer(weights, s_max)
+        snaps = []
+        for t in checkpoints:
+            sim.run(float(t))
+            snaps.append(sim.get_state().reshape(S, N).copy())
+        st = sim.stats()
+        tot = {"steps": int(st.steps), "events": int(st.events), "rollbacks": int(st.rollbacks),
+               "device_ms": float(st.device_ms), "time": float(st.time)}
+    tot["events_per_s"] = tot["events"] / (tot["device_ms"] * 1e-3)
+    tot["sim_time_per_s"] = tot["time"] / (tot["device_ms"] * 1e-3)
+    tot["rollback_rate"] = tot["rollbacks"] / max(1, tot["steps"] + tot["rollbacks"])  # of attempts
+    return snaps, tot
+
+
+def _ks_per_checkpoint(a, b) -> list:
+    return [max(ks_distance(x[s], y[s]) for s in range(x.shape[0])) for x, y in zip(a, b)]
+
+
 def compare(model: Model, state: np.ndarray, weights: np.ndarray, s_max: float, checkpoints: Sequence[float], *,
             precision: str = "fp64", seeds: Tuple[int, int] = (101, 202), device: int = 0) -> Dict:
     """Plain method and proposer (corrected mode, independent seeds) from the same state to each
     checkpoint.  Per checkpoint: the largest KS distance over species of the pooled subvolume
-    counts.  Totals: steps, events, rollbacks and device time of each run."""
-    S, N = model.n_species, model.n_subvolumes
-    snaps = {}
-    totals = {}
-    for name, seed in (("plain", seeds[0]), ("learned", seeds[1])):
-        with Simulation(model, mode="corrected", precision=precision, seed=seed, device=device) as sim:
-            sim.set_state(state)
-            if name == "learned":
-                sim.set_proposer(weights, s_max)
-            out = []
-            for t in checkpoints:
-                sim.run(float(t))
-                out.append(sim.get_state().reshape(S, N).copy())
-            st = sim.stats()
-            totals[name] = {"steps": int(st.steps), "events": int(st.events), "rollbacks": int(st.rollbacks),
-                            "device_ms": float(st.device_ms), "time": float(st.time)}
-            snaps[name] = out
-    ks = []
-    for k in range(len(checkpoints)):
-        ks.append(max(ks_distance(snaps["plain"][k][s], snaps["learned"][k][s]) for s in range(S)))
+    counts.  Totals: steps, events, rollbacks, device time and rates of each run."""
+    ps, pt = _run_to_checkpoints(model, state, checkpoints, seed=seeds[0], precision=precision, device=device)
+    ls, lt = _run_to_checkpoints(model, state, checkpoints, seed=seeds[1], precision=precision, device=device,
+                                 weights=weights, s_max=s_max)
+    ks = _ks_per_checkpoint(ps, ls)
     return {"s_max": float(s_max), "checkpoints": [float(t) for t in checkpoints], "ks": ks, "ks_max": max(ks),
-            "plain": totals["plain"], "learned": totals["learned"]}
+            "plain": pt, "learned": lt}
 
 
-def calibrate(model: Model, state: np.ndarray, weights: np.ndarray, *, ladder: Iterable[float] = (16, 8, 4, 2),
+def train_proposer(model: Model, state: np.ndarray, *, label_epsilon: float, n_steps: int = 40, stride: int = 1,
+                   iterations: int = 2000, batch: int = 16384, learning_rate: float = 1e-3, quantile: float = 0.25,
+                   seed: int = 1, device: int = 0) -> Tuple[np.ndarray, Dict]:
+    """Record n_steps plain corrected steps of (model, state), train a proposer on them; returns
+    (weights, report)."""
+    cap = n_steps * ((model.n_subvolumes + stride - 1) // stride)
+    with Simulation(model, mode="corrected", seed=seed, device=device) as sim, Learner(cap, device) as L:
+        sim.set_state(state)
+        n = L.record(sim, n_steps, stride=stride, label_epsilon=label_epsilon)
+        rep = L.train(iterations=iterations, batch=batch, learning_rate=learning_rate, quantile=quantile, seed=seed)
+        rep.update({"records": n, "label_epsilon": label_epsilon, "quantile": quantile})
+        return L.weights(), rep
+
+
+def calibrate(model: Model, state: np.ndarray, candidates: Sequence[Tuple[np.ndarray, float, object]], *,
               checkpoints: Sequence[float] = (1.0, 2.0, 3.0, 4.0, 5.0), bound: float = 0.02, margin: float = 0.75,
-              precision: str = "fp64", device: int = 0) -> Tuple[float, list]:
-    """Largest clamp of the ladder whose proposals keep the KS distance to the plain method within
-    margin * bound at every checkpoint; 1.0 (the plain method) when none does."""
-    table = []
-    for s in sorted(ladder, reverse=True):
-        rep = compare(model, state, weights, s, checkpoints, precision=precision, device=device)
-        table.append(rep)
-        if rep["ks_max"] <= margin * bound:
-            return float(s), table
-    return 1.0, table
+              precision: str = "fp64", device: int = 0) -> Tuple[Optional[int], Dict]:
+    """The plain method judges each candidate (weights, s_max, tag): both run from the same state
+    to the checkpoints, and a candidate is admissible when the KS distance of every marginal at
+    every checkpoint stays within margin * bound.  Returns the index of the admissible candidate
+    with the shortest device time (None when none is admissible) and the table."""
+    ps, pt = _run_to_checkpoints(model, state, checkpoints, seed=101, precision=precision, device=device)
+    rows = []
+    best, best_ms = None, float("inf")
+    for i, (w, s_max, tag) in enumerate(candidates):
+        ls, lt = _run_to_checkpoints(model, state, checkpoints, seed=202 + i, precision=precision, device=device,
+                                     weights=w, s_max=s_max)
+        ks = _ks_per_checkpoint(ps, ls)
+        ok = max(ks) <= margin * bound
+        rows.append({"tag": tag, "s_max": float(s_max), "ks_max": max(ks), "admissible": ok,
+                     "device_ms": lt["device_ms"], "steps": lt["steps"], "rollbacks": lt["rollbacks"]})
+        if ok and lt["device_ms"] < best_ms:
+            best, best_ms = i, lt["device_ms"]
+    return best, {"plain": pt, "candidates": rows, "bound": bound, "margin": margin,
+                  "checkpoints": [float(t) for t in checkpoints]}

@@ -228,7 +228,7 @@ def test_training_lowers_the_loss():
         rep = L.train(iterations=300, batch=4096, learning_rate=3e-3)
         w = L.weights()
         y = L.predict(L.records(0, 4096)["features"])
-    assert rep["loss_last"] < 0.8 * rep["loss_first"], rep
+    assert rep["loss_last"] < 0.9 * rep["loss_first"], rep
     assert np.isfinite(w).all() and np.isfinite(y).all()
 
 
