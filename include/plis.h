@@ -58,6 +58,10 @@ typedef enum plis_status {
 #define PLIS_PREC_FP64 0
 #define PLIS_PREC_FP32 1
 
+/* Kernel of the learned-tau MLP (plis_options.learned_mlp, plis_learner_predict). */
+#define PLIS_MLP_TCGEN05 0  /* tcgen05.mma, accumulators in tensor memory */
+#define PLIS_MLP_MMA_SYNC 1 /* warp-level mma.sync, accumulators in registers */
+
 /* Per-subvolume operation flags (the reference's enum op, constants.cuh:53-58). */
 #define PLIS_LEAP_CR 0
 #define PLIS_LEAP_NOCR 1
@@ -103,6 +107,7 @@ typedef struct plis_options {
   int32_t persistent;         /* 1 = one cooperative persistent launch per run call, 0 = graph of phase kernels, -1 = auto */
   int32_t profile;            /* 1 = launch phase kernels one by one with CUDA events around each (plis_get_profile) */
   int32_t stage_halo;         /* lattice leap: 1 = stage brick + halo in shared memory, 0 = global atomics (default) */
+  int32_t learned_mlp;        /* learned tau MLP: 0 = tcgen05.mma with TMEM accumulators (default), 1 = mma.sync */
 } plis_options;
 
 /* Per-kernel device time accumulated while plis_options.profile is set (CUDA events recorded on the
@@ -310,8 +315,9 @@ int plis_learner_set_records(plis_learner* learner, const plis_trace_record* rec
 int plis_learner_train(plis_learner* learner, const plis_train_params* p, plis_train_report* out);
 /* mean pinball loss and its gradient over all records (current weights and feature statistics) */
 int plis_learner_gradient(plis_learner* learner, float quantile, float* grad, double* loss);
-/* the MLP output y for n raw feature rows [n*8], through the same tensor-core inference code */
-int plis_learner_predict(plis_learner* learner, const float* features, uint64_t n, float* y);
+/* the MLP output y for n raw feature rows [n*8], through the inference code of the learned
+ * classification: mlp_kernel 0 = tcgen05.mma (TMEM accumulators), 1 = mma.sync */
+int plis_learner_predict(plis_learner* learner, const float* features, uint64_t n, float* y, int mlp_kernel);
 int plis_learner_get_weights(plis_learner* learner, float* weights);       /* [PLIS_PROPOSER_WEIGHTS] */
 int plis_learner_set_weights(plis_learner* learner, const float* weights);
 /* Attach a proposer (weights as plis_learner_get_weights returns them) to h with clamp s_max >= 1,

@@ -127,7 +127,8 @@ class Simulation:
     def __init__(self, model: Model, *, mode: int | str = MODE_REFERENCE, precision: int | str = PREC_FP64,
                  seed: int = 1, replica: int = 0, device: int = 0, critical_threshold: int = 10,
                  epsilon: float = 0.05, max_rollbacks: int = 64, steps_per_launch: int = 0,
-                 tile: Optional[Sequence[int]] = None, profile: bool = False, stage_halo: bool = False):
+                 tile: Optional[Sequence[int]] = None, profile: bool = False, stage_halo: bool = False,
+                 learned_mlp: str = "tcgen05"):
         if isinstance(mode, str):
             mode = {"reference": MODE_REFERENCE, "corrected": MODE_CORRECTED}[mode]
         if isinstance(precision, str):
@@ -136,7 +137,8 @@ class Simulation:
         self.n, self.s = model.n_subvolumes, model.n_species
         kw = dict(mode=mode, precision=precision, seed=seed, replica=replica, device=device,
                   critical_threshold=critical_threshold, epsilon=epsilon, max_rollbacks=max_rollbacks,
-                  steps_per_launch=steps_per_launch, profile=int(bool(profile)), stage_halo=int(bool(stage_halo)))
+                  steps_per_launch=steps_per_launch, profile=int(bool(profile)), stage_halo=int(bool(stage_halo)),
+                  learned_mlp={"tcgen05": 0, "mma.sync": 1}[learned_mlp])
         if tile is not None:
             kw["tile"] = tile
         self.options = _lib.default_options(**kw)

@@ -38,7 +38,7 @@ class Options(ctypes.Structure):
     _fields_ = [("size", u32), ("mode", i32), ("precision", i32), ("critical_threshold", i32),
                 ("epsilon", f64), ("seed", u64), ("replica", u32), ("device", i32), ("max_rollbacks", i32),
                 ("steps_per_launch", i32), ("tile", i32 * 3), ("persistent", i32), ("profile", i32),
-                ("stage_halo", i32)]
+                ("stage_halo", i32), ("learned_mlp", i32)]
 
 
 class Profile(ctypes.Structure):
@@ -141,7 +141,7 @@ def _load() -> ctypes.CDLL:
         "plis_learner_set_records": (i32, [vp, vp, u64]),
         "plis_learner_train": (i32, [vp, P(TrainParams), P(TrainReport)]),
         "plis_learner_gradient": (i32, [vp, ctypes.c_float, vp, P(f64)]),
-        "plis_learner_predict": (i32, [vp, vp, u64, vp]),
+        "plis_learner_predict": (i32, [vp, vp, u64, vp, i32]),
         "plis_learner_get_weights": (i32, [vp, vp]),
         "plis_learner_set_weights": (i32, [vp, vp]),
         "plis_set_proposer": (i32, [vp, vp, f64]),

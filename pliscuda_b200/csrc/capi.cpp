@@ -88,6 +88,7 @@ void plis_options_init(plis_options* o) {
   o->steps_per_launch = 0;
   o->persistent = -1;
   o->stage_halo = 0;
+  o->learned_mlp = 0;
 }
 
 int plis_create(const plis_model_desc* model, const plis_options* opts, plis_handle** out) {
@@ -106,6 +107,7 @@ int plis_create(const plis_model_desc* model, const plis_options* opts, plis_han
     g_err = "critical_threshold, epsilon or max_rollbacks out of range";
     return PLIS_ERR_INVALID;
   }
+  if (o.learned_mlp != PLIS_MLP_TCGEN05 && o.learned_mlp != PLIS_MLP_MMA_SYNC) { g_err = "unknown learned_mlp"; return PLIS_ERR_INVALID; }
   plis::Model m;
   std::string err;
   int rc = plis::build_model(model, &m, &err);
@@ -270,10 +272,11 @@ int plis_learner_gradient(plis_learner* L, float quantile, float* grad, double* 
   PLIS_GUARD_END
 }
 
-int plis_learner_predict(plis_learner* L, const float* features, uint64_t n, float* y) {
+int plis_learner_predict(plis_learner* L, const float* features, uint64_t n, float* y, int mlp_kernel) {
   PLIS_GUARD_BEGIN
   if (!L || ((!features || !y) && n)) { g_err = "null argument"; return PLIS_ERR_INVALID; }
-  return lfail(L, L->l.predict(features, n, y));
+  if (mlp_kernel != PLIS_MLP_TCGEN05 && mlp_kernel != PLIS_MLP_MMA_SYNC) { g_err = "unknown MLP kernel"; return PLIS_ERR_INVALID; }
+  return lfail(L, L->l.predict(features, n, y, mlp_kernel));
   PLIS_GUARD_END
 }
 

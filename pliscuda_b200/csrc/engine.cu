@@ -334,8 +334,9 @@ int Engine::set_proposer(const float* weights, double s_max) {
       return PLIS_ERR_UNSUPPORTED;
     }
     if (s_max < 1.0) { err_ = "s_max must be >= 1"; return PLIS_ERR_INVALID; }
-    llaunch_ = learned_pick(opt_.precision, model_.S);
-    if (!llaunch_.classify) { err_ = "learned tau proposals support up to 4 species"; return PLIS_ERR_LIMIT; }
+    if (model_.S > 4) { err_ = "learned tau proposals support up to 4 species"; return PLIS_ERR_LIMIT; }
+    llaunch_ = learned_pick(opt_.precision, model_.S, opt_.learned_mlp);
+    if (!llaunch_.classify) { err_ = "cannot configure the learned classification kernel"; return PLIS_ERR_CUDA; }
     int rc;
     if (!d_lp_) {
       if ((rc = dmalloc((void**)&d_lp_, sizeof(LearnedParams)))) return rc;
@@ -360,7 +361,7 @@ int Engine::set_proposer(const float* weights, double s_max) {
 }
 
 int Engine::trace_features(TraceRec* out, uint32_t offset, uint32_t stride, uint32_t count) {
-  LearnedLaunch l = learned_pick(opt_.precision, model_.S);
+  LearnedLaunch l = learned_pick(opt_.precision, model_.S, PLIS_MLP_MMA_SYNC);
   if (!l.features) { err_ = "trace recording supports up to 4 species"; return PLIS_ERR_LIMIT; }
   if (!state_set_) { err_ = "no state set"; return PLIS_ERR_INVALID; }
   if (count == 0) return PLIS_OK;
@@ -371,7 +372,7 @@ int Engine::trace_features(TraceRec* out, uint32_t offset, uint32_t stride, uint
 }
 
 int Engine::trace_label(TraceRec* recs, uint32_t count, double tau_step, double label_eps) {
-  LearnedLaunch l = learned_pick(opt_.precision, model_.S);
+  LearnedLaunch l = learned_pick(opt_.precision, model_.S, PLIS_MLP_MMA_SYNC);
   if (!l.label) { err_ = "trace recording supports up to 4 species"; return PLIS_ERR_LIMIT; }
   if (count == 0) return PLIS_OK;
   l.label(args_, recs, count, tau_step, (float)(label_eps > 0.0 ? label_eps : opt_.epsilon), stream_);

@@ -25,6 +25,7 @@
 #include "engine.h"
 #include "engine_kernels.cuh"
 #include "learned.h"
+#include "tc_mlp.cuh"
 
 namespace plis {
 
@@ -165,6 +166,17 @@ __device__ __forceinline__ void normalise(const LearnedParams* __restrict__ P, f
   for (int k = 0; k < kFeat; ++k) f[k] = (f[k] - __ldg(&P->fmean[k])) * __ldg(&P->finv[k]);
 }
 
+__device__ __forceinline__ tc::Params tc_params(const LearnedParams* P) {
+  tc::Params t;
+  t.wimg = P->wimg;
+  t.b1 = P->b1;
+  t.b2 = P->b2;
+  t.b3 = P->b3;
+  t.w4 = P->w4;
+  t.b4 = P->b4;
+  return t;
+}
+
 // ------------------------------------------------------------------------------------------------
 // classification with proposals
 // ------------------------------------------------------------------------------------------------
@@ -262,6 +274,70 @@ __global__ void __launch_bounds__(256, 2) k_classify_learned(KArgs A) {
     classify_control(A, K, gridDim.x);
 }
 
+// The same classification with the MLP on tcgen05 (tc_mlp.cuh): the CTA's rows are its subvolumes.
+template <typename Real, int MAXS>
+__global__ void __launch_bounds__(256, 2) k_classify_learned_tc(KArgs A) {
+  extern __shared__ __align__(128) uint8_t tsm[];
+  __shared__ int s_err;
+  Ctrl* K = A.b.ctrl;
+  if (K->done) return;
+  if (threadIdx.x == 0) s_err = 0;
+  const ClassifyCtx C = classify_ctx(A, K);
+  const LearnedParams* P = A.b.lp;
+  const DevModel& m = A.m;
+  Cell cl;
+  const bool valid = cell_of(A, blockIdx.x, cl);
+  const uint32_t c = cl.c;
+  double tn = PLIS_INF_D, tp = PLIS_INF_D;
+  long long ti = 0x7FFFFFFFFFFFFFFFll;
+  int fl = F_SSA_FF, bad = 0;
+  bool ff = false;
+  Real tau_ncr = RT<Real>::inf(), rate = (Real)0;
+  float f[kFeat];
+#pragma unroll
+  for (int k = 0; k < kFeat; ++k) f[k] = 0.f;
+  if (valid) {
+    Counts<MAXS> x;
+    load_counts(m, C.Xe, c, x);
+#pragma unroll
+    for (int s = 0; s < MAXS; ++s)
+      if (s < (int)m.S) {
+        if (x.v[s] < 0) bad = 1;
+        C.Xz[(size_t)s * m.Npad + c] = 0;
+      }
+    Nbr q;
+    nbr_info(m, cl, q);
+    ff = classify_ff(A.o.mode, C.tau_cur[c], C.flag_cur[c], C.step, C.ff, tn, fl);
+    if (!ff) {
+      cell_tau_parts<Real>(A, c, q, x, C.Xe, tau_ncr, rate);
+      if (!plis_isinf_d((double)tau_ncr)) {
+        cell_features<Real>(A, c, q, x, C.Xe, tau_ncr, f);
+        normalise(P, f);
+      }
+    }
+  }
+  const float y = tc::mlp_cta(tc_params(P), f, tsm, &s_err);
+  if (threadIdx.x == 0 && s_err) atomicExch(&K->status, (int)PLIS_ERR_TIMEOUT);
+  if (valid) {
+    if (ff) {
+      tp = tn;
+    } else {
+      const double tcr = cell_tau_cr<Real>(A, c, C.step, C.attempt, rate);
+      const double tnd = (double)tau_ncr;
+      int fp;
+      cell_decide(tnd, tcr, tp, fp);
+      const float ls = fminf(fmaxf(y, 0.f), P->log_smax);
+      const double sc = ls > 0.f ? (double)expf(ls) : 1.0;
+      cell_decide(plis_isinf_d(tnd) ? tnd : tnd * sc, tcr, tn, fl);
+    }
+    C.tau_new[c] = tn;
+    C.flag_new[c] = (uint8_t)fl;
+    ti = c;
+  }
+  if (classify_slot_learned(A, K, blockIdx.x, gridDim.x, tn, ti, tp, valid && fl == F_LEAP_CR, bad))
+    classify_control(A, K, gridDim.x);
+}
+
 // ------------------------------------------------------------------------------------------------
 // trace recording
 // ------------------------------------------------------------------------------------------------
@@ -338,6 +414,13 @@ struct LearnedSet {
   static void classify(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) {
     k_classify_learned<Real, MAXS><<<g, b, 0, s>>>(a);
   }
+  static void classify_tc(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) {
+    k_classify_learned_tc<Real, MAXS><<<g, b, tc::kTcSmemBytes, s>>>(a);
+  }
+  static cudaError_t prepare_tc() {
+    return cudaFuncSetAttribute(k_classify_learned_tc<Real, MAXS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)tc::kTcSmemBytes);
+  }
   static void features(const KArgs& a, TraceRec* out, uint32_t offset, uint32_t stride, uint32_t count,
                        cudaStream_t s) {
     k_trace_features<Real, MAXS><<<(count + 127) / 128, 128, 0, s>>>(a, out, offset, stride, count);
@@ -347,21 +430,55 @@ struct LearnedSet {
   }
 };
 
+template <typename Real, int MAXS>
+static LearnedLaunch learned_set(int mlp) {
+  using L = LearnedSet<Real, MAXS>;
+  if (mlp == PLIS_MLP_MMA_SYNC) return {L::classify, L::features, L::label};
+  if (L::prepare_tc() != cudaSuccess) return {nullptr, nullptr, nullptr};
+  return {L::classify_tc, L::features, L::label};
+}
+
 template <typename Real>
-static LearnedLaunch learned_pick_impl(uint32_t S) {
-  if (S <= 1) return {LearnedSet<Real, 1>::classify, LearnedSet<Real, 1>::features, LearnedSet<Real, 1>::label};
-  if (S <= 2) return {LearnedSet<Real, 2>::classify, LearnedSet<Real, 2>::features, LearnedSet<Real, 2>::label};
-  if (S <= 4) return {LearnedSet<Real, 4>::classify, LearnedSet<Real, 4>::features, LearnedSet<Real, 4>::label};
+static LearnedLaunch learned_pick_impl(uint32_t S, int mlp) {
+  if (S <= 1) return learned_set<Real, 1>(mlp);
+  if (S <= 2) return learned_set<Real, 2>(mlp);
+  if (S <= 4) return learned_set<Real, 4>(mlp);
   return {nullptr, nullptr, nullptr};
 }
 
-LearnedLaunch learned_pick(int precision, uint32_t S) {
-  return precision == PLIS_PREC_FP32 ? learned_pick_impl<float>(S) : learned_pick_impl<double>(S);
+LearnedLaunch learned_pick(int precision, uint32_t S, int mlp_kernel) {
+  return precision == PLIS_PREC_FP32 ? learned_pick_impl<float>(S, mlp_kernel) : learned_pick_impl<double>(S, mlp_kernel);
 }
 
 // ------------------------------------------------------------------------------------------------
 // packing, inference for tests
 // ------------------------------------------------------------------------------------------------
+// the tcgen05 weight image: element (n, k) of W_l^T (= W_l[k][n]) at its K-major canonical offset
+__global__ void k_pack_image(const float* __restrict__ w, LearnedParams* __restrict__ P) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;  // 64*16 + 2*64*64 elements
+  if (i >= 64 * 16 + 2 * 64 * 64) return;
+  uint16_t* img = reinterpret_cast<uint16_t*>(P->wimg);
+  int n, k, base, chunk;
+  float v;
+  if (i < 64 * 16) {
+    n = i / 16;
+    k = i % 16;
+    v = k < kFeat ? w[kOffW1 + k * kHid + n] : 0.f;
+    base = 0;
+    chunk = 1024;
+  } else {
+    const int ii = i - 64 * 16, layer = ii / 4096, e = ii % 4096;
+    n = e / 64;
+    k = e % 64;
+    v = w[(layer == 0 ? kOffW2 : kOffW3) + k * kHid + n];
+    base = tc::kW1Bytes + layer * tc::kWBytes;
+    chunk = 1024;
+  }
+  const uint32_t off = (uint32_t)base + tc::canon((uint32_t)n, (uint32_t)k, (uint32_t)chunk);
+  const __nv_bfloat16 b = __float2bfloat16_rn(v);
+  img[off / 2] = *reinterpret_cast<const uint16_t*>(&b);
+}
+
 __global__ void k_pack(const float* __restrict__ w, float log_smax, LearnedParams* __restrict__ P) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = i & 31, g = lane >> 2, t = lane & 3;
@@ -398,6 +515,22 @@ __global__ void k_pack(const float* __restrict__ w, float log_smax, LearnedParam
 void learned_pack(const float* w, double s_max, LearnedParams* out, cudaStream_t s) {
   const float ls = s_max > 1.0 ? (float)std::log(s_max) : 0.f;
   k_pack<<<(8 * 32 + 2 * 32 * 32 + 255) / 256, 256, 0, s>>>(w, ls, out);
+  k_pack_image<<<(64 * 16 + 2 * 64 * 64 + 255) / 256, 256, 0, s>>>(w, out);
+}
+
+__global__ void __launch_bounds__(256) k_predict_tc(const LearnedParams* __restrict__ P, const float* __restrict__ feats,
+                                                    uint64_t n, float* __restrict__ y, int* __restrict__ status) {
+  extern __shared__ __align__(128) uint8_t tsm[];
+  __shared__ int s_err;
+  if (threadIdx.x == 0) s_err = 0;
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  float f[kFeat];
+#pragma unroll
+  for (int k = 0; k < kFeat; ++k) f[k] = i < n ? feats[i * kFeat + k] : 0.f;
+  if (i < n) normalise(P, f);
+  const float v = tc::mlp_cta(tc_params(P), f, tsm, &s_err);
+  if (i < n) y[i] = v;
+  if (threadIdx.x == 0 && s_err) atomicExch(status, PLIS_ERR_TIMEOUT);
 }
 
 __global__ void k_predict(const LearnedParams* __restrict__ P, const float* __restrict__ feats, uint64_t n,
@@ -891,23 +1024,36 @@ int Learner::gradient(float* grad, double* loss, float quantile) {
   return PLIS_OK;
 }
 
-int Learner::predict(const float* features, uint64_t n, float* y) {
+int Learner::predict(const float* features, uint64_t n, float* y, int mlp_kernel) {
   PLIS_LCU(cudaSetDevice(device_));
   if (n == 0) return PLIS_OK;
   float *d_f = nullptr, *d_y = nullptr;
+  int* d_st = nullptr;
   PLIS_LCU(cudaMalloc(&d_f, n * kFeat * sizeof(float)));
   cudaError_t e = cudaMalloc(&d_y, n * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&d_st, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_st, 0, sizeof(int), stream_);
   if (e == cudaSuccess) e = cudaMemcpyAsync(d_f, features, n * kFeat * sizeof(float), cudaMemcpyHostToDevice, stream_);
   if (e == cudaSuccess) {
     learned_pack(w_, 1.0, packed_, stream_);
-    k_predict<<<(unsigned)((n + 127) / 128), 128, 0, stream_>>>(packed_, d_f, n, d_y);
-    e = cudaGetLastError();
+    if (mlp_kernel == PLIS_MLP_MMA_SYNC) {
+      k_predict<<<(unsigned)((n + 127) / 128), 128, 0, stream_>>>(packed_, d_f, n, d_y);
+    } else {
+      e = cudaFuncSetAttribute(k_predict_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::kTcSmemBytes);
+      if (e == cudaSuccess)
+        k_predict_tc<<<(unsigned)((n + 255) / 256), 256, tc::kTcSmemBytes, stream_>>>(packed_, d_f, n, d_y, d_st);
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
   }
+  int st = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(y, d_y, n * sizeof(float), cudaMemcpyDeviceToHost, stream_);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&st, d_st, sizeof(int), cudaMemcpyDeviceToHost, stream_);
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
   cudaFree(d_f);
   if (d_y) cudaFree(d_y);
+  if (d_st) cudaFree(d_st);
   if (e != cudaSuccess) { err_ = cudaGetErrorString(e); return PLIS_ERR_CUDA; }
+  if (st) { err_ = "tensor-core MLP wait timed out"; return st; }
   return PLIS_OK;
 }
 

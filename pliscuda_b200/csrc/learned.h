@@ -30,9 +30,11 @@ static_assert(kNParams == 8961, "parameter count");
 constexpr int kNWeights = kNParams + 2 * kFeat;  // 8977
 static_assert(kNWeights == PLIS_PROPOSER_WEIGHTS, "weights layout");
 
-// Device copy the inference reads: BF16 B fragments of mma.sync.m16n8k16 (one uint2 per lane per
-// 16x8 tile; layer 1's K is padded from 8 to 16 with zeros), the rest binary32.
+// Device copy the inference reads: the BF16 weight image of the tcgen05 kernel (tc_mlp.cuh), BF16
+// B fragments of mma.sync.m16n8k16 (one uint2 per lane per 16x8 tile; layer 1's K is padded from 8
+// to 16 with zeros), the rest binary32.
 struct LearnedParams {
+  uint4 wimg[(2 * 1024 + 2 * 8 * 1024) / 16];  // W1^T, W2^T, W3^T, BF16, tcgen05 K-major canonical image
   uint2 w1f[8 * 32];       // [n-tile][lane]
   uint2 w2f[4 * 8 * 32];   // [k-tile][n-tile][lane]
   uint2 w3f[4 * 8 * 32];
@@ -58,8 +60,9 @@ struct LearnedLaunch {
   void (*features)(const KArgs&, TraceRec*, uint32_t offset, uint32_t stride, uint32_t count, cudaStream_t);
   void (*label)(const KArgs&, TraceRec*, uint32_t count, double tau_step, float eps, cudaStream_t);
 };
+// mlp_kernel: PLIS_MLP_TCGEN05 or PLIS_MLP_MMA_SYNC (include/plis.h)
 // nullptr members when the species count is above 4
-LearnedLaunch learned_pick(int precision, uint32_t S);
+LearnedLaunch learned_pick(int precision, uint32_t S, int mlp_kernel);
 // pack master weights (device, kNWeights floats) into a LearnedParams
 void learned_pack(const float* w, double s_max, LearnedParams* out, cudaStream_t s);
 
@@ -76,7 +79,7 @@ class Learner {
   int set_records(const void* recs, uint64_t n);
   int train(const plis_train_params& p, plis_train_report* out);
   int gradient(float* grad, double* loss, float quantile);
-  int predict(const float* features, uint64_t n, float* y);
+  int predict(const float* features, uint64_t n, float* y, int mlp_kernel);
   int get_weights(float* w);
   int set_weights(const float* w);
   const std::string& error() const { return err_; }

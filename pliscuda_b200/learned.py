@@ -100,10 +100,12 @@ class Learner:
         _check(_lib.lib.plis_learner_gradient(self._h, float(quantile), _c(g), ctypes.byref(loss)))
         return g, float(loss.value)
 
-    def predict(self, features: np.ndarray) -> np.ndarray:
+    def predict(self, features: np.ndarray, kernel: str = "tcgen05") -> np.ndarray:
+        """MLP outputs for raw feature rows, through the tcgen05 or the mma.sync inference kernel."""
         f = np.ascontiguousarray(features, dtype=np.float32).reshape(-1, 8)
         y = np.empty(f.shape[0], np.float32)
-        _check(_lib.lib.plis_learner_predict(self._h, _c(f), int(f.shape[0]), _c(y)))
+        k = {"tcgen05": 0, "mma.sync": 1}[kernel]
+        _check(_lib.lib.plis_learner_predict(self._h, _c(f), int(f.shape[0]), _c(y), k))
         return y
 
     def weights(self) -> np.ndarray:

@@ -88,13 +88,15 @@ def _learner(cap=1 << 16):
     return Learner(cap)
 
 
-def test_inference_matches_a_bf16_reference():
+@pytest.mark.parametrize("kernel", ["tcgen05", "mma.sync"])
+def test_inference_matches_a_bf16_reference(kernel):
+    """1000 rows: 3 full CTAs of the tcgen05 kernel and a partial one."""
     rng = np.random.default_rng(3)
     w = random_weights(1)
     feats = rng.normal(0, 2, (1000, 8)).astype(np.float32)
     with _learner() as L:
         L.set_weights(w)
-        y = L.predict(feats)
+        y = L.predict(feats, kernel=kernel)
     ref = mlp_bf16(w, feats)
     err = np.abs(y - ref) / (1 + np.abs(ref))
     assert np.median(err) < 1e-5, np.median(err)
@@ -120,9 +122,22 @@ def test_gradient_matches_float64_backprop():
     assert np.abs(g - gref).max() < 2e-3 * scale, (np.abs(g - gref).max(), scale)
 
 
+def test_both_inference_kernels_agree():
+    rng = np.random.default_rng(8)
+    w = random_weights(4)
+    feats = rng.normal(0, 2, (4096, 8)).astype(np.float32)
+    with _learner() as L:
+        L.set_weights(w)
+        a = L.predict(feats, kernel="tcgen05")
+        b = L.predict(feats, kernel="mma.sync")
+    err = np.abs(a - b) / (1 + np.abs(b))
+    assert np.median(err) < 1e-5 and err.max() < 2e-2
+
+
+@pytest.mark.parametrize("mlp", ["tcgen05", "mma.sync"])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 @pytest.mark.parametrize("case", ["schlogl16", "small_ab6", "react9_eps3"])
-def test_unit_clamp_is_the_plain_method(case, precision):
+def test_unit_clamp_is_the_plain_method(case, precision, mlp):
     """Any weights with s_max = 1: counts, taus, flags, times and counters equal the plain
     corrected run at every step; the plain run itself equals the oracle."""
     from oracle.oracle import Oracle
@@ -137,7 +152,7 @@ def test_unit_clamp_is_the_plain_method(case, precision):
         kw = {"epsilon": 3.0}
     w = random_weights(7, scale=3.0)
     a = Simulation(model, mode="corrected", precision=precision, seed=9, **kw)
-    b = Simulation(model, mode="corrected", precision=precision, seed=9, **kw)
+    b = Simulation(model, mode="corrected", precision=precision, seed=9, learned_mlp=mlp, **kw)
     o = Oracle.from_model(model, mode=1, precision=0 if precision == "fp64" else 1, seed=9, **kw)
     a.set_state(state)
     b.set_state(state)
