@@ -203,6 +203,23 @@ def ncu_case(args):
     return 0
 
 
+def ncu_learned_case(args):
+    """Fixed small case for ncu captures of the learned step: a proposer trained briefly on 10 plain
+    corrected steps of the workload (clamp 16), then 10 + 3 learned steps (plain launches).  Filter
+    the capture to the step's kernels, e.g. -k regex:"k_leap|k_exact|k_learned|k_mlp"."""
+    from pliscuda_b200 import Simulation
+    from pliscuda_b200.learned import train_proposer
+    model, state = _workload(args.workload)
+    w, _ = train_proposer(model, state, label_epsilon=1.6, n_steps=10, iterations=300)
+    with Simulation(model, mode="corrected", precision=args.precision, seed=1000) as sim:
+        sim.set_state(state)
+        sim.set_proposer(w, 16.0)
+        sim.step(10)
+        st = sim.step(3)
+    print(json.dumps({"ncu_learned_case": args.workload, "steps": st.steps, "events": st.events}))
+    return 0
+
+
 def precision_report(args):
     """FP32 form vs binary64 on the precision configuration: the seeded random 10-species,
     20-reaction network (orders 0-2) on a 128^3 lattice.  The binary64 GPU step is bit-identical to
@@ -304,6 +321,7 @@ def main(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--ncu-case", action="store_true", help="run only the fixed ncu capture case")
+    ap.add_argument("--ncu-learned-case", action="store_true", help="run only the fixed ncu case of the learned step")
     ap.add_argument("--precision-report", action="store_true", help="FP32 form vs binary64 on the precision config")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-tau comparison")
     ap.add_argument("--learned-report", action="store_true", help="print only the learned-tau comparison")
@@ -314,6 +332,8 @@ def main(argv=None):
         return run_reference(args)
     if args.ncu_case:
         return ncu_case(args)
+    if args.ncu_learned_case:
+        return ncu_learned_case(args)
     if args.precision_report:
         return precision_report(args)
     if args.learned_report:

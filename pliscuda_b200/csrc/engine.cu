@@ -343,16 +343,30 @@ int Engine::set_proposer(const float* weights, double s_max) {
       if ((rc = dmalloc((void**)&d_lw_, PLIS_PROPOSER_WEIGHTS * sizeof(float)))) return rc;
       if ((rc = dmalloc((void**)&d_slot_plain_, (size_t)args_.g.nblocks * sizeof(double)))) return rc;
     }
+    if (opt_.learned_mlp == PLIS_MLP_TCGEN05 && !d_feat_) {  // the split classification's buffers
+      const size_t rows = ((size_t)args_.m.Npad + 127) / 128 * 128;
+      if ((rc = dmalloc((void**)&d_feat_, rows * sizeof(uint4)))) return rc;
+      PLIS_CU(cudaMemset(d_feat_, 0, rows * sizeof(uint4)));
+      if ((rc = dmalloc((void**)&d_pre_, (size_t)args_.m.Npad * sizeof(double2)))) return rc;
+      if ((rc = dmalloc((void**)&d_pre_kind_, (size_t)args_.m.Npad))) return rc;
+      if ((rc = dmalloc((void**)&d_ymlp_, rows * sizeof(float)))) return rc;
+    }
     PLIS_CU(cudaMemcpyAsync(d_lw_, weights, PLIS_PROPOSER_WEIGHTS * sizeof(float), cudaMemcpyHostToDevice, stream_));
     learned_pack(d_lw_, s_max, d_lp_, stream_);
     PLIS_CU(cudaGetLastError());
     args_.b.lp = d_lp_;
     args_.b.slot_tau_plain = d_slot_plain_;
+    args_.b.feat = d_feat_;
+    args_.b.pre = d_pre_;
+    args_.b.pre_kind = d_pre_kind_;
+    args_.b.ymlp = d_ymlp_;
   } else {
     args_.b.lp = nullptr;
     args_.b.slot_tau_plain = nullptr;
   }
   use_learned_ = on;
+  const int classify_launches = (on && opt_.learned_mlp == PLIS_MLP_TCGEN05) ? 3 : 1;
+  kernels_per_step_ = ((opt_.mode == PLIS_MODE_REFERENCE) ? 4 : 3) + classify_launches - 1;
   if (graph_exec_) {  // the graph holds the kernel arguments by value
     cudaGraphExecDestroy(graph_exec_);
     graph_exec_ = nullptr;

@@ -85,6 +85,10 @@ struct DevBufs {
   uint32_t* slot_bad;
   double* slot_tau_plain;  // learned classification: per-CTA min of the plain taus (else null)
   const struct LearnedParams* lp;  // learned classification: the proposer's packed weights
+  uint4* feat;             // learned classification (split): normalised BF16 features, 16 B per subvolume
+  double2* pre;            // (leap bound or fast-forwarded tau, critical rate) per subvolume
+  uint8_t* pre_kind;       // 1: fast-forwarded, 2: leap bound computed
+  float* ymlp;             // MLP output per subvolume
   Ctrl* ctrl;
 };
 

@@ -78,6 +78,10 @@ class Engine {
   LearnedParams* d_lp_ = nullptr;
   float* d_lw_ = nullptr;
   double* d_slot_plain_ = nullptr;
+  uint4* d_feat_ = nullptr;
+  double2* d_pre_ = nullptr;
+  uint8_t* d_pre_kind_ = nullptr;
+  float* d_ymlp_ = nullptr;
 };
 
 }  // namespace plis

@@ -7,8 +7,9 @@
 //    is, after bias + ReLU + BF16 rounding, exactly the A fragment of the next layer, so hidden
 //    activations never leave registers; B fragments are pre-packed per lane (16 KB per layer, read
 //    through L1).
-//  * k_classify_learned: the classification with proposals, a second (plain) min-tau reduction
-//    for the rollback fallback, and the usual last-CTA control.
+//  * k_classify_learned (MLP by mma.sync inside the classification) or k_learned_pre + k_mlp_tc
+//    (tcgen05, tc_mlp.cuh) + k_learned_post: the classification with proposals, a second (plain)
+//    min-tau reduction for the rollback fallback, and the usual last-CTA control.
 //  * k_trace_features / k_trace_label: recording of (features, label) pairs from plain steps.
 //  * k_train / k_adam / feature statistics / k_pack: training in FP32 (one CTA = 128 records, the
 //    forward and backward pass of the whole MLP in shared memory, per-CTA gradients reduced in a
@@ -274,28 +275,22 @@ __global__ void __launch_bounds__(256, 2) k_classify_learned(KArgs A) {
     classify_control(A, K, gridDim.x);
 }
 
-// The same classification with the MLP on tcgen05 (tc_mlp.cuh): the CTA's rows are its subvolumes.
+// The classification with proposals split in three launches, the MLP on tcgen05 in between:
+// k_learned_pre (per subvolume: negativity check, zeroing of the next target, fast-forward or leap
+// bound and critical rate, normalised BF16 features), k_mlp_tc (persistent, tc_mlp.cuh), and
+// k_learned_post (critical time, decision against the proposal and the plain bound, reductions,
+// last-CTA control).  The pre and post passes keep the plain classification's occupancy.
 template <typename Real, int MAXS>
-__global__ void __launch_bounds__(256, 2) k_classify_learned_tc(KArgs A) {
-  extern __shared__ __align__(128) uint8_t tsm[];
-  __shared__ int s_err;
+__global__ void __launch_bounds__(256) k_learned_pre(KArgs A) {
   Ctrl* K = A.b.ctrl;
   if (K->done) return;
-  if (threadIdx.x == 0) s_err = 0;
   const ClassifyCtx C = classify_ctx(A, K);
   const LearnedParams* P = A.b.lp;
   const DevModel& m = A.m;
   Cell cl;
   const bool valid = cell_of(A, blockIdx.x, cl);
   const uint32_t c = cl.c;
-  double tn = PLIS_INF_D, tp = PLIS_INF_D;
-  long long ti = 0x7FFFFFFFFFFFFFFFll;
-  int fl = F_SSA_FF, bad = 0;
-  bool ff = false;
-  Real tau_ncr = RT<Real>::inf(), rate = (Real)0;
-  float f[kFeat];
-#pragma unroll
-  for (int k = 0; k < kFeat; ++k) f[k] = 0.f;
+  int bad = 0;
   if (valid) {
     Counts<MAXS> x;
     load_counts(m, C.Xe, c, x);
@@ -307,33 +302,69 @@ __global__ void __launch_bounds__(256, 2) k_classify_learned_tc(KArgs A) {
       }
     Nbr q;
     nbr_info(m, cl, q);
-    ff = classify_ff(A.o.mode, C.tau_cur[c], C.flag_cur[c], C.step, C.ff, tn, fl);
-    if (!ff) {
+    double tn;
+    int fl;
+    float f[kFeat];
+#pragma unroll
+    for (int k = 0; k < kFeat; ++k) f[k] = 0.f;
+    if (classify_ff(A.o.mode, C.tau_cur[c], C.flag_cur[c], C.step, C.ff, tn, fl)) {
+      A.b.pre[c] = make_double2(tn, 0.0);
+      A.b.pre_kind[c] = 1;
+    } else {
+      Real tau_ncr, rate;
       cell_tau_parts<Real>(A, c, q, x, C.Xe, tau_ncr, rate);
+      A.b.pre[c] = make_double2((double)tau_ncr, (double)rate);
+      A.b.pre_kind[c] = 2;
       if (!plis_isinf_d((double)tau_ncr)) {
         cell_features<Real>(A, c, q, x, C.Xe, tau_ncr, f);
         normalise(P, f);
       }
     }
+    A.b.feat[c] = make_uint4(pack_bf16x2(f[0], f[1]), pack_bf16x2(f[2], f[3]), pack_bf16x2(f[4], f[5]),
+                             pack_bf16x2(f[6], f[7]));
   }
-  const float y = tc::mlp_cta(tc_params(P), f, tsm, &s_err);
-  if (threadIdx.x == 0 && s_err) atomicExch(&K->status, (int)PLIS_ERR_TIMEOUT);
+  const int nbad = __syncthreads_or(bad);
+  if (threadIdx.x == 0) A.b.slot_bad[blockIdx.x] = nbad ? 1u : 0u;
+}
+
+__global__ void __launch_bounds__(128) k_mlp_tc(const Ctrl* __restrict__ K, const LearnedParams* __restrict__ P,
+                                                const uint4* __restrict__ feats, float* __restrict__ y, uint32_t nrows,
+                                                uint32_t ntiles, int* status) {
+  extern __shared__ __align__(128) uint8_t tsm[];
+  if (K && K->done) return;
+  tc::mlp_tiles(tc_params(P), feats, y, nrows, ntiles, tsm, status);
+}
+
+template <typename Real, int MAXS>
+__global__ void __launch_bounds__(256) k_learned_post(KArgs A) {
+  Ctrl* K = A.b.ctrl;
+  if (K->done) return;
+  const ClassifyCtx C = classify_ctx(A, K);
+  const LearnedParams* P = A.b.lp;
+  Cell cl;
+  const bool valid = cell_of(A, blockIdx.x, cl);
+  const uint32_t c = cl.c;
+  double tn = PLIS_INF_D, tp = PLIS_INF_D;
+  long long ti = 0x7FFFFFFFFFFFFFFFll;
+  int fl = F_SSA_FF;
   if (valid) {
-    if (ff) {
+    const double2 pr = A.b.pre[c];
+    if (A.b.pre_kind[c] == 1) {
+      tn = pr.x;
       tp = tn;
     } else {
-      const double tcr = cell_tau_cr<Real>(A, c, C.step, C.attempt, rate);
-      const double tnd = (double)tau_ncr;
+      const double tcr = cell_tau_cr<Real>(A, c, C.step, C.attempt, (Real)pr.y);
       int fp;
-      cell_decide(tnd, tcr, tp, fp);
-      const float ls = fminf(fmaxf(y, 0.f), P->log_smax);
+      cell_decide(pr.x, tcr, tp, fp);
+      const float ls = fminf(fmaxf(A.b.ymlp[c], 0.f), P->log_smax);
       const double sc = ls > 0.f ? (double)expf(ls) : 1.0;
-      cell_decide(plis_isinf_d(tnd) ? tnd : tnd * sc, tcr, tn, fl);
+      cell_decide(plis_isinf_d(pr.x) ? pr.x : pr.x * sc, tcr, tn, fl);
     }
     C.tau_new[c] = tn;
     C.flag_new[c] = (uint8_t)fl;
     ti = c;
   }
+  const int bad = threadIdx.x == 0 ? (int)A.b.slot_bad[blockIdx.x] : 0;
   if (classify_slot_learned(A, K, blockIdx.x, gridDim.x, tn, ti, tp, valid && fl == F_LEAP_CR, bad))
     classify_control(A, K, gridDim.x);
 }
@@ -409,17 +440,29 @@ __global__ void k_trace_label(KArgs A, TraceRec* recs, uint32_t count, double ta
   recs[i] = r;
 }
 
+// persistent grid of the tile kernel: 4 CTAs per SM at most, never more CTAs than tiles
+static uint32_t mlp_grid(uint32_t ntiles) {
+  static int sms = 0;
+  if (sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+  }
+  const uint32_t g = 4u * (uint32_t)sms;
+  return ntiles < g ? (ntiles ? ntiles : 1u) : g;
+}
+
 template <typename Real, int MAXS>
 struct LearnedSet {
   static void classify(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) {
     k_classify_learned<Real, MAXS><<<g, b, 0, s>>>(a);
   }
-  static void classify_tc(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) {
-    k_classify_learned_tc<Real, MAXS><<<g, b, tc::kTcSmemBytes, s>>>(a);
-  }
-  static cudaError_t prepare_tc() {
-    return cudaFuncSetAttribute(k_classify_learned_tc<Real, MAXS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)tc::kTcSmemBytes);
+  static void classify_split(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) {
+    k_learned_pre<Real, MAXS><<<g, b, 0, s>>>(a);
+    const uint32_t ntiles = a.m.Npad / 128u + ((a.m.Npad % 128u) ? 1u : 0u);
+    k_mlp_tc<<<mlp_grid(ntiles), 128, tc::kPSmemBytes, s>>>(a.b.ctrl, a.b.lp, a.b.feat, a.b.ymlp, a.m.Npad, ntiles,
+                                                            &a.b.ctrl->status);
+    k_learned_post<Real, MAXS><<<g, b, 0, s>>>(a);
   }
   static void features(const KArgs& a, TraceRec* out, uint32_t offset, uint32_t stride, uint32_t count,
                        cudaStream_t s) {
@@ -434,8 +477,9 @@ template <typename Real, int MAXS>
 static LearnedLaunch learned_set(int mlp) {
   using L = LearnedSet<Real, MAXS>;
   if (mlp == PLIS_MLP_MMA_SYNC) return {L::classify, L::features, L::label};
-  if (L::prepare_tc() != cudaSuccess) return {nullptr, nullptr, nullptr};
-  return {L::classify_tc, L::features, L::label};
+  if (cudaFuncSetAttribute(k_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::kPSmemBytes) != cudaSuccess)
+    return {nullptr, nullptr, nullptr};
+  return {L::classify_split, L::features, L::label};
 }
 
 template <typename Real>
@@ -518,19 +562,21 @@ void learned_pack(const float* w, double s_max, LearnedParams* out, cudaStream_t
   k_pack_image<<<(64 * 16 + 2 * 64 * 64 + 255) / 256, 256, 0, s>>>(w, out);
 }
 
-__global__ void __launch_bounds__(256) k_predict_tc(const LearnedParams* __restrict__ P, const float* __restrict__ feats,
-                                                    uint64_t n, float* __restrict__ y, int* __restrict__ status) {
-  extern __shared__ __align__(128) uint8_t tsm[];
-  __shared__ int s_err;
-  if (threadIdx.x == 0) s_err = 0;
+// raw features -> normalised BF16 rows (rows n .. nrows-1 zero)
+__global__ void k_feat_rows(const LearnedParams* __restrict__ P, const float* __restrict__ feats, uint64_t n,
+                            uint64_t nrows, uint4* __restrict__ rows) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nrows) return;
   float f[kFeat];
 #pragma unroll
   for (int k = 0; k < kFeat; ++k) f[k] = i < n ? feats[i * kFeat + k] : 0.f;
   if (i < n) normalise(P, f);
-  const float v = tc::mlp_cta(tc_params(P), f, tsm, &s_err);
-  if (i < n) y[i] = v;
-  if (threadIdx.x == 0 && s_err) atomicExch(status, PLIS_ERR_TIMEOUT);
+  else {
+#pragma unroll
+    for (int k = 0; k < kFeat; ++k) f[k] = 0.f;
+  }
+  rows[i] = make_uint4(pack_bf16x2(f[0], f[1]), pack_bf16x2(f[2], f[3]), pack_bf16x2(f[4], f[5]),
+                       pack_bf16x2(f[6], f[7]));
 }
 
 __global__ void k_predict(const LearnedParams* __restrict__ P, const float* __restrict__ feats, uint64_t n,
@@ -1039,9 +1085,18 @@ int Learner::predict(const float* features, uint64_t n, float* y, int mlp_kernel
     if (mlp_kernel == PLIS_MLP_MMA_SYNC) {
       k_predict<<<(unsigned)((n + 127) / 128), 128, 0, stream_>>>(packed_, d_f, n, d_y);
     } else {
-      e = cudaFuncSetAttribute(k_predict_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::kTcSmemBytes);
+      const uint64_t ntiles = (n + 127) / 128;
+      uint4* d_rows = nullptr;
+      e = cudaMalloc(&d_rows, ntiles * 128 * sizeof(uint4));
       if (e == cudaSuccess)
-        k_predict_tc<<<(unsigned)((n + 255) / 256), 256, tc::kTcSmemBytes, stream_>>>(packed_, d_f, n, d_y, d_st);
+        e = cudaFuncSetAttribute(k_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::kPSmemBytes);
+      if (e == cudaSuccess) {
+        k_feat_rows<<<(unsigned)((ntiles * 128 + 255) / 256), 256, 0, stream_>>>(packed_, d_f, n, ntiles * 128, d_rows);
+        k_mlp_tc<<<mlp_grid((uint32_t)ntiles), 128, tc::kPSmemBytes, stream_>>>(nullptr, packed_, d_rows, d_y,
+                                                                                (uint32_t)n, (uint32_t)ntiles, d_st);
+        e = cudaStreamSynchronize(stream_);
+      }
+      if (d_rows) cudaFree(d_rows);
     }
     if (e == cudaSuccess) e = cudaGetLastError();
   }

@@ -1,21 +1,21 @@
-// tc_mlp.cuh — the proposer's MLP for the 256 rows of a CTA on the 5th-generation tensor cores
-// (tcgen05.mma, accumulators in tensor memory).
+// tc_mlp.cuh — the proposer's MLP on the 5th-generation tensor cores (tcgen05.mma, accumulators in
+// tensor memory), over 128-row tiles.
 //
-// Layout.  Row r of the CTA (its thread r) is row r % 128 of M-tile r / 128.  Operands are BF16 in
-// shared memory in the K-major canonical layout without swizzle: 8x8-element core matrices of
-// 128 contiguous bytes (8 rows x 16 bytes); core matrix (row group g, K chunk c) of an A tile sits
-// at c * 2048 + g * 128 (LBO = 2048, SBO = 128), of a weight image (64 output rows) at
-// c * 1024 + g * 128 (LBO = 1024, SBO = 128).  One tcgen05.mma (M = 128, N = 64, K = 16,
-// kind::f16, BF16 x BF16 -> FP32) covers two K chunks; layer 1 is one MMA per tile (its K is
-// padded from 8 to 16 with zeros), layers 2 and 3 four.  The accumulators of tile t are TMEM
-// columns 64t .. 64t + 63, lane = row, so after each layer every thread reads exactly its own row
-// back with tcgen05.ld.32x32b (a warp reads the 32 lanes of its quarter), applies bias + ReLU,
-// rounds to BF16 and writes the next layer's A row.
+// Layout.  Operands are BF16 in shared memory in the K-major canonical layout without swizzle:
+// 8x8-element core matrices of 128 contiguous bytes (8 rows x 16 bytes); core matrix (row group g,
+// K chunk c) of an A tile sits at c * LBO + g * 128 (SBO = 128), so within one K chunk the 128 rows
+// are contiguous 16-byte rows: the layer-1 tile is the stored features as they are (K chunk 0)
+// followed by a zero chunk (K padded from 8 to 16).  A weight image (64 output rows) has
+// LBO = 1024.  One tcgen05.mma (M = 128, N = 64, K = 16, kind::f16, BF16 x BF16 -> FP32) covers
+// two K chunks: one per tile for layer 1, four for layers 2 and 3.  Accumulators are TMEM columns
+// 0..63, lane = row, so after each layer each of the 128 threads reads its own row back with
+// tcgen05.ld.32x32b (a warp reads the 32 lanes of its quarter), applies bias + ReLU, rounds to
+// BF16 and writes the next layer's A row.
 //
 // Synchronisation.  One thread issues the MMAs and commits them to an mbarrier; every thread
-// waits on it with an iteration limit.  A wait that runs out sets *err and the remaining layers
-// are skipped; TMEM is always freed.  The CTA allocates 128 TMEM columns and its shared memory
-// (kTcSmemBytes) keeps at most 3 CTAs on an SM, so allocation never has to wait.
+// waits on it with an iteration limit.  A wait that runs out stops the CTA with a status; TMEM is
+// always freed.  A CTA allocates 64 TMEM columns, so the 512 columns of an SM hold 8 CTAs and its
+// shared memory keeps at most 5 on an SM: allocation never has to wait.
 #ifndef PLIS_TC_MLP_CUH_
 #define PLIS_TC_MLP_CUH_
 
@@ -30,18 +30,6 @@ constexpr uint32_t kABytes = 8 * 2048;         // A tile of layers 2, 3: 128 row
 constexpr uint32_t kW1Bytes = 2 * 1024;        // W1^T: 64 x 16
 constexpr uint32_t kWBytes = 8 * 1024;         // W2^T, W3^T: 64 x 64
 constexpr uint32_t kWImageBytes = kW1Bytes + 2 * kWBytes;  // 18 KB, the packed weight image
-// shared memory: weights | A1 x 2 | A x 2 | b1 b2 b3 w4 (floats) | mbarrier | tmem slot | error
-constexpr uint32_t kOffW = 0;
-constexpr uint32_t kOffA1 = kOffW + kWImageBytes;
-constexpr uint32_t kOffA = kOffA1 + 2 * kA1Bytes;
-constexpr uint32_t kOffVec = kOffA + 2 * kABytes;
-constexpr uint32_t kOffBar = kOffVec + 4 * 64 * 4;
-constexpr uint32_t kUsed = kOffBar + 16;
-// padded so that at most 3 CTAs fit on an SM (3 x 128 TMEM columns <= 512)
-constexpr uint32_t kTcSmemBytes = 62 * 1024;
-static_assert(kUsed <= kTcSmemBytes, "tcgen05 MLP shared memory");
-static_assert(4 * (kTcSmemBytes + 1024) > 228 * 1024, "at most 3 CTAs per SM");
-constexpr uint32_t kTmemCols = 128;
 constexpr uint32_t kWaitLimit = 1u << 22;
 
 // instruction descriptor: D F32, A BF16, B BF16, both K-major, N = 64, M = 128
@@ -124,81 +112,85 @@ struct Params {
   float b4;
 };
 
-// y of this thread's row from its 8 normalised features.  All threads of the CTA (blockDim.x <=
-// 256, a multiple of 32) must call it; *err (shared, zero on entry) is set when a wait ran out.
-__device__ float mlp_cta(const Params& P, const float f[8], uint8_t* smem, volatile int* err) {
-  const uint32_t tid = threadIdx.x, nthr = blockDim.x;
+// Persistent tile kernel: shared memory of one CTA (128 threads, one 128-row tile at a time)
+constexpr uint32_t kPOffW = 0;
+constexpr uint32_t kPOffA1 = kPOffW + kWImageBytes;  // features: K chunk 0 of the layer-1 A tile
+constexpr uint32_t kPOffZero = kPOffA1 + 2048;       // K chunk 1: zeros (the padding of K 8 -> 16)
+constexpr uint32_t kPOffA = kPOffZero + 2048;        // A tile of layers 2, 3
+constexpr uint32_t kPOffVec = kPOffA + kABytes;
+constexpr uint32_t kPOffBar = kPOffVec + 4 * 64 * 4;
+constexpr uint32_t kPSmemBytes = kPOffBar + 16;
+constexpr uint32_t kPTmemCols = 64;  // <= 8 CTAs per SM ever fit the 512 columns
+static_assert(kPSmemBytes * 6 > 228 * 1024, "at most 5 CTAs per SM");
+
+// y[r] for the rows of `feats` (normalised BF16 features, 16 bytes per row, rows 0 .. 128*ntiles-1
+// readable) with the MLP on tcgen05.  Tiles are taken round robin; every CTA loads the weights once.
+// A wait that runs out sets *status and the CTA stops; TMEM is always freed.
+__device__ void mlp_tiles(const Params& P, const uint4* __restrict__ feats, float* __restrict__ y, uint32_t nrows,
+                          uint32_t ntiles, uint8_t* smem, int* status) {
+  __shared__ int s_err;
+  const uint32_t tid = threadIdx.x;  // blockDim.x == 128
   const uint32_t warp = tid >> 5;
-  const uint32_t tile = tid >> 7, row = tid & 127u;
-  const uint32_t ntiles = (nthr + 127u) >> 7;
   const uint32_t sbase = smem_u32(smem);
-  const uint32_t bar = sbase + kOffBar;
-  uint32_t* slot = reinterpret_cast<uint32_t*>(smem + kOffBar + 8);
-  float* vec = reinterpret_cast<float*>(smem + kOffVec);
-  // weights and vectors into shared memory, mbarrier, TMEM
+  const uint32_t bar = sbase + kPOffBar;
+  uint32_t* slot = reinterpret_cast<uint32_t*>(smem + kPOffBar + 8);
+  float* vec = reinterpret_cast<float*>(smem + kPOffVec);
+  if (tid == 0) s_err = 0;
   {
-    uint4* dst = reinterpret_cast<uint4*>(smem + kOffW);
-    for (uint32_t i = tid; i < kWImageBytes / 16; i += nthr) dst[i] = __ldg(&P.wimg[i]);
-    for (uint32_t i = tid; i < 64; i += nthr) {
-      vec[i] = __ldg(&P.b1[i]);
-      vec[64 + i] = __ldg(&P.b2[i]);
-      vec[128 + i] = __ldg(&P.b3[i]);
-      vec[192 + i] = __ldg(&P.w4[i]);
+    uint4* dst = reinterpret_cast<uint4*>(smem + kPOffW);
+    for (uint32_t i = tid; i < kWImageBytes / 16; i += 128) dst[i] = __ldg(&P.wimg[i]);
+    reinterpret_cast<uint4*>(smem + kPOffZero)[tid] = make_uint4(0u, 0u, 0u, 0u);
+    if (tid < 64) {
+      vec[tid] = __ldg(&P.b1[tid]);
+      vec[64 + tid] = __ldg(&P.b2[tid]);
+      vec[128 + tid] = __ldg(&P.b3[tid]);
+      vec[192 + tid] = __ldg(&P.w4[tid]);
     }
     if (tid == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
     if (warp == 0) {
-      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbase + kOffBar + 8),
-                   "r"(kTmemCols)
+      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbase + kPOffBar + 8),
+                   "r"(kPTmemCols)
                    : "memory");
       asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
   }
-  // this row of the layer-1 A tile: features 0..7, then the zero chunk
-  {
-    uint8_t* a1 = smem + kOffA1 + tile * kA1Bytes;
-    const uint4 v = make_uint4(bf16x2(f[0], f[1]), bf16x2(f[2], f[3]), bf16x2(f[4], f[5]), bf16x2(f[6], f[7]));
-    *reinterpret_cast<uint4*>(a1 + canon(row, 0, 2048)) = v;
-    *reinterpret_cast<uint4*>(a1 + canon(row, 8, 2048)) = make_uint4(0u, 0u, 0u, 0u);
-  }
-  if (nthr < ntiles * 128u) {  // rows without a thread: zero
-    for (uint32_t r = nthr; r < ntiles * 128u; ++r)
-      if (tid == 0) {
-        uint8_t* a1 = smem + kOffA1 + (r >> 7) * kA1Bytes;
-        *reinterpret_cast<uint4*>(a1 + canon(r & 127u, 0, 2048)) = make_uint4(0u, 0u, 0u, 0u);
-        *reinterpret_cast<uint4*>(a1 + canon(r & 127u, 8, 2048)) = make_uint4(0u, 0u, 0u, 0u);
-      }
-  }
   fence_before();
-  fence_async_smem();
   __syncthreads();
   fence_after();
   const uint32_t tmem = *slot;
-  const uint32_t my_cols = tmem + ((32u * (warp & 3u)) << 16) + 64u * tile;
-  float y = 0.f;
-  bool ok = true;
-  for (int layer = 0; layer < 3; ++layer) {
-    if (tid == 0 && !*err) {
-      fence_after();
-      for (uint32_t t = 0; t < ntiles; ++t) {
-        const uint32_t d = tmem + 64u * t;
+  const uint32_t my_cols = tmem + ((32u * warp) << 16);
+  const volatile int* err = &s_err;
+  uint32_t phase = 0;
+  for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const uint32_t r = tile * 128u + tid;
+    // row tid of chunk 0 of the layer-1 A tile sits at tid * 16: the features as they are stored
+    reinterpret_cast<uint4*>(smem + kPOffA1)[tid] = feats[r];
+    fence_before();
+    fence_async_smem();
+    __syncthreads();
+    bool ok = true;
+    float out = 0.f;
+    for (int layer = 0; layer < 3 && ok; ++layer) {
+      if (tid == 0 && !*err) {
+        fence_after();
         if (layer == 0) {
-          mma(d, sdesc(sbase + kOffA1 + t * kA1Bytes, 2048, 128), sdesc(sbase + kOffW, 1024, 128), 0u);
+          mma(tmem, sdesc(sbase + kPOffA1, kPOffZero - kPOffA1, 128), sdesc(sbase + kPOffW, 1024, 128), 0u);
         } else {
-          const uint32_t wofs = kOffW + kW1Bytes + (layer == 1 ? 0u : kWBytes);
+          const uint32_t wofs = kPOffW + kW1Bytes + (layer == 1 ? 0u : kWBytes);
           for (uint32_t ks = 0; ks < 4; ++ks)
-            mma(d, sdesc(sbase + kOffA + t * kABytes + ks * 2u * 2048u, 2048, 128),
-                sdesc(sbase + wofs + ks * 2u * 1024u, 1024, 128), ks > 0 ? 1u : 0u);
+            mma(tmem, sdesc(sbase + kPOffA + ks * 2u * 2048u, 2048, 128), sdesc(sbase + wofs + ks * 2u * 1024u, 1024, 128),
+                ks > 0 ? 1u : 0u);
         }
+        commit(bar);
       }
-      commit(bar);
-    }
-    ok = ok && wait_phase(bar, (uint32_t)(layer & 1), err);
-    fence_after();
-    ok = __syncthreads_and(ok && !*err) != 0;  // CTA-uniform: the loads below are warp-collective
-    if (ok) {
+      bool got = !*err && wait_phase(bar, phase & 1u, (volatile int*)err);
+      phase += 1;
+      fence_after();
+      ok = __syncthreads_and(got && !*err) != 0;
+      if (!ok) break;
       if (layer < 2) {
         const float* b = vec + 64 * layer;
-        uint8_t* a = smem + kOffA + tile * kABytes;
+        uint8_t* a = smem + kPOffA;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
           float v[16];
@@ -207,8 +199,8 @@ __device__ float mlp_cta(const Params& P, const float f[8], uint8_t* smem, volat
 #pragma unroll
           for (int i = 0; i < 8; ++i)
             p[i] = bf16x2(fmaxf(v[2 * i] + b[16 * c + 2 * i], 0.f), fmaxf(v[2 * i + 1] + b[16 * c + 2 * i + 1], 0.f));
-          *reinterpret_cast<uint4*>(a + canon(row, 16u * c, 2048)) = make_uint4(p[0], p[1], p[2], p[3]);
-          *reinterpret_cast<uint4*>(a + canon(row, 16u * c + 8u, 2048)) = make_uint4(p[4], p[5], p[6], p[7]);
+          *reinterpret_cast<uint4*>(a + canon(tid, 16u * c, 2048)) = make_uint4(p[0], p[1], p[2], p[3]);
+          *reinterpret_cast<uint4*>(a + canon(tid, 16u * c + 8u, 2048)) = make_uint4(p[4], p[5], p[6], p[7]);
         }
       } else {
         const float* b = vec + 128;
@@ -218,19 +210,23 @@ __device__ float mlp_cta(const Params& P, const float f[8], uint8_t* smem, volat
           float v[16];
           ld16(my_cols + 16u * c, v);
 #pragma unroll
-          for (int i = 0; i < 16; ++i) y = y + fmaxf(v[i] + b[16 * c + i], 0.f) * w[16 * c + i];
+          for (int i = 0; i < 16; ++i) out = out + fmaxf(v[i] + b[16 * c + i], 0.f) * w[16 * c + i];
         }
-        y = y + P.b4;
+        out = out + P.b4;
       }
+      fence_before();
+      fence_async_smem();
+      __syncthreads();
     }
-    fence_before();
-    fence_async_smem();
-    __syncthreads();
+    if (!ok) break;
+    if (r < nrows) y[r] = out;
   }
+  fence_before();
+  __syncthreads();
   fence_after();
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
-  return ok ? y : 0.f;
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kPTmemCols) : "memory");
+  if (tid == 0 && s_err) atomicExch(status, 6 /* PLIS_ERR_TIMEOUT */);
 }
 
 }  // namespace tc
