@@ -16,6 +16,9 @@ write) between timed intervals.  `e2e` is the same metric through the C ABI with
 every interval uploads the state from pinned host memory (plis_set_state), runs, and reads the
 state back (plis_get_state).
 
+`batched` (rank 0, N = 1): the batched form on 256 Brusselator replicas of uneven sizes in one
+persistent launch against the same replicas as single handles (batch_report).
+
 `learned` (rank 0, N = 1): learned tau proposals against the plain method on Schlogl 128^3 to
 t = 20 (corrected semantics, FP64): events/s and sim-time/s of both on this GPU, the KS distance of
 the marginals at every checkpoint, rollbacks, and the training and calibration that produced the
@@ -308,6 +311,49 @@ def learned_report():
     return out
 
 
+def batch_report(t0: float = 0.001, t1: float = 0.006):
+    """Batched form: 256 Brusselator replicas (side ~ U{8..48}, 7.77 M subvolumes, a ~ U[50,200],
+    b ~ U[100,600], reference semantics, FP64) in one persistent cooperative launch, brick shape
+    autotuned.  The configuration runs to t = 5, which takes ~2.7 M steps for the stiffest replica;
+    the measurement is the slice t0 -> t1 after a warm-up to t0.  The unbatched alternative is the
+    same 256 replicas run one after another as single handles with the same streams (identical
+    trajectories, so identical events)."""
+    import numpy as np
+    from pliscuda_b200 import Simulation, workloads
+    from pliscuda_b200.batch import Batch
+    reps = workloads.brusselator_batch(256)
+    n = len(reps)
+    cells = np.array([r[0].n_subvolumes for r in reps])
+    with Batch.from_models([r[0] for r in reps], seed=1) as b:
+        for i, r in enumerate(reps):
+            b.set_state(i, r[1])
+        tune = b.autotune(10)
+        b.run(t0)
+        a = [b.stats(i) for i in range(n)]
+        b.run(t1)
+        c = [b.stats(i) for i in range(n)]
+    steps = np.array([c[i].steps - a[i].steps for i in range(n)])
+    ev = int(sum(c[i].events - a[i].events for i in range(n)))
+    ms = c[0].device_ms - a[0].device_ms
+    s_ms, s_ev = 0.0, 0
+    for i, (m, st, _) in enumerate(reps):
+        with Simulation(m, mode="reference", seed=1, replica=i) as sim:
+            sim.set_state(st)
+            sim.run(t0)
+            x = sim.stats()
+            sim.run(t1)
+            y = sim.stats()
+            s_ms += y.device_ms - x.device_ms
+            s_ev += y.events - x.events
+    return {"workload": f"brusselator x{n}: {int(cells.sum())} subvolumes, sides 8..48, reference semantics, FP64, "
+                        f"slice t = {t0} -> {t1}",
+            "tuning": tune, "events": ev, "device_ms": ms, "events_per_s": ev / (ms * 1e-3),
+            "sim_time_per_s": (t1 - t0) / (ms * 1e-3), "subvolume_steps": int((steps * cells).sum()),
+            "steps_per_replica_q0_50_100": [int(np.quantile(steps, q)) for q in (0, 0.5, 1)],
+            "single_handles": {"device_ms": s_ms, "events": int(s_ev), "events_per_s": s_ev / (s_ms * 1e-3)},
+            "speedup_vs_single_handles": s_ms / ms}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -324,6 +370,8 @@ def main(argv=None):
     ap.add_argument("--ncu-learned-case", action="store_true", help="run only the fixed ncu case of the learned step")
     ap.add_argument("--precision-report", action="store_true", help="FP32 form vs binary64 on the precision config")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-tau comparison")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-replicas measurement")
+    ap.add_argument("--batch-report", action="store_true", help="print only the batched-replicas measurement")
     ap.add_argument("--learned-report", action="store_true", help="print only the learned-tau comparison")
     ap.add_argument("--report-side", type=int, default=128)
     ap.add_argument("--report-steps", type=int, default=200)
@@ -338,6 +386,9 @@ def main(argv=None):
         return precision_report(args)
     if args.learned_report:
         print(json.dumps(learned_report()))
+        return 0
+    if args.batch_report:
+        print(json.dumps(batch_report()))
         return 0
 
     import numpy as np
@@ -430,6 +481,9 @@ def main(argv=None):
     learned = None
     if rank == 0 and world == 1 and not args.no_learned:
         learned = learned_report()
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batch:
+        batched = batch_report()
 
     if rank == 0:
         line = {
@@ -452,6 +506,7 @@ def main(argv=None):
             "cpu_baseline": cpu,
             "clocks": ck,
             "learned": learned,
+            "batched": batched,
         }
         print(json.dumps(line))
     replicas.finish(dist)

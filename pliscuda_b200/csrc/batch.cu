@@ -313,9 +313,10 @@ int BatchEngine::layout(const int tile[3]) {
   }
   PLIS_CU(cudaMemcpy(d_views_, views.data(), nrep_ * sizeof(KArgs), cudaMemcpyHostToDevice));
   PLIS_CU(cudaMemcpy(d_rep_, rep.data(), nrep_ * sizeof(RepDesc), cudaMemcpyHostToDevice));
-  if (geo_.box_bytes > 48u * 1024u) PLIS_CU(launch_.set_smem((int)geo_.box_bytes));
+  const uint32_t dyn = batch_dyn_smem(geo_.box_bytes, nrep_);
+  if (dyn > 48u * 1024u) PLIS_CU(launch_.set_smem((int)dyn));
   int bps = 0, sms = 0;
-  PLIS_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, launch_.kernel, (int)geo_.threads, geo_.box_bytes));
+  PLIS_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, launch_.kernel, (int)geo_.threads, dyn));
   PLIS_CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, opt_.device));
   if (bps < 1) { err_ = "the persistent kernel does not fit on an SM"; return PLIS_ERR_UNSUPPORTED; }
   blocks_per_sm_ = bps;
@@ -349,6 +350,7 @@ static BatchArgs make_args(const DevModel& dm, const DevOpts& o, const Geo& g, v
   B.err = err;
   B.spin_limit = 1ull << 26;  // x >= 32 ns per poll: a barrier gives up after at least ~2 s
   B.max_iters = iters;
+  B.plan_off = batch_plan_offset(g.box_bytes);
   return B;
 }
 
@@ -363,7 +365,8 @@ int BatchEngine::launch(uint32_t max_iters) {
   PLIS_CU(cudaMemsetAsync(d_work_, 0, 12 * sizeof(unsigned), stream_));
   PLIS_CU(cudaMemsetAsync(d_bar_, 0, 2 * sizeof(unsigned), stream_));
   void* args[] = {&B};
-  PLIS_CU(cudaLaunchCooperativeKernel(launch_.kernel, dim3(grid_), dim3(geo_.threads), args, geo_.box_bytes, stream_));
+  PLIS_CU(cudaLaunchCooperativeKernel(launch_.kernel, dim3(grid_), dim3(geo_.threads), args,
+                                      batch_dyn_smem(geo_.box_bytes, nrep_), stream_));
   launches_ += 1;
   return PLIS_OK;
 }

@@ -59,7 +59,14 @@ struct BatchArgs {
   int* err;            // 1 = a barrier timed out
   unsigned long long spin_limit;
   uint32_t max_iters;  // global iterations per launch
+  uint32_t plan_off;   // byte offset of the plan arrays in dynamic shared memory (after the staging box)
 };
+
+// dynamic shared memory of k_batch: the staging box (if any), then four plan arrays of nrep + 1
+__host__ __device__ inline uint32_t batch_plan_offset(uint32_t box_bytes) { return (box_bytes + 15u) & ~15u; }
+__host__ __device__ inline uint32_t batch_dyn_smem(uint32_t box_bytes, uint32_t nrep) {
+  return batch_plan_offset(box_bytes) + 4u * (nrep + 1u) * (uint32_t)sizeof(uint32_t);
+}
 
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
   unsigned v;
@@ -169,12 +176,15 @@ __device__ __forceinline__ uint32_t find_replica(const uint32_t* p, uint32_t n, 
 template <typename Real, int MAXS>
 __global__ void __launch_bounds__(256, PLIS_BATCH_MIN_BLOCKS) k_batch(BatchArgs B) {
   extern __shared__ int32_t s_box[];
-  __shared__ uint32_t s_lp[kMaxBatchReplicas + 1];  // bricks leaping, prefix over replicas
-  __shared__ uint32_t s_cp[kMaxBatchReplicas + 1];  // bricks classifying, prefix over replicas
+  const uint32_t nrep = B.nrep;
+  // plan: prefix sums over replicas of the work items of each phase
+  uint32_t* s_lp = reinterpret_cast<uint32_t*>(reinterpret_cast<uint8_t*>(s_box) + B.plan_off);  // bricks leaping
+  uint32_t* s_cp = s_lp + (nrep + 1);  // bricks classifying
+  uint32_t* s_xp = s_cp + (nrep + 1);  // exact events: every brick (critical events) or one item (arg-min event)
+  uint32_t* s_ap = s_xp + (nrep + 1);  // bricks applying critical-event deltas
   __shared__ int s_exact, s_apply;
   __shared__ long long s_ev[32];
   __shared__ int s_big;
-  const uint32_t nrep = B.nrep;
   Box box;
   box.acc = B.g.staged ? s_box : nullptr;
   box.bx = (int)B.g.tx + 2;
@@ -194,15 +204,21 @@ __global__ void __launch_bounds__(256, PLIS_BATCH_MIN_BLOCKS) k_batch(BatchArgs 
       const uint32_t nt = B.rep[r].ntiles;
       s_lp[r + 1] = (!done && phase == 1) ? nt : 0u;
       s_cp[r + 1] = (!done) ? nt : 0u;
+      uint32_t xi = 0, ai = 0;
       if (!done && phase == 1) {
         const uint32_t ex = __ldcg(&K->exact);
         if (ex) s_exact = 1;
         if (ex & 1u) s_apply = 1;
+        xi = (ex & 1u) ? nt : ((ex & 2u) ? 1u : 0u);
+        ai = (ex & 1u) ? nt : 0u;
       }
+      s_xp[r + 1] = xi;
+      s_ap[r + 1] = ai;
     }
-    if (threadIdx.x == 0) { s_lp[0] = 0; s_cp[0] = 0; }
+    if (threadIdx.x == 0) { s_lp[0] = 0; s_cp[0] = 0; s_xp[0] = 0; s_ap[0] = 0; }
     __syncthreads();
     block_prefix2(s_lp + 1, s_cp + 1, nrep);
+    block_prefix2(s_xp + 1, s_ap + 1, nrep);
     const uint32_t n_leap = s_lp[nrep], n_class = s_cp[nrep];
     const int any_exact = s_exact, any_apply = s_apply;
     if (n_class == 0) break;
@@ -246,13 +262,14 @@ __global__ void __launch_bounds__(256, PLIS_BATCH_MIN_BLOCKS) k_batch(BatchArgs 
       if (!grid_barrier(B)) return;
     }
 
-    // ---- exact events (rare): one replica per CTA at a time ----
+    // ---- exact events: critical events brick by brick, the arg-min event with brick 0 ----
     if (any_exact) {
+      const uint32_t n_ex = s_xp[nrep];
       while (true) {
-        const unsigned r = grab(B.work + 1 * 3 + gen, nrep);
-        if (r >= nrep) break;
-        const Ctrl* Kr = B.ctrl + r;
-        if (__ldcg(&Kr->done) || __ldcg(&Kr->phase) != 1u || __ldcg(&Kr->exact) == 0u) continue;
+        const unsigned w = grab(B.work + 1 * 3 + gen, n_ex);
+        if (w >= n_ex) break;
+        const uint32_t r = find_replica(s_xp, nrep, w);
+        const uint32_t item = w - s_xp[r];
         const KArgs& sA = B.views[r];
         Ctrl* K = sA.b.ctrl;
         const uint32_t ex = K->exact;
@@ -262,17 +279,15 @@ __global__ void __launch_bounds__(256, PLIS_BATCH_MIN_BLOCKS) k_batch(BatchArgs 
         const uint64_t step = K->step + 1;
         const uint32_t attempt = K->attempt;
         int fired = 0;
-        if (ex & 1u) {
-          for (uint32_t c = threadIdx.x; c < sA.m.N; c += blockDim.x) {
-            if (flag[c] == F_LEAP_CR) {
-              Counts<MAXS> x;
-              load_counts(sA.m, Xc, c, x);
-              fired += critical_event_ref<Real>(sA, c, x, Xt, step, attempt, sA.b.D, flag);
-            }
+        if (ex & 1u) {  // reference: every LEAP_CR subvolume of this brick
+          Cell cl;
+          if (cell_of(sA, item, cl) && flag[cl.c] == F_LEAP_CR) {
+            Counts<MAXS> x;
+            load_counts(sA.m, Xc, cl.c, x);
+            fired += critical_event_ref<Real>(sA, cl.c, x, Xt, step, attempt, sA.b.D, flag);
           }
         }
-        __syncthreads();
-        if ((ex & 2u) && threadIdx.x == 0) {
+        if ((ex & 2u) && item == 0 && threadIdx.x == 0) {
           const uint32_t am = (uint32_t)K->argmin;
           const uint8_t fa = flag[am];
           Counts<MAXS> x;
@@ -286,31 +301,33 @@ __global__ void __launch_bounds__(256, PLIS_BATCH_MIN_BLOCKS) k_batch(BatchArgs 
             fired += argmin_event<Real>(sA, am, x, step, attempt, dst, flag, false);
           }
         }
-        if (fired) {
+        if (fired) {  // exact events are rare: one atomic per firing thread
           atomicAdd(&K->ev_attempt, (unsigned long long)fired);
           atomicAdd(&K->ex_attempt, (unsigned long long)fired);
         }
-        __syncthreads();
       }
       if (!grid_barrier(B)) return;
-      if (any_apply) {
+      if (any_apply) {  // the staged critical-event deltas, brick by brick
+        const uint32_t n_ap = s_ap[nrep];
         while (true) {
-          const unsigned r = grab(B.work + 2 * 3 + gen, nrep);
-          if (r >= nrep) break;
-          const Ctrl* Kr = B.ctrl + r;
-          if (__ldcg(&Kr->done) || __ldcg(&Kr->phase) != 1u || !(__ldcg(&Kr->exact) & 1u)) continue;
-          const RepDesc& d = B.rep[r];
-          int32_t* Xt = B.X[__ldcg(&Kr->tgt)] + d.coff;
-          int32_t* Dr = B.D + d.coff;
-          for (uint32_t c = threadIdx.x; c < d.N; c += blockDim.x)
-            for (uint32_t s = 0; s < B.m.S; ++s) {
-              const size_t i = (size_t)s * B.m.Npad + c;
+          const unsigned w = grab(B.work + 2 * 3 + gen, n_ap);
+          if (w >= n_ap) break;
+          const uint32_t r = find_replica(s_ap, nrep, w);
+          const KArgs& sA = B.views[r];
+          const Ctrl* K = sA.b.ctrl;
+          Cell cl;
+          if (cell_of(sA, w - s_ap[r], cl)) {
+            int32_t* Xt = sA.b.X[__ldcg(&K->tgt)];
+            int32_t* Dr = sA.b.D;
+            for (uint32_t sp = 0; sp < sA.m.S; ++sp) {
+              const size_t i = (size_t)sp * sA.m.Npad + cl.c;
               const int32_t v = Dr[i];
               if (v) {
                 Xt[i] += v;
                 Dr[i] = 0;
               }
             }
+          }
         }
         if (!grid_barrier(B)) return;
       }
