@@ -166,15 +166,16 @@ int plis_step(plis_handle* h, uint64_t n_steps);
 int plis_get_stats(plis_handle* h, plis_stats* out);
 
 /* The reference's whole run_simulation (driver.cu:12-408) in one call: create a handle with opts
- * (NULL = defaults), set counts, run until simulated time >= end_time, writing
+ * (NULL = defaults), set counts at simulated time start_time (0 for a new run; a snapshot's time,
+ * plis_read_snapshot, to resume one), run until simulated time >= end_time, writing
  * sim<unix time>_<time>.dat into out_dir (NULL or "" = the working directory) each time at least
  * log_freq of simulated time has passed since the last snapshot (log_freq > 0; driver.cu:362-375)
  * and once at the end (driver.cu:390-397), and, when verbose, print the reference's progress and
  * final statistics lines to stdout (driver.cu:246, 380, 399-405).  A step with no possible event
  * ends the run early as in the reference (driver.cu:269-272; stats.stop_reason ==
  * PLIS_STOP_NO_EVENT).  *out (may be NULL) receives the final statistics. */
-int plis_run_simulation(const plis_model_desc* model, const uint32_t* counts, double end_time, double log_freq,
-                        const plis_options* opts, const char* out_dir, int verbose, plis_stats* out);
+int plis_run_simulation(const plis_model_desc* model, const uint32_t* counts, double start_time, double end_time,
+                        double log_freq, const plis_options* opts, const char* out_dir, int verbose, plis_stats* out);
 
 /* Per-kernel timing of profiled run/step calls (plis_options.profile = 1); reset by plis_set_state. */
 int plis_get_profile(plis_handle* h, plis_profile* out);
@@ -350,6 +351,12 @@ int plis_parse_state(const char* path, uint32_t* n_out, uint32_t* s_out, uint32_
 int plis_parse_reactions(const char* path, uint32_t* r_out, uint32_t* s_out, int32_t** reactants_out,
                          int32_t** products_out);
 void plis_free(void* p);
+
+/* Read a .dat snapshot (the format print_state_snapshot writes, driver.cu:435-447) back: counts
+ * [S*N] species-major (malloc'd, free with plis_free) and the snapshot's time, to resume a run from
+ * it (plis_set_state + plis_set_time, or plis_run_simulation's start_time).  The time has the
+ * snapshot's six decimals. */
+int plis_read_snapshot(const char* path, uint32_t* n_out, uint32_t* s_out, double* time_out, uint32_t** counts_out);
 
 /* Snapshot in the reference's .dat format (print_state_snapshot, driver.cu:435-447). */
 int plis_write_snapshot(const char* path, const uint32_t* counts, uint32_t n, uint32_t s, double time);

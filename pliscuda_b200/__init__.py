@@ -33,7 +33,7 @@ from ._lib import (LEAP_CR, LEAP_NOCR, MODE_CORRECTED, MODE_REFERENCE, PREC_FP32
 
 __all__ = [
     "Model", "Simulation", "PlisError", "InvalidArgument", "load_configuration", "run_simulation",
-    "canonical_neighbours", "write_snapshot", "parse_topology", "parse_state", "parse_reactions",
+    "canonical_neighbours", "write_snapshot", "read_snapshot", "parse_topology", "parse_state", "parse_reactions",
     "LEAP_CR", "LEAP_NOCR", "SSA", "SSA_FF", "MODE_REFERENCE", "MODE_CORRECTED", "PREC_FP64", "PREC_FP32",
     "STOP_NONE", "STOP_TIME", "STOP_STEPS", "STOP_NO_EVENT", "STOP_ERROR", "library_path",
 ]
@@ -286,6 +286,20 @@ def parse_reactions(path: str) -> Tuple[int, int, np.ndarray, np.ndarray]:
         _lib.lib.plis_free(pr)
         _lib.lib.plis_free(pp)
     return r.value, s.value, re, pd
+
+
+def read_snapshot(path: str) -> Tuple[np.ndarray, float]:
+    """A .dat snapshot read back: (counts uint32[S*N] species-major, time), to resume a run
+    (Simulation.set_state + set_time)."""
+    n, s, t = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_double()
+    p = ctypes.c_void_p()
+    _check(_lib.lib.plis_read_snapshot(os.fsencode(path), ctypes.byref(n), ctypes.byref(s), ctypes.byref(t),
+                                       ctypes.byref(p)))
+    try:
+        a = np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ctypes.c_uint32)), shape=(n.value * s.value,)).copy()
+    finally:
+        _lib.lib.plis_free(p)
+    return a, t.value
 
 
 def write_snapshot(path: str, counts: np.ndarray, n: int, s: int, time: float) -> None:

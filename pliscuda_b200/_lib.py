@@ -131,7 +131,8 @@ def _load() -> ctypes.CDLL:
         "plis_parse_reactions": (i32, [ctypes.c_char_p, P(u32), P(u32), P(vp), P(vp)]),
         "plis_free": (None, [vp]),
         "plis_write_snapshot": (i32, [ctypes.c_char_p, vp, u32, u32, f64]),
-        "plis_run_simulation": (i32, [P(ModelDesc), vp, f64, f64, P(Options), ctypes.c_char_p, i32, P(Stats)]),
+        "plis_run_simulation": (i32, [P(ModelDesc), vp, f64, f64, f64, P(Options), ctypes.c_char_p, i32, P(Stats)]),
+        "plis_read_snapshot": (i32, [ctypes.c_char_p, P(u32), P(u32), P(f64), P(vp)]),
         "plis_train_params_init": (None, [P(TrainParams)]),
         "plis_learner_create": (i32, [u64, i32, P(vp)]),
         "plis_learner_destroy": (i32, [vp]),

@@ -50,7 +50,7 @@ void run_simulation(Topology t, State s, Reactions r, float* h_rrc, float* h_drc
   std::vector<uint32_t> buf((size_t)n * spc);
   for (size_t i = 0; i < buf.size(); ++i) buf[i] = (uint32_t)s.getState()[i];
   std::cout.flush();
-  int rc = plis_run_simulation(&d, buf.data(), endTime, log_freq, &o, nullptr, 1, nullptr);
+  int rc = plis_run_simulation(&d, buf.data(), 0.0, endTime, log_freq, &o, nullptr, 1, nullptr);
   if (rc) {  // gpuErrchk prints and exits (cpp_utils.hpp:97-105)
     std::fprintf(stderr, "GPUassert: %s (%s)\n", plis_last_error(), plis_status_string(rc));
     std::exit(rc);

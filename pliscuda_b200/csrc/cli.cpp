@@ -9,6 +9,7 @@
 //   --precision fp64|fp32        (default fp64)
 //   --seed N                     (default: PLIS_SEED from the environment, else the clock, as the
 //                                 reference's non-TEST build seeds from clock64(), init.cu:8)
+//   --resume sim<ts>_<t>.dat     start from a snapshot's counts and time instead of initialState
 // and a CUDA error exits with the library's status code, as gpuErrchk exits (cpp_utils.hpp:97-105).
 #include <cuda_runtime.h>
 
@@ -33,6 +34,7 @@ int usage() {
 
 int main(int argc, char* argv[]) {
   const char* conf = nullptr;
+  const char* resume = nullptr;
   plis_options o;
   plis_options_init(&o);
   const char* env_seed = std::getenv("PLIS_SEED");
@@ -40,9 +42,11 @@ int main(int argc, char* argv[]) {
                     : (uint64_t)std::chrono::high_resolution_clock::now().time_since_epoch().count();
   for (int i = 1; i < argc; ++i) {
     std::string a = argv[i];
-    if ((a == "--mode" || a == "--precision" || a == "--seed") && i + 1 < argc) {
+    if ((a == "--mode" || a == "--precision" || a == "--seed" || a == "--resume") && i + 1 < argc) {
       std::string v = argv[++i];
-      if (a == "--mode") {
+      if (a == "--resume") {
+        resume = argv[i];
+      } else if (a == "--mode") {
         if (v == "reference") o.mode = PLIS_MODE_REFERENCE;
         else if (v == "corrected") o.mode = PLIS_MODE_CORRECTED;
         else return usage();
@@ -98,8 +102,29 @@ int main(int argc, char* argv[]) {
   }
   plis_config_view v;
   plis_config_view_get(cfg, &v);
+  const uint32_t* counts = v.initial_state;
+  uint32_t* snap = nullptr;
+  double t0 = 0.0;
+  if (resume) {
+    uint32_t sn = 0, ss = 0;
+    rc = plis_read_snapshot(resume, &sn, &ss, &t0, &snap);
+    if (rc == PLIS_OK && (sn != v.model.n_subvolumes || ss != v.model.n_species)) {
+      std::fprintf(stderr, "pliscuda: %s has %u subvolumes x %u species, the configuration %u x %u\n", resume, sn, ss,
+                   v.model.n_subvolumes, v.model.n_species);
+      plis_free(snap);
+      plis_config_free(cfg);
+      return PLIS_ERR_INVALID;
+    }
+    if (rc) {
+      std::fprintf(stderr, "pliscuda: %s (%s)\n", plis_last_error(), plis_status_string(rc));
+      plis_config_free(cfg);
+      return rc;
+    }
+    counts = snap;
+  }
   std::cout.flush();
-  rc = plis_run_simulation(&v.model, v.initial_state, v.end_time, v.log_freq, &o, nullptr, 1, nullptr);
+  rc = plis_run_simulation(&v.model, counts, t0, v.end_time, v.log_freq, &o, nullptr, 1, nullptr);
+  if (snap) plis_free(snap);
   plis_config_free(cfg);
   if (rc) {
     std::fprintf(stderr, "GPUassert: %s (%s)\n", plis_last_error(), plis_status_string(rc));

@@ -9,6 +9,11 @@
 //   * a topology that lists fewer rows than its header (rows stay uninitialised, Topology.hpp:122),
 //   * a reactions file with a different number of lines than its header (Reactions.hpp:185-219),
 //   * a constants line with fewer values than reactions/species (std::out_of_range, cpp_utils.hpp:33).
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <cerrno>
 #include <climits>
 #include <cmath>
@@ -24,38 +29,122 @@
 
 namespace plis {
 
+// A whole input file, memory-mapped read-only (or read into memory when it cannot be mapped).
 struct Text {
-  std::string buf;
+  const char* p = nullptr;
+  size_t n = 0;
   size_t pos = 0;
-  bool eof() const { return pos >= buf.size(); }
+  void* map = nullptr;
+  std::string own;
+  bool eof() const { return pos >= n; }
+  Text() = default;
+  Text(const Text&) = delete;
+  Text& operator=(const Text&) = delete;
+  ~Text() {
+    if (map) munmap(map, n);
+  }
 };
 
 static int read_file(const std::string& path, Text* t, std::string* err) {
+  const int fd = open(path.c_str(), O_RDONLY);
+  if (fd < 0) { *err = "file " + path + " not found"; return PLIS_ERR_IO; }
+  struct stat st;
+  if (fstat(fd, &st) == 0 && S_ISREG(st.st_mode) && st.st_size > 0) {
+    void* m = mmap(nullptr, (size_t)st.st_size, PROT_READ, MAP_PRIVATE, fd, 0);
+    if (m != MAP_FAILED) {
+      madvise(m, (size_t)st.st_size, MADV_SEQUENTIAL);
+      t->map = m;
+      t->p = static_cast<const char*>(m);
+      t->n = (size_t)st.st_size;
+      t->pos = 0;
+      close(fd);
+      return PLIS_OK;
+    }
+  }
+  close(fd);
   std::ifstream f(path, std::ios::binary);
   if (!f.good()) { *err = "file " + path + " not found"; return PLIS_ERR_IO; }
   std::ostringstream ss;
   ss << f.rdbuf();
-  t->buf = ss.str();
+  t->own = ss.str();
+  t->p = t->own.data();
+  t->n = t->own.size();
   t->pos = 0;
   return PLIS_OK;
 }
 
-// std::getline(is, out, delim): extracts up to delim (consumed, not stored); false if nothing extracted
-static bool getline_d(Text* t, char delim, std::string* out) {
+// std::getline(is, out, delim) as a view [*b, *e) into the file: extracts up to delim (consumed,
+// not stored); false if nothing extracted
+static bool getline_v(Text* t, char delim, const char** b, const char** e) {
   if (t->eof()) return false;
-  size_t e = t->buf.find(delim, t->pos);
-  if (e == std::string::npos) {
-    *out = t->buf.substr(t->pos);
-    t->pos = t->buf.size();
-    return true;
+  const char* s = t->p + t->pos;
+  const char* end = t->p + t->n;
+  const char* d = static_cast<const char*>(memchr(s, delim, (size_t)(end - s)));
+  *b = s;
+  if (!d) {
+    *e = end;
+    t->pos = t->n;
+  } else {
+    *e = d;
+    t->pos = (size_t)(d - t->p) + 1;
   }
-  *out = t->buf.substr(t->pos, e - t->pos);
-  t->pos = e + 1;
+  return true;
+}
+
+static bool getline_d(Text* t, char delim, std::string* out) {
+  const char *b, *e;
+  if (!getline_v(t, delim, &b, &e)) return false;
+  out->assign(b, e);
   return true;
 }
 
 static void get_char(Text* t) {
   if (!t->eof()) t->pos++;
+}
+
+// std::stoi on the text [s, e): leading whitespace, optional sign, at least one digit, trailing
+// text ignored, int range
+static bool int_at(const char* s, const char* e, long long* v) {
+  while (s < e && (*s == ' ' || *s == '\t' || *s == '\n' || *s == '\r' || *s == '\f' || *s == '\v')) ++s;
+  bool neg = false;
+  if (s < e && (*s == '+' || *s == '-')) {
+    neg = *s == '-';
+    ++s;
+  }
+  if (s >= e || *s < '0' || *s > '9') return false;
+  long long r = 0;
+  while (s < e && *s >= '0' && *s <= '9') {
+    r = r * 10 + (*s - '0');
+    if (r > (long long)INT_MAX + 1) return false;
+    ++s;
+  }
+  r = neg ? -r : r;
+  if (r > INT_MAX || r < INT_MIN) return false;
+  *v = r;
+  return true;
+}
+
+static bool only_space_v(const char* b, const char* e) {
+  for (; b < e; ++b)
+    if (!(*b == ' ' || *b == '\n' || *b == '\r' || *b == '\t')) return false;
+  return true;
+}
+
+// PLISCuda::split(line, ' ') over a view: calls f(index, token_begin, token_end) for every token
+// between single spaces (a trailing empty token is dropped); returns the token count, or -1 if f
+// failed
+template <typename F>
+static long long for_tokens(const char* b, const char* e, F f) {
+  long long k = 0;
+  while (b < e) {
+    const char* sp = static_cast<const char*>(memchr(b, ' ', (size_t)(e - b)));
+    const char* te = sp ? sp : e;
+    if (!f(k, b, te)) return -1;
+    ++k;
+    if (!sp) break;
+    b = sp + 1;
+  }
+  return k;
 }
 
 // std::stoi semantics: leading whitespace, optional sign, at least one digit, trailing text ignored
@@ -117,30 +206,37 @@ int parse_topology(const std::string& path, uint32_t* n_out, std::vector<uint32_
   nb->assign((size_t)6 * n, 0);
   get_char(&t);
   uint32_t counter = 0;
-  std::string sub, line;
-  std::vector<std::string> tok;
-  while (getline_d(&t, ':', &sub)) {
-    if (only_space(sub) && t.eof()) break;
+  const char *sb, *se, *lb = nullptr, *le = nullptr;
+  while (getline_v(&t, ':', &sb, &se)) {
+    if (only_space_v(sb, se) && t.eof()) break;
     long long idx;
-    if (!to_int(sub.c_str(), &idx) || idx != (long long)counter) {
-      *err = "Invalid subvolume number : " + sub;
+    if (!int_at(sb, se, &idx) || idx != (long long)counter || counter >= (uint32_t)n) {
+      *err = "Invalid subvolume number : " + std::string(sb, se);
       return PLIS_ERR_PARSE;
     }
-    if (counter >= (uint32_t)n) { *err = "Invalid subvolume number : " + sub; return PLIS_ERR_PARSE; }
     counter++;
     get_char(&t);
-    getline_d(&t, '\n', &line);
-    split_sp(strip_cr(line), &tok);
-    if (tok.size() > 6) { *err = "more than 6 neighbours for subvolume " + std::to_string(counter - 1); return PLIS_ERR_PARSE; }
-    size_t i = 0;
-    for (auto& s : tok) {
+    // at the end of the file std::getline leaves the previous line in place, and so does this
+    getline_v(&t, '\n', &lb, &le);
+    if (!lb) lb = le = t.p + t.n;
+    const char* lend = (le > lb && le[-1] == '\r') ? le - 1 : le;
+    uint32_t* row = nb->data() + (size_t)(counter - 1) * 6;
+    int code = 0;
+    const long long k = for_tokens(lb, lend, [&](long long i, const char* b, const char* e) {
+      if (i >= 6) { code = 1; return false; }
       long long v;
-      if (!to_int(s.c_str(), &v)) { *err = "parse of neighbour number failed"; return PLIS_ERR_PARSE; }
-      if ((unsigned long long)(unsigned int)v >= (unsigned long long)n) { *err = "Invalid: sub >= n"; return PLIS_ERR_PARSE; }
-      (*nb)[(size_t)(counter - 1) * 6 + i] = (uint32_t)v;
-      ++i;
+      if (!int_at(b, e, &v)) { code = 2; return false; }
+      if ((unsigned long long)(unsigned int)v >= (unsigned long long)n) { code = 3; return false; }
+      row[i] = (uint32_t)v;
+      return true;
+    });
+    if (k < 0) {
+      if (code == 1) { *err = "more than 6 neighbours for subvolume " + std::to_string(counter - 1); return PLIS_ERR_PARSE; }
+      if (code == 2) { *err = "parse of neighbour number failed"; return PLIS_ERR_PARSE; }
+      *err = "Invalid: sub >= n";
+      return PLIS_ERR_PARSE;
     }
-    for (; i < 6; ++i) (*nb)[(size_t)(counter - 1) * 6 + i] = counter - 1;  // self padding, Topology.hpp:181-184
+    for (long long i = k; i < 6; ++i) row[i] = counter - 1;  // self padding, Topology.hpp:181-184
   }
   if (counter != (uint32_t)n) {
     *err = "topology lists " + std::to_string(counter) + " of " + std::to_string(n) + " subvolumes";
@@ -172,27 +268,31 @@ int parse_state(const std::string& path, uint32_t* n_out, uint32_t* s_out, std::
   long long n, s;
   if ((rc = parse_header2(&t, "subvolume", "species", &n, &s, err))) return rc;
   st->assign((size_t)n * s, 0);
-  std::string sub, line;
-  std::vector<std::string> tok;
-  while (getline_d(&t, ':', &sub)) {
-    if (only_space(sub) && t.eof()) break;
+  const char *sb, *se, *lb = nullptr, *le = nullptr;
+  while (getline_v(&t, ':', &sb, &se)) {
+    if (only_space_v(sb, se) && t.eof()) break;
     long long idx;
-    if (!to_int(sub.c_str(), &idx)) { *err = "Invalid subvolume number : " + sub; return PLIS_ERR_PARSE; }
+    if (!int_at(sb, se, &idx)) { *err = "Invalid subvolume number : " + std::string(sb, se); return PLIS_ERR_PARSE; }
     if (idx < 0 || idx >= n) { *err = "Unexpected subvolume number. Got: " + std::to_string(idx); return PLIS_ERR_PARSE; }
     get_char(&t);
-    getline_d(&t, '\n', &line);
-    line = strip_cr(line);
-    split_sp(line, &tok);
-    if ((long long)tok.size() != s) {
-      *err = "Parse of subvolume line failed (subvolume " + line + ") has wrong length";
+    getline_v(&t, '\n', &lb, &le);  // at the end of the file the previous line stays, as with std::getline
+    if (!lb) lb = le = t.p + t.n;
+    const char* lend = (le > lb && le[-1] == '\r') ? le - 1 : le;
+    const long long k = for_tokens(lb, lend, [&](long long, const char*, const char*) { return true; });
+    if (k != s) {
+      *err = "Parse of subvolume line failed (subvolume " + std::string(lb, lend) + ") has wrong length";
       return PLIS_ERR_PARSE;
     }
-    for (long long i = 0; i < s; ++i) {
+    int code = 0;
+    for_tokens(lb, lend, [&](long long i, const char* b, const char* e) {
       long long c;
-      if (!to_int(tok[i].c_str(), &c)) { *err = "parse of species count number failed"; return PLIS_ERR_PARSE; }
-      if (c < 0) { *err = "Invalid: species count < 0"; return PLIS_ERR_PARSE; }
-      (*st)[(size_t)idx + (size_t)n * i] = (uint32_t)c;  // species-major, State.hpp:210
-    }
+      if (!int_at(b, e, &c)) { code = 1; return false; }
+      if (c < 0) { code = 2; return false; }
+      (*st)[(size_t)idx + (size_t)n * (size_t)i] = (uint32_t)c;  // species-major, State.hpp:210
+      return true;
+    });
+    if (code == 1) { *err = "parse of species count number failed"; return PLIS_ERR_PARSE; }
+    if (code == 2) { *err = "Invalid: species count < 0"; return PLIS_ERR_PARSE; }
   }
   *n_out = (uint32_t)n;
   *s_out = (uint32_t)s;
@@ -452,6 +552,75 @@ extern "C" void plis_free(void* p) { free(p); }
 
 // print_state_snapshot, driver.cu:435-447: header lines, blank line, one line of S counts per
 // subvolume each followed by a space.  The time is printed like std::to_string(float).
+// The .dat snapshot print_state_snapshot writes (driver.cu:435-447): "subvolumes=N", "species=S",
+// "time=T", an empty line, then N lines of S counts each followed by a space.
+extern "C" int plis_read_snapshot(const char* path, uint32_t* n_out, uint32_t* s_out, double* time_out,
+                                  uint32_t** counts_out) {
+  using plis::Text;
+  using plis::read_file;
+  using plis::getline_v;
+  using plis::int_at;
+  using plis::for_tokens;
+  if (!path || !n_out || !s_out || !time_out || !counts_out) { set_error("null argument"); return PLIS_ERR_INVALID; }
+  *counts_out = nullptr;
+  Text t;
+  std::string err;
+  int rc = read_file(path, &t, &err);
+  if (rc) { set_error(err); return rc; }
+  const char *b, *e;
+  long long hv[2];
+  const char* keys[2] = {"subvolumes=", "species="};
+  for (int i = 0; i < 2; ++i) {
+    const size_t kl = strlen(keys[i]);
+    if (!getline_v(&t, '\n', &b, &e) || (size_t)(e - b) < kl || strncmp(b, keys[i], kl) != 0 ||
+        !int_at(b + kl, e, &hv[i]) || hv[i] < 1) {
+      set_error(std::string("snapshot ") + path + ": expected " + keys[i] + "<positive integer>");
+      return PLIS_ERR_PARSE;
+    }
+  }
+  if (!getline_v(&t, '\n', &b, &e) || (e - b) < 5 || strncmp(b, "time=", 5) != 0) {
+    set_error(std::string("snapshot ") + path + ": expected time=<value>");
+    return PLIS_ERR_PARSE;
+  }
+  const std::string tv(b + 5, e);
+  char* endp = nullptr;
+  const double time = strtod(tv.c_str(), &endp);
+  if (endp == tv.c_str()) {
+    set_error(std::string("snapshot ") + path + ": bad time value");
+    return PLIS_ERR_PARSE;
+  }
+  getline_v(&t, '\n', &b, &e);  // the empty line
+  const uint64_t n = (uint64_t)hv[0], ns = (uint64_t)hv[1];
+  if (n * ns > (1ull << 34)) { set_error("snapshot too large"); return PLIS_ERR_LIMIT; }
+  uint32_t* out = static_cast<uint32_t*>(malloc(n * ns * sizeof(uint32_t)));
+  if (!out) { set_error("out of host memory"); return PLIS_ERR_OOM; }
+  for (uint64_t i = 0; i < n; ++i) {
+    if (!getline_v(&t, '\n', &b, &e)) {
+      free(out);
+      set_error(std::string("snapshot ") + path + ": " + std::to_string(i) + " of " + std::to_string(n) + " subvolume lines");
+      return PLIS_ERR_PARSE;
+    }
+    if (e > b && e[-1] == '\r') --e;
+    int bad = 0;
+    const long long k = for_tokens(b, e, [&](long long j, const char* tb, const char* te) {
+      long long v;
+      if (j >= (long long)ns || !int_at(tb, te, &v) || v < 0) { bad = 1; return false; }
+      out[(size_t)j * n + i] = (uint32_t)v;  // species-major
+      return true;
+    });
+    if (bad || k != (long long)ns) {
+      free(out);
+      set_error(std::string("snapshot ") + path + ": bad counts for subvolume " + std::to_string(i));
+      return PLIS_ERR_PARSE;
+    }
+  }
+  *n_out = (uint32_t)n;
+  *s_out = (uint32_t)ns;
+  *time_out = time;
+  *counts_out = out;
+  return PLIS_OK;
+}
+
 extern "C" int plis_write_snapshot(const char* path, const uint32_t* counts, uint32_t n, uint32_t s, double time) {
   if (!path || !counts) { set_error("null argument"); return PLIS_ERR_INVALID; }
   FILE* f = fopen(path, "w");

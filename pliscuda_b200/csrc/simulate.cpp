@@ -47,9 +47,9 @@ void print_eltime(double secs) {
 
 }  // namespace
 
-extern "C" int plis_run_simulation(const plis_model_desc* model, const uint32_t* counts, double end_time,
-                                   double log_freq, const plis_options* opts, const char* out_dir, int verbose,
-                                   plis_stats* out) {
+extern "C" int plis_run_simulation(const plis_model_desc* model, const uint32_t* counts, double start_time,
+                                   double end_time, double log_freq, const plis_options* opts, const char* out_dir,
+                                   int verbose, plis_stats* out) {
   if (!model || !counts) {
     plis::set_error("null argument");
     return PLIS_ERR_INVALID;
@@ -64,6 +64,7 @@ extern "C" int plis_run_simulation(const plis_model_desc* model, const uint32_t*
   const uint32_t n = model->n_subvolumes, s = model->n_species;
   std::vector<uint32_t> buf((size_t)n * s);
   rc = plis_set_state(h, counts);
+  if (rc == PLIS_OK && start_time != 0.0) rc = plis_set_time(h, start_time);
   if (rc) {
     plis_destroy(h);
     return rc;

@@ -119,3 +119,32 @@ def test_cli_reports_parse_errors_like_the_reference(tmp_path):
     assert not glob.glob(str(tmp_path / "sim*.dat"))
     r = _run(["missing.txt"], str(tmp_path))
     assert r.returncode == 1 and "Couldn't load configuration file" in r.stdout
+
+
+@pytest.mark.gpu
+def test_cli_resumes_from_a_snapshot(tmp_path):
+    """--resume: the run continues from a snapshot's counts and time; with the same seed it equals
+    Simulation.set_state + set_time + run, and the final snapshot time is past the end time."""
+    from pliscuda_b200 import Simulation, read_snapshot
+    model, state, _, _ = ref_fixture("test_diff-64")
+    write_reference_files(str(tmp_path), model, state, end_time=0.5, log_freq=0.0)
+    r = _run(["conf.txt", "--seed", "5"], str(tmp_path))
+    assert r.returncode == 0, r.stdout + r.stderr
+    first = glob.glob(str(tmp_path / "sim*.dat"))
+    assert len(first) == 1
+    counts, t0 = read_snapshot(first[0])
+    res = tmp_path / "resume"
+    res.mkdir()
+    write_reference_files(str(res), model, state, end_time=1.0, log_freq=0.0)
+    r = _run(["conf.txt", "--seed", "7", "--resume", first[0]], str(res))
+    assert r.returncode == 0, r.stdout + r.stderr
+    dats = glob.glob(str(res / "sim*.dat"))
+    assert len(dats) == 1
+    x, t = _read_dat(dats[0])
+    assert t >= 1.0
+    with Simulation(model, seed=7) as sim:
+        sim.set_state(counts)
+        sim.set_time(t0)
+        st = sim.run(1.0)
+        assert "%f" % float(np.float32(st.time)) == "%f" % t
+        assert np.array_equal(sim.get_state().reshape(x.shape).astype(np.int64), x)

@@ -178,3 +178,34 @@ def test_snapshot_bytes_match_reference_golden(fixture, tmp_path):
     p = str(tmp_path / "e.dat")
     plis.write_snapshot(p, counts, n, s, t)
     assert open(p).read() == open(gold).read()
+
+
+def test_snapshot_round_trip(tmp_path):
+    """plis_read_snapshot reads back what plis_write_snapshot writes (the reference's .dat format):
+    counts exactly, the time to its six printed decimals."""
+    from pliscuda_b200 import read_snapshot, write_snapshot
+    rng = np.random.default_rng(2)
+    n, s = 37, 3
+    counts = rng.integers(0, 2**30, n * s).astype(np.uint32)
+    p = str(tmp_path / "sim1_0.250000.dat")
+    write_snapshot(p, counts, n, s, 0.25)
+    back, t = read_snapshot(p)
+    assert np.array_equal(back, counts) and t == 0.25
+    write_snapshot(p, counts, n, s, 1.0 / 3.0)
+    assert abs(read_snapshot(p)[1] - 1.0 / 3.0) < 1e-6
+
+
+@pytest.mark.parametrize("text,msg", [
+    ("subvolumes=2\nspecies=1\ntime=0.5\n\n3 \n", "1 of 2 subvolume lines"),
+    ("subvolumes=2\nspecies=1\ntime=0.5\n\n3 \n4 5 \n", "bad counts for subvolume 1"),
+    ("subvolumes=2\nspecies=1\ntime=0.5\n\n3 \n-4 \n", "bad counts for subvolume 1"),
+    ("subvolume=2\nspecies=1\ntime=0.5\n\n", "expected subvolumes="),
+    ("subvolumes=2\nspecies=1\ntim=0.5\n\n", "expected time="),
+])
+def test_snapshot_errors(tmp_path, text, msg):
+    from pliscuda_b200 import PlisError, read_snapshot
+    p = tmp_path / "bad.dat"
+    p.write_text(text)
+    with pytest.raises(PlisError) as e:
+        read_snapshot(str(p))
+    assert msg in str(e.value)
