@@ -215,7 +215,7 @@ void Engine::enqueue_step() {
   const dim3 gx((args_.m.N + 255) / 256), bx(256);
   launch_.leap(args_, gc, bc, stream_);
   launch_.exact(args_, gx, bx, stream_);
-  if (opt_.mode == PLIS_MODE_REFERENCE) k_apply<<<gx, bx, 0, stream_>>>(args_);
+  if (opt_.mode == PLIS_MODE_REFERENCE) launch_pdl(k_apply, gx, bx, 0, stream_, args_);
   launch_classify();
 }
 
@@ -230,7 +230,7 @@ int Engine::enqueue_step_profiled() {
   PLIS_CU(cudaEventRecord(pev_[1], stream_));
   launch_.exact(args_, gx, bx, stream_);
   PLIS_CU(cudaEventRecord(pev_[2], stream_));
-  if (opt_.mode == PLIS_MODE_REFERENCE) k_apply<<<gx, bx, 0, stream_>>>(args_);
+  if (opt_.mode == PLIS_MODE_REFERENCE) launch_pdl(k_apply, gx, bx, 0, stream_, args_);
   PLIS_CU(cudaEventRecord(pev_[3], stream_));
   launch_classify();
   PLIS_CU(cudaEventRecord(pev_[4], stream_));

@@ -36,6 +36,31 @@ namespace plis {
 // ------------------------------------------------------------------------------------------------
 // precision traits
 // ------------------------------------------------------------------------------------------------
+// Programmatic dependent launch.  Every kernel of the step loop starts by waiting until its
+// predecessor in the stream has completed and its writes are visible (griddepcontrol.wait), then
+// lets its successor begin launching (griddepcontrol.launch_dependents): the successor's launch and
+// CTA scheduling overlap this kernel's tail instead of following it.  Results are unchanged; launched
+// without the attribute (launch_pdl) both instructions are no-ops.
+__device__ __forceinline__ void pdl_entry() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename Kern, typename... Args>
+inline void launch_pdl(Kern kern, dim3 g, dim3 b, size_t smem, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = g;
+  cfg.blockDim = b;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 template <typename Real> struct RT;
 template <> struct RT<double> {
   static __device__ __forceinline__ double poisson(plis_stream* s, double lam) { return plis_poisson_d(s, lam); }
@@ -824,6 +849,7 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
 
 template <typename Real, int MAXS>
 __global__ void __launch_bounds__(256, PLIS_LEAP_MIN_BLOCKS) k_leap(KArgs A) {
+  pdl_entry();
   Ctrl* K = A.b.ctrl;
   if (K->done) return;
   extern __shared__ int32_t s_box[];
@@ -1039,6 +1065,7 @@ __device__ int argmin_event(const KArgs& A, uint32_t mcell, const Counts<MAXS>& 
 
 template <typename Real, int MAXS>
 __global__ void __launch_bounds__(256) k_exact(KArgs A) {
+  pdl_entry();
   Ctrl* K = A.b.ctrl;
   if (K->done) return;
   const uint32_t ex = K->exact;
@@ -1079,6 +1106,7 @@ __global__ void __launch_bounds__(256) k_exact(KArgs A) {
 
 #ifdef PLIS_ENGINE_HOST_TU
 __global__ void __launch_bounds__(256) k_apply(KArgs A) {
+  pdl_entry();
   Ctrl* K = A.b.ctrl;
   if (K->done || !(K->exact & 1u)) return;
   const DevModel& m = A.m;
@@ -1282,6 +1310,7 @@ __device__ __forceinline__ void classify_control(const KArgs& A, Ctrl* K, uint32
 
 template <typename Real, int MAXS>
 __global__ void __launch_bounds__(256) k_classify(KArgs A) {
+  pdl_entry();
   Ctrl* K = A.b.ctrl;
   if (K->done) return;
   const ClassifyCtx C = classify_ctx(A, K);
@@ -1304,12 +1333,12 @@ __global__ void k_fill_tau(double* t, uint8_t* f, uint32_t n) {
 // kernel launchers of each (precision, species capacity)
 template <typename Real, int MAXS>
 struct KernelSet {
-  static void leap(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) { k_leap<Real, MAXS><<<g, b, a.g.box_bytes, s>>>(a); }
+  static void leap(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) { launch_pdl(k_leap<Real, MAXS>, g, b, a.g.box_bytes, s, a); }
   static cudaError_t leap_smem(int bytes) {
     return cudaFuncSetAttribute(k_leap<Real, MAXS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   }
-  static void exact(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) { k_exact<Real, MAXS><<<g, b, 0, s>>>(a); }
-  static void classify(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) { k_classify<Real, MAXS><<<g, b, 0, s>>>(a); }
+  static void exact(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) { launch_pdl(k_exact<Real, MAXS>, g, b, 0, s, a); }
+  static void classify(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) { launch_pdl(k_classify<Real, MAXS>, g, b, 0, s, a); }
 };
 
 template <typename Real>

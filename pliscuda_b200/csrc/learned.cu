@@ -217,6 +217,7 @@ __device__ __forceinline__ bool classify_slot_learned(const KArgs& A, Ctrl* K, u
 
 template <typename Real, int MAXS>
 __global__ void __launch_bounds__(256, 2) k_classify_learned(KArgs A) {
+  pdl_entry();
   Ctrl* K = A.b.ctrl;
   if (K->done) return;
   const ClassifyCtx C = classify_ctx(A, K);
@@ -282,6 +283,7 @@ __global__ void __launch_bounds__(256, 2) k_classify_learned(KArgs A) {
 // last-CTA control).  The pre and post passes keep the plain classification's occupancy.
 template <typename Real, int MAXS>
 __global__ void __launch_bounds__(256) k_learned_pre(KArgs A) {
+  pdl_entry();
   Ctrl* K = A.b.ctrl;
   if (K->done) return;
   const ClassifyCtx C = classify_ctx(A, K);
@@ -331,12 +333,14 @@ __global__ void __launch_bounds__(128) k_mlp_tc(const Ctrl* __restrict__ K, cons
                                                 const uint4* __restrict__ feats, float* __restrict__ y, uint32_t nrows,
                                                 uint32_t ntiles, int* status) {
   extern __shared__ __align__(128) uint8_t tsm[];
+  pdl_entry();
   if (K && K->done) return;
   tc::mlp_tiles(tc_params(P), feats, y, nrows, ntiles, tsm, status);
 }
 
 template <typename Real, int MAXS>
 __global__ void __launch_bounds__(256) k_learned_post(KArgs A) {
+  pdl_entry();
   Ctrl* K = A.b.ctrl;
   if (K->done) return;
   const ClassifyCtx C = classify_ctx(A, K);
@@ -455,14 +459,14 @@ static uint32_t mlp_grid(uint32_t ntiles) {
 template <typename Real, int MAXS>
 struct LearnedSet {
   static void classify(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) {
-    k_classify_learned<Real, MAXS><<<g, b, 0, s>>>(a);
+    launch_pdl(k_classify_learned<Real, MAXS>, g, b, 0, s, a);
   }
   static void classify_split(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) {
-    k_learned_pre<Real, MAXS><<<g, b, 0, s>>>(a);
+    launch_pdl(k_learned_pre<Real, MAXS>, g, b, 0, s, a);
     const uint32_t ntiles = a.m.Npad / 128u + ((a.m.Npad % 128u) ? 1u : 0u);
-    k_mlp_tc<<<mlp_grid(ntiles), 128, tc::kPSmemBytes, s>>>(a.b.ctrl, a.b.lp, a.b.feat, a.b.ymlp, a.m.Npad, ntiles,
-                                                            &a.b.ctrl->status);
-    k_learned_post<Real, MAXS><<<g, b, 0, s>>>(a);
+    launch_pdl(k_mlp_tc, dim3(mlp_grid(ntiles)), dim3(128), tc::kPSmemBytes, s, (const Ctrl*)a.b.ctrl,
+               (const LearnedParams*)a.b.lp, (const uint4*)a.b.feat, a.b.ymlp, a.m.Npad, ntiles, (int*)&a.b.ctrl->status);
+    launch_pdl(k_learned_post<Real, MAXS>, g, b, 0, s, a);
   }
   static void features(const KArgs& a, TraceRec* out, uint32_t offset, uint32_t stride, uint32_t count,
                        cudaStream_t s) {
