@@ -223,6 +223,24 @@ def ncu_learned_case(args):
     return 0
 
 
+def ncu_batch_case(args):
+    """Fixed small case for ncu captures of the batched form: 32 Brusselator replicas (sides 8..24),
+    brick 8x8x2, one persistent launch of 20 steps after a 5-step one (capture with -k regex:k_batch
+    -s 1 -c 1)."""
+    from pliscuda_b200 import workloads
+    from pliscuda_b200.batch import Batch
+    reps = workloads.brusselator_batch(32, side_range=(8, 24))
+    with Batch.from_models([r[0] for r in reps], seed=1, tile=(8, 8, 2)) as b:
+        for i, r in enumerate(reps):
+            b.set_state(i, r[1])
+        b.step(5)
+        b.step(20)
+        st = [b.stats(i) for i in range(len(reps))]
+    print(json.dumps({"ncu_batch_case": len(reps), "steps": [min(x.steps for x in st), max(x.steps for x in st)],
+                      "events": sum(x.events for x in st), "subvolumes": sum(r[0].n_subvolumes for r in reps)}))
+    return 0
+
+
 def precision_report(args):
     """FP32 form vs binary64 on the precision configuration: the seeded random 10-species,
     20-reaction network (orders 0-2) on a 128^3 lattice.  The binary64 GPU step is bit-identical to
@@ -368,6 +386,7 @@ def main(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--ncu-case", action="store_true", help="run only the fixed ncu capture case")
     ap.add_argument("--ncu-learned-case", action="store_true", help="run only the fixed ncu case of the learned step")
+    ap.add_argument("--ncu-batch-case", action="store_true", help="run only the fixed ncu case of the batched form")
     ap.add_argument("--precision-report", action="store_true", help="FP32 form vs binary64 on the precision config")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-tau comparison")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-replicas measurement")
@@ -382,6 +401,8 @@ def main(argv=None):
         return ncu_case(args)
     if args.ncu_learned_case:
         return ncu_learned_case(args)
+    if args.ncu_batch_case:
+        return ncu_batch_case(args)
     if args.precision_report:
         return precision_report(args)
     if args.learned_report:
