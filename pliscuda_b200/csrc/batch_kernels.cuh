@@ -107,13 +107,17 @@ __device__ __forceinline__ bool grid_barrier(const BatchArgs& B) {
   return s_ok != 0;
 }
 
-// next unit of a phase for this CTA: a work index in [0, total) or total when exhausted
-__device__ __forceinline__ unsigned grab(unsigned* counter, unsigned total) {
-  __shared__ unsigned s_w;
-  if (threadIdx.x == 0) s_w = atomicAdd(counter, 1u);
+// next unit of a phase for this CTA: a work index in [0, total) or total when exhausted.  One CTA
+// barrier per call: the index goes through one of two shared slots, alternating with `par` (the same
+// sequence of calls in every thread), so a slot is rewritten only after the barrier of the next call,
+// by which time every thread has read it.
+__device__ __forceinline__ unsigned grab(unsigned* counter, unsigned total, unsigned& par) {
+  __shared__ unsigned s_w[2];
+  const unsigned slot = par;
+  par ^= 1u;
+  if (threadIdx.x == 0) s_w[slot] = atomicAdd(counter, 1u);
   __syncthreads();
-  const unsigned w = s_w;
-  __syncthreads();
+  const unsigned w = s_w[slot];
   return w < total ? w : total;
 }
 
@@ -183,8 +187,7 @@ __global__ void __launch_bounds__(256, PLIS_BATCH_MIN_BLOCKS) k_batch(BatchArgs 
   uint32_t* s_xp = s_cp + (nrep + 1);  // exact events: every brick (critical events) or one item (arg-min event)
   uint32_t* s_ap = s_xp + (nrep + 1);  // bricks applying critical-event deltas
   __shared__ int s_exact, s_apply;
-  __shared__ long long s_ev[32];
-  __shared__ int s_big;
+  unsigned par = 0;  // slot parity of grab()
   Box box;
   box.acc = B.g.staged ? s_box : nullptr;
   box.bx = (int)B.g.tx + 2;
@@ -226,12 +229,10 @@ __global__ void __launch_bounds__(256, PLIS_BATCH_MIN_BLOCKS) k_batch(BatchArgs 
     // ---- leap ----
     if (n_leap > 0) {
       while (true) {
-        const unsigned w = grab(B.work + 0 * 3 + gen, n_leap);
+        const unsigned w = grab(B.work + 0 * 3 + gen, n_leap, par);
         if (w >= n_leap) break;
         const uint32_t r = find_replica(s_lp, nrep, w);
         const KArgs& sA = B.views[r];
-        if (threadIdx.x == 0) s_big = 0;
-        __syncthreads();
         Ctrl* K = sA.b.ctrl;
         LeapCtx L;
         L.Xc = sA.b.X[K->cur];
@@ -243,21 +244,10 @@ __global__ void __launch_bounds__(256, PLIS_BATCH_MIN_BLOCKS) k_batch(BatchArgs 
         long long ev;
         int big;
         leap_tile<Real, MAXS>(sA, w - s_lp[r], L, tl, box, ev, big);
-        ev = warp_sum(ev);
-        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-        if (big) s_big = 1;
-        if (lane == 0) s_ev[wid] = ev;
-        __syncthreads();
-        if (wid == 0) {
-          const int nw = (blockDim.x + 31) >> 5;
-          long long v = lane < nw ? s_ev[lane] : 0;
-          v = warp_sum(v);
-          if (lane == 0) {
-            if (v) atomicAdd(&K->ev_attempt, (unsigned long long)v);
-            if (s_big) atomicOr(&K->blocks_done, 0x80000000u);
-          }
-        }
-        __syncthreads();
+        ev = warp_sum(ev);  // events by warp, straight into the replica's counter (integer: order-free)
+        if ((threadIdx.x & 31) == 0 && ev) atomicAdd(&K->ev_attempt, (unsigned long long)ev);
+        if (big) atomicOr(&K->blocks_done, 0x80000000u);  // rare: an oversized draw forces a rollback
+        if (box.acc) __syncthreads();  // the staging box is reused by the next brick
       }
       if (!grid_barrier(B)) return;
     }
@@ -266,7 +256,7 @@ __global__ void __launch_bounds__(256, PLIS_BATCH_MIN_BLOCKS) k_batch(BatchArgs 
     if (any_exact) {
       const uint32_t n_ex = s_xp[nrep];
       while (true) {
-        const unsigned w = grab(B.work + 1 * 3 + gen, n_ex);
+        const unsigned w = grab(B.work + 1 * 3 + gen, n_ex, par);
         if (w >= n_ex) break;
         const uint32_t r = find_replica(s_xp, nrep, w);
         const uint32_t item = w - s_xp[r];
@@ -310,7 +300,7 @@ __global__ void __launch_bounds__(256, PLIS_BATCH_MIN_BLOCKS) k_batch(BatchArgs 
       if (any_apply) {  // the staged critical-event deltas, brick by brick
         const uint32_t n_ap = s_ap[nrep];
         while (true) {
-          const unsigned w = grab(B.work + 2 * 3 + gen, n_ap);
+          const unsigned w = grab(B.work + 2 * 3 + gen, n_ap, par);
           if (w >= n_ap) break;
           const uint32_t r = find_replica(s_ap, nrep, w);
           const KArgs& sA = B.views[r];
@@ -335,7 +325,7 @@ __global__ void __launch_bounds__(256, PLIS_BATCH_MIN_BLOCKS) k_batch(BatchArgs 
 
     // ---- classify + per-replica control ----
     while (true) {
-      const unsigned w = grab(B.work + 3 * 3 + gen, n_class);
+      const unsigned w = grab(B.work + 3 * 3 + gen, n_class, par);
       if (w >= n_class) break;
       const uint32_t r = find_replica(s_cp, nrep, w);
       const KArgs& sA = B.views[r];
