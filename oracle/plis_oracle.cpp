@@ -52,6 +52,12 @@ template <> struct RealOps<double> {
     return lam < 10.0 ? plis_poisson_small_d(s, lam, em) : plis_poisson_d(s, lam);
   }
   static int64_t count(double k) { return (int64_t)plis_count_d(k); }
+  // inversion draw i of a group of n from the group's shared Philox blocks (plis_group_uniforms_d)
+  static double inv_group(const plis_stream* g, uint32_t i, int n, double lam, double em) {
+    double u[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    plis_group_uniforms_d(g, 1u << i, u, n);
+    return plis_poisson_inv_d(u[i], lam, em);
+  }
   static double uniform(plis_stream* s) { return plis_uniform_d(s); }
   static double inf() { return PLIS_INF_D; }
   static double fabs_(double x) { return fabs(x); }
@@ -64,6 +70,11 @@ template <> struct RealOps<float> {
     return lam < 10.0f ? plis_poisson_small_f(s, lam, em) : plis_poisson_d(s, (double)lam);
   }
   static int64_t count(double k) { return (int64_t)plis_count_d(k); }
+  static double inv_group(const plis_stream* g, uint32_t i, int n, float lam, float em) {
+    float u[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    plis_group_uniforms_f(g, 1u << i, u, n);
+    return plis_poisson_inv_f(u[i], lam, em);
+  }
   static float uniform(plis_stream* s) { return plis_uniform_f(s); }
   static float inf() { return PLIS_INF_F; }
   static float fabs_(float x) { return fabsf(x); }
@@ -388,8 +399,15 @@ struct Sim : Base {
         Real a = rr_c[(size_t)r * N + c];
         bool fire = (mode == 0) ? !crit_ref(x, c, r) : ((a > (Real)0) && !crit_fix(x, c, r, a));
         if (!fire) continue;
-        plis_stream sr = plis_stream_make(opt.seed, opt.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_react(r));
-        int64_t k = Ops::count(Ops::poisson(&sr, tl * a));
+        const Real lam = tl * a;
+        int64_t k;
+        if (lam > (Real)0 && lam < (Real)10) {  // inversion: uniform r % 4 of reaction group r / 4
+          plis_stream g = plis_stream_make(opt.seed, opt.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_rgroup(r >> 2));
+          k = Ops::count(Ops::inv_group(&g, r & 3u, 4, lam, Ops::emlam(lam)));
+        } else {
+          plis_stream sr = plis_stream_make(opt.seed, opt.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_react(r));
+          k = Ops::count(Ops::poisson(&sr, lam));
+        }
         ev += k;
         for (auto& e : rx[r].net) {
           int64_t v = k * e.second;
@@ -405,8 +423,14 @@ struct Sim : Base {
         Real lam = tl * dr_c[(size_t)s * N + c];
         Real em = Ops::emlam(lam);
         for (int j = 0; j < n; ++j) {
-          plis_stream sd = plis_stream_make(opt.seed, opt.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_diff(s, j));
-          int64_t k = Ops::count(Ops::poisson_shared(&sd, lam, em));
+          int64_t k;
+          if (lam > (Real)0 && lam < (Real)10) {  // inversion: uniform j of the species' diffusion group
+            plis_stream g = plis_stream_make(opt.seed, opt.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_dgroup(s));
+            k = Ops::count(Ops::inv_group(&g, (uint32_t)j, 6, lam, em));
+          } else {
+            plis_stream sd = plis_stream_make(opt.seed, opt.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_diff(s, j));
+            k = Ops::count(Ops::poisson_shared(&sd, lam, em));
+          }
           if (k >= kBigJump) big = 1;
           outk[((size_t)c * S + s) * 6 + j] = k;
           own[(size_t)c * S + s] -= k;

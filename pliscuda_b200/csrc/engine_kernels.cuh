@@ -92,11 +92,17 @@ template <> struct RT<float> {
 template <typename Real> struct DiffTraits;
 template <> struct DiffTraits<double> {
   static __device__ __forceinline__ double uni(plis_stream* s) { return plis_uniform_d(s); }
+  static __device__ __forceinline__ void group(const plis_stream* g, uint32_t need, double* u, int n) {
+    plis_group_uniforms_d(g, need, u, n);
+  }
   static constexpr double tail = 8.673617379884035e-19;
   static constexpr int kmax = 200;
 };
 template <> struct DiffTraits<float> {
   static __device__ __forceinline__ float uni(plis_stream* s) { return plis_uniform_f(s); }
+  static __device__ __forceinline__ void group(const plis_stream* g, uint32_t need, float* u, int n) {
+    plis_group_uniforms_f(g, need, u, n);
+  }
   static constexpr float tail = 2.9802322e-08f;
   static constexpr int kmax = 100;
 };
@@ -125,13 +131,16 @@ __device__ __forceinline__ void diffusion_draws(const KArgs& A, uint32_t c, int 
   Real p = em, F = em;
   bool pending = false;
 #pragma unroll
+  for (int j = 0; j < 6; ++j) u[j] = (Real)0;
+  {  // the slots' uniforms from the species' grouped blocks
+    const plis_stream g = plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_dgroup(s));
+    DiffTraits<Real>::group(&g, (1u << n) - 1u, u, 6);
+  }
+#pragma unroll
   for (int j = 0; j < 6; ++j) {
-    u[j] = (Real)0;
     open_[j] = false;
     k[j] = 0;
     if (j < n) {
-      plis_stream st = plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_diff(s, j));
-      u[j] = DiffTraits<Real>::uni(&st);
       open_[j] = u[j] > F;
       pending |= open_[j];
     }
@@ -733,6 +742,7 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
         Real u[4], lam[4];
         bool act[4];
         long long kk[4];
+        uint32_t need = 0;
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
           const int r = r0 + i;
@@ -745,15 +755,20 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
             const bool fire = (mode == 0) ? !crit_ref(m, x, r, nc) : ((a > (Real)0) && !crit_fix(m, x, r, a, nc));
             lam[i] = fire ? tl * a : (Real)0;
             if (lam[i] > (Real)0) {
-              plis_stream st = plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_react(r));
               if (lam[i] < (Real)10) {
-                act[i] = true;
-                u[i] = DiffTraits<Real>::uni(&st);  // the inversion search's single uniform
+                act[i] = true;  // inversion search: its single uniform comes from the group's blocks
+                need |= 1u << i;
               } else {
+                plis_stream st = plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_react(r));
                 kk[i] = RT<Real>::count(RT<Real>::poisson(&st, lam[i]));
               }
             }
           }
+        }
+        if (need) {
+          const plis_stream g =
+              plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_rgroup((uint32_t)r0 >> 2));
+          DiffTraits<Real>::group(&g, need, u, 4);
         }
         long long ks[4];
         batched_small_draws<Real>(u, lam, act, ks);

@@ -145,6 +145,15 @@ enum {
 #define PLIS_CH_DIFF_BASE 0x40000u  // diffusion channels: base + species * 8 + slot
 PLIS_HD uint32_t plis_ch_react(uint32_t r) { return r; }
 PLIS_HD uint32_t plis_ch_diff(uint32_t s, uint32_t slot) { return PLIS_CH_DIFF_BASE + s * 8u + slot; }
+// Grouped channels: the single uniforms of the inversion-searched draws (means below 10) of a group
+// come from shared Philox blocks, two binary64 or four binary32 uniforms per block (uniform i of a
+// group: block i / per-block, words in order).  Reactions 4g .. 4g+3 form group g; the six
+// neighbour slots of one species form its diffusion group.  Draws searched by PTRS keep their own
+// channels (plis_ch_react, plis_ch_diff).
+#define PLIS_CH_RGROUP_BASE 0x20000u  // + reaction group
+#define PLIS_CH_DGROUP_BASE 0x60000u  // + species
+PLIS_HD uint32_t plis_ch_rgroup(uint32_t g) { return PLIS_CH_RGROUP_BASE + g; }
+PLIS_HD uint32_t plis_ch_dgroup(uint32_t s) { return PLIS_CH_DGROUP_BASE + s; }
 
 typedef struct plis_stream {
   plis_u32x4 ctr;
@@ -198,6 +207,55 @@ PLIS_HD double plis_uniform_d(plis_stream* s) {
 PLIS_HD float plis_uniform_f(plis_stream* s) {
   uint32_t x = plis_stream_u32(s) >> 9;
   return ((float)x + 0.5f) * 1.1920928955078125e-07f;  // 2^-23
+}
+
+// Uniforms 0 .. n-1 of a group (n <= 8): u[i] for every i whose bit is set in `need` (the others may
+// be left unset).  `g` is the group's stream (plis_stream_make with the group channel); its blocks
+// are computed here, only those holding a needed uniform.  binary64: uniform i from words
+// (2(i%2), 2(i%2)+1) of block i/2; binary32: word i%4 of block i/4; the conversions are
+// plis_uniform_d / plis_uniform_f's.
+PLIS_HD plis_u32x4 plis_group_block(const plis_stream* g, uint32_t b) {
+  plis_u32x4 ctr = g->ctr;
+  ctr.y = (ctr.y & 0xFFFFF000u) | (b & 0xFFFu);
+  return plis_philox4x32_10(ctr, g->k0, g->k1);
+}
+
+PLIS_HD double plis_u64_to_uniform_d(uint32_t hi, uint32_t lo) {
+  uint64_t x = (((uint64_t)hi << 32) | (uint64_t)lo) >> 12;
+  return ((double)x + 0.5) * 2.220446049250313e-16;  // 2^-52
+}
+
+PLIS_HD float plis_u32_to_uniform_f(uint32_t w) {
+  uint32_t x = w >> 9;
+  return ((float)x + 0.5f) * 1.1920928955078125e-07f;  // 2^-23
+}
+
+PLIS_HD void plis_group_uniforms_d(const plis_stream* g, uint32_t need, double* u, int n) {
+#if defined(__CUDA_ARCH__)
+#pragma unroll
+#endif
+  for (int b = 0; b < 4; ++b) {
+    if (2 * b < n && (need >> (2 * b)) & 3u) {
+      const plis_u32x4 w = plis_group_block(g, (uint32_t)b);
+      u[2 * b] = plis_u64_to_uniform_d(w.x, w.y);
+      if (2 * b + 1 < n) u[2 * b + 1] = plis_u64_to_uniform_d(w.z, w.w);
+    }
+  }
+}
+
+PLIS_HD void plis_group_uniforms_f(const plis_stream* g, uint32_t need, float* u, int n) {
+#if defined(__CUDA_ARCH__)
+#pragma unroll
+#endif
+  for (int b = 0; b < 2; ++b) {
+    if (4 * b < n && (need >> (4 * b)) & 15u) {
+      const plis_u32x4 w = plis_group_block(g, (uint32_t)b);
+      u[4 * b] = plis_u32_to_uniform_f(w.x);
+      if (4 * b + 1 < n) u[4 * b + 1] = plis_u32_to_uniform_f(w.y);
+      if (4 * b + 2 < n) u[4 * b + 2] = plis_u32_to_uniform_f(w.z);
+      if (4 * b + 3 < n) u[4 * b + 3] = plis_u32_to_uniform_f(w.w);
+    }
+  }
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -359,6 +417,22 @@ static const double plis_inv_k_tab[201] = {PLIS_INV_K_VALUES};
 
 // Poisson(lam) for lam < 10 by inversion (sequential search from 0), given emlam = exp(-lam):
 // draws that share a mean (the per-neighbour diffusion draws of one species) share the exp.
+// inversion by sequential search from the uniform u (plis_poisson_small_d without its draw)
+PLIS_HD double plis_poisson_inv_d(double u, double lam, double emlam) {
+  double p = emlam;
+  double F = p;
+  double k = 0.0;
+  int ki = 0;
+  while (u > F) {
+    k += 1.0;
+    ki += 1;
+    p = (p * lam) * plis_inv_k_tab[ki];
+    F += p;
+    if (p <= F * 8.673617379884035e-19 || ki >= 200) break;  // tail below 2^-60: stop
+  }
+  return k;
+}
+
 PLIS_HD double plis_poisson_small_d(plis_stream* st, double lam, double emlam) {
   double u = plis_uniform_d(st);
   double p = emlam;
@@ -468,6 +542,21 @@ PLIS_HD float plis_logf(float x) {
   float lm = 2.0f * PLIS_FMAF(s * s2, q, s);
   float ef = (float)e;
   return ef * PLIS_LN2_HI_F + (ef * PLIS_LN2_LO_F + lm);
+}
+
+PLIS_HD double plis_poisson_inv_f(float u, float lam, float emlam) {
+  float p = emlam;
+  float F = p;
+  float k = 0.0f;
+  int ki = 0;
+  while (u > F) {
+    k += 1.0f;
+    ki += 1;
+    p = (p * lam) * (float)plis_inv_k_tab[ki];
+    F += p;
+    if (p <= F * 2.9802322e-08f || ki >= 100) break;  // tail below 2^-25
+  }
+  return (double)k;
 }
 
 PLIS_HD double plis_poisson_small_f(plis_stream* st, float lam, float emlam) {
