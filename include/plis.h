@@ -248,6 +248,12 @@ int plis_batch_get_stats(plis_batch* b, uint32_t replica, plis_stats* out);
  * the number of replicas per CTA adapts to their sizes at run time. */
 int plis_batch_autotune(plis_batch* b, uint64_t pilot_steps, plis_batch_tuning* out);
 int plis_batch_get_tuning(plis_batch* b, plis_batch_tuning* out);
+/* Learned tau proposals for every replica of the batch (the proposer of plis_set_proposer, same
+ * rules: corrected mode, up to 4 species, weights NULL or s_max <= 0 detaches).  Replica r then
+ * follows exactly the trajectory of a handle with options.replica = replica_ids[r],
+ * learned_mlp = PLIS_MLP_MMA_SYNC and the same proposer.  Every replica's current state is
+ * classified again; times and statistics are kept. */
+int plis_batch_set_proposer(plis_batch* b, const float* weights, double s_max);
 
 /* ---------------------------------------------------------------------------------------------
  * Learned tau proposals (no counterpart in the reference).  A proposer is an MLP 8 -> 64 -> 64 ->

@@ -122,6 +122,7 @@ def _load() -> ctypes.CDLL:
         "plis_batch_get_stats": (i32, [vp, u32, P(Stats)]),
         "plis_batch_autotune": (i32, [vp, u64, P(BatchTuning)]),
         "plis_batch_get_tuning": (i32, [vp, P(BatchTuning)]),
+        "plis_batch_set_proposer": (i32, [vp, vp, f64]),
         "plis_canonical_neighbours": (i32, [u32, vp, vp, vp, vp]),
         "plis_config_load": (i32, [ctypes.c_char_p, P(vp)]),
         "plis_config_view_get": (i32, [vp, P(ConfigView)]),

@@ -117,6 +117,19 @@ class Batch:
         _check(_lib.lib.plis_batch_autotune(self._h, int(pilot_steps), ctypes.byref(t)))
         return {"tile": tuple(t.tile), "blocks_per_sm": t.blocks_per_sm, "grid": t.grid, "events_per_s": t.events_per_s}
 
+    def set_proposer(self, weights: Optional[np.ndarray], s_max: float = 0.0) -> None:
+        """Learned tau proposals for every replica (corrected mode; weights from
+        pliscuda_b200.learned.Learner.weights()), or none (weights None).  Replica r then follows
+        Simulation(model_r, mode="corrected", replica=replica_ids[r], learned_mlp="mma.sync") with
+        the same proposer exactly."""
+        if weights is None or s_max <= 0:
+            _check(_lib.lib.plis_batch_set_proposer(self._h, None, 0.0))
+            return
+        w = np.ascontiguousarray(weights, dtype=np.float32).reshape(-1)
+        if w.size != _lib.PROPOSER_WEIGHTS:
+            raise ValueError(f"proposer weights must hold {_lib.PROPOSER_WEIGHTS} floats")
+        _check(_lib.lib.plis_batch_set_proposer(self._h, _c(w), float(s_max)))
+
     def tuning(self) -> dict:
         t = _lib.BatchTuning()
         _check(_lib.lib.plis_batch_get_tuning(self._h, ctypes.byref(t)))

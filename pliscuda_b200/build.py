@@ -35,7 +35,7 @@ SOURCES = ["inst_f64.cu", "inst_f32.cu", "batch_f64.cu", "batch_f32.cu", "engine
            "learned.cu",
            "capi.cpp", "loader.cpp", "simulate.cpp", "plis_model.cpp"]
 HEADERS = ["engine_kernels.cuh", "batch_kernels.cuh", "batch.h", "engine.cuh", "engine.h", "learned.h",
-           "tc_mlp.cuh", "plis_model.h", "plis_stream.h"]
+           "tc_mlp.cuh", "learned_dev.cuh", "plis_model.h", "plis_stream.h"]
 
 
 def _newest(paths):

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "batch.h"
+#include "learned.h"
 #include "batch_kernels.cuh"
 
 namespace plis {
@@ -236,7 +237,7 @@ int BatchEngine::create(const plis_batch_desc& d, const plis_options& opt) {
   }
   PLIS_CU(cudaMemcpy(d_ctrl_, h_ctrl_.data(), nrep_ * sizeof(Ctrl), cudaMemcpyHostToDevice));
   pending_.assign(nrep_, 2);  // 2 = never given a state
-  launch_ = (opt.precision == PLIS_PREC_FP32) ? batch_pick_f32(S_) : batch_pick_f64(S_);
+  launch_ = (opt.precision == PLIS_PREC_FP32) ? batch_pick_f32(S_, false) : batch_pick_f64(S_, false);
   int tile[3] = {opt.tile[0], opt.tile[1], opt.tile[2]};
   if (tile[0] <= 0 || tile[1] <= 0 || tile[2] <= 0) { tile[0] = 8; tile[1] = 8; tile[2] = 4; }
   rc = layout(tile);
@@ -284,6 +285,10 @@ int BatchEngine::layout(const int tile[3]) {
     if ((rc = dmalloc((void**)&d_slot_bad_, (size_t)total_tiles_ * 4))) return rc;
     max_tiles_ = total_tiles_;
   }
+  if (learned_ && total_tiles_ > plain_tiles_) {
+    if ((rc = dmalloc((void**)&d_slot_plain_, (size_t)total_tiles_ * 8))) return rc;
+    plain_tiles_ = total_tiles_;
+  }
   std::vector<KArgs> views(nrep_);
   const size_t rsz = opt_.precision == PLIS_PREC_FP32 ? sizeof(float) : sizeof(double);
   for (uint32_t r = 0; r < nrep_; ++r) {
@@ -310,6 +315,10 @@ int BatchEngine::layout(const int tile[3]) {
     v.b.slot_cr = d_slot_cr_ + rep[r].tile_off;
     v.b.slot_bad = d_slot_bad_ + rep[r].tile_off;
     v.b.ctrl = d_ctrl_ + r;
+    if (learned_) {
+      v.b.lp = d_lp_;
+      v.b.slot_tau_plain = d_slot_plain_ + rep[r].tile_off;
+    }
   }
   PLIS_CU(cudaMemcpy(d_views_, views.data(), nrep_ * sizeof(KArgs), cudaMemcpyHostToDevice));
   PLIS_CU(cudaMemcpy(d_rep_, rep.data(), nrep_ * sizeof(RepDesc), cudaMemcpyHostToDevice));
@@ -369,6 +378,43 @@ int BatchEngine::launch(uint32_t max_iters) {
                                       batch_dyn_smem(geo_.box_bytes, nrep_), stream_));
   launches_ += 1;
   return PLIS_OK;
+}
+
+int BatchEngine::set_proposer(const float* weights, double s_max) {
+  const bool on = weights != nullptr && s_max > 0.0;
+  if (on) {
+    if (opt_.mode != PLIS_MODE_CORRECTED) { err_ = "learned tau proposals need corrected mode"; return PLIS_ERR_UNSUPPORTED; }
+    if (s_max < 1.0) { err_ = "s_max must be >= 1"; return PLIS_ERR_INVALID; }
+    if (S_ > 4) { err_ = "learned tau proposals support up to 4 species"; return PLIS_ERR_LIMIT; }
+    int rc;
+    if (!d_lp_) {
+      if ((rc = dmalloc((void**)&d_lp_, sizeof(LearnedParams)))) return rc;
+      if ((rc = dmalloc((void**)&d_lw_, PLIS_PROPOSER_WEIGHTS * sizeof(float)))) return rc;
+    }
+    PLIS_CU(cudaMemcpyAsync(d_lw_, weights, PLIS_PROPOSER_WEIGHTS * sizeof(float), cudaMemcpyHostToDevice, stream_));
+    learned_pack(d_lw_, s_max, d_lp_, stream_);
+    PLIS_CU(cudaGetLastError());
+    PLIS_CU(cudaStreamSynchronize(stream_));
+  }
+  learned_ = on;
+  launch_ = (opt_.precision == PLIS_PREC_FP32) ? batch_pick_f32(S_, on) : batch_pick_f64(S_, on);
+  const int tile[3] = {(int)tile_[0], (int)tile_[1], (int)tile_[2]};
+  int rc = layout(tile);
+  if (rc) return rc;
+  // classify every replica's current state again (time, step and statistics are kept)
+  if ((rc = read_ctrls())) return rc;
+  for (uint32_t r = 0; r < nrep_; ++r) {
+    if (pending_[r] != 0) continue;
+    Ctrl& k = h_ctrl_[r];
+    if (k.status != PLIS_OK) continue;
+    k.phase = 0;
+    k.dt = 0.0;
+    k.done = 0;
+    pending_[r] = 1;
+    any_pending_ = true;
+  }
+  PLIS_CU(cudaMemcpy(d_ctrl_, h_ctrl_.data(), nrep_ * sizeof(Ctrl), cudaMemcpyHostToDevice));
+  return init_pending();
 }
 
 int BatchEngine::read_ctrls() {

@@ -21,8 +21,8 @@ struct BatchLaunch {
   void* kernel;        // k_batch<Real, MAXS>
   cudaError_t (*set_smem)(int bytes);
 };
-BatchLaunch batch_pick_f64(uint32_t S);
-BatchLaunch batch_pick_f32(uint32_t S);
+BatchLaunch batch_pick_f64(uint32_t S, bool learned);
+BatchLaunch batch_pick_f32(uint32_t S, bool learned);
 void batch_prepare(const BatchArgs& B, double t_end, unsigned long long n_steps, cudaStream_t s);
 
 class BatchEngine {
@@ -37,6 +37,8 @@ class BatchEngine {
   int stats(uint32_t r, plis_stats* st);
   int autotune(uint64_t pilot_steps, plis_batch_tuning* out);
   int tuning(plis_batch_tuning* out);
+  // learned tau proposals for every replica (corrected mode, <= 4 species); null / s_max <= 0 detaches
+  int set_proposer(const float* weights, double s_max);
   const std::string& error() const { return err_; }
 
  private:
@@ -89,6 +91,11 @@ class BatchEngine {
   std::vector<Ctrl> h_ctrl_;
   double device_ms_ = 0.0;
   uint64_t launches_ = 0;
+  bool learned_ = false;
+  struct LearnedParams* d_lp_ = nullptr;
+  float* d_lw_ = nullptr;
+  double* d_slot_plain_ = nullptr;
+  uint32_t plain_tiles_ = 0;
 };
 
 }  // namespace plis

@@ -22,6 +22,7 @@
 
 #include "batch.h"
 #include "engine_kernels.cuh"
+#include "learned_dev.cuh"
 
 namespace plis {
 
@@ -177,7 +178,9 @@ __device__ __forceinline__ uint32_t find_replica(const uint32_t* p, uint32_t n, 
 #ifndef PLIS_BATCH_MIN_BLOCKS
 #define PLIS_BATCH_MIN_BLOCKS 2
 #endif
-template <typename Real, int MAXS>
+// LEARNED: the classification phase takes learned tau proposals (learned_dev.cuh; corrected
+// semantics, every replica's view holds the proposer and its plain-min slots).
+template <typename Real, int MAXS, bool LEARNED>
 __global__ void __launch_bounds__(256, PLIS_BATCH_MIN_BLOCKS) k_batch(BatchArgs B) {
   extern __shared__ int32_t s_box[];
   const uint32_t nrep = B.nrep;
@@ -331,14 +334,18 @@ __global__ void __launch_bounds__(256, PLIS_BATCH_MIN_BLOCKS) k_batch(BatchArgs 
       const KArgs& sA = B.views[r];
       Ctrl* K = sA.b.ctrl;
       const ClassifyCtx C = classify_ctx(sA, K);
-      double tn;
-      long long ti;
-      int fl, bad;
-      bool valid;
       const uint32_t tile = w - s_cp[r];
-      classify_tile<Real, MAXS>(sA, tile, C, tn, ti, fl, bad, valid);
-      if (classify_slot(sA, K, tile, sA.g.nblocks, tn, ti, valid && fl == F_LEAP_CR, bad))
-        classify_control(sA, K, sA.g.nblocks);
+      if constexpr (LEARNED) {
+        if (learned_classify_tile<Real, MAXS>(sA, K, C, tile, sA.g.nblocks)) classify_control(sA, K, sA.g.nblocks);
+      } else {
+        double tn;
+        long long ti;
+        int fl, bad;
+        bool valid;
+        classify_tile<Real, MAXS>(sA, tile, C, tn, ti, fl, bad, valid);
+        if (classify_slot(sA, K, tile, sA.g.nblocks, tn, ti, valid && fl == F_LEAP_CR, bad))
+          classify_control(sA, K, sA.g.nblocks);
+      }
       __syncthreads();
     }
     if (!grid_barrier(B)) return;
@@ -347,21 +354,25 @@ __global__ void __launch_bounds__(256, PLIS_BATCH_MIN_BLOCKS) k_batch(BatchArgs 
   }
 }
 
-template <typename Real, int MAXS>
+template <typename Real, int MAXS, bool LEARNED>
 struct BatchKernelSet {
-  static void* kernel() { return (void*)&k_batch<Real, MAXS>; }
+  static void* kernel() { return (void*)&k_batch<Real, MAXS, LEARNED>; }
   static cudaError_t set_smem(int bytes) {
-    return cudaFuncSetAttribute(k_batch<Real, MAXS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return cudaFuncSetAttribute(k_batch<Real, MAXS, LEARNED>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   }
 };
 
-template <typename Real>
+template <typename Real, bool LEARNED>
 BatchLaunch batch_pick_impl(uint32_t S) {
-  if (S <= 1) return {BatchKernelSet<Real, 1>::kernel(), BatchKernelSet<Real, 1>::set_smem};
-  if (S <= 2) return {BatchKernelSet<Real, 2>::kernel(), BatchKernelSet<Real, 2>::set_smem};
-  if (S <= 4) return {BatchKernelSet<Real, 4>::kernel(), BatchKernelSet<Real, 4>::set_smem};
-  if (S <= 8) return {BatchKernelSet<Real, 8>::kernel(), BatchKernelSet<Real, 8>::set_smem};
-  return {BatchKernelSet<Real, 16>::kernel(), BatchKernelSet<Real, 16>::set_smem};
+  if (S <= 1) return {BatchKernelSet<Real, 1, LEARNED>::kernel(), BatchKernelSet<Real, 1, LEARNED>::set_smem};
+  if (S <= 2) return {BatchKernelSet<Real, 2, LEARNED>::kernel(), BatchKernelSet<Real, 2, LEARNED>::set_smem};
+  if (S <= 4) return {BatchKernelSet<Real, 4, LEARNED>::kernel(), BatchKernelSet<Real, 4, LEARNED>::set_smem};
+  if constexpr (LEARNED) {
+    return {nullptr, nullptr};  // learned proposals: up to 4 species
+  } else {
+    if (S <= 8) return {BatchKernelSet<Real, 8, false>::kernel(), BatchKernelSet<Real, 8, false>::set_smem};
+    return {BatchKernelSet<Real, 16, false>::kernel(), BatchKernelSet<Real, 16, false>::set_smem};
+  }
 }
 
 }  // namespace plis

@@ -398,6 +398,13 @@ int plis_batch_get_tuning(plis_batch* b, plis_batch_tuning* out) {
   PLIS_GUARD_END
 }
 
+int plis_batch_set_proposer(plis_batch* b, const float* weights, double s_max) {
+  PLIS_GUARD_BEGIN
+  if (!b) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return bfail(b, b->eng.set_proposer(weights, s_max));
+  PLIS_GUARD_END
+}
+
 int plis_canonical_neighbours(uint32_t n, const uint32_t* table, const uint32_t lattice_in[3], uint32_t* canonical,
                               uint32_t lattice_out[3]) {
   PLIS_GUARD_BEGIN

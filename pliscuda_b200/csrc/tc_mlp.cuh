@@ -126,7 +126,7 @@ static_assert(kPSmemBytes * 6 > 228 * 1024, "at most 5 CTAs per SM");
 // y[r] for the rows of `feats` (normalised BF16 features, 16 bytes per row, rows 0 .. 128*ntiles-1
 // readable) with the MLP on tcgen05.  Tiles are taken round robin; every CTA loads the weights once.
 // A wait that runs out sets *status and the CTA stops; TMEM is always freed.
-__device__ void mlp_tiles(const Params& P, const uint4* __restrict__ feats, float* __restrict__ y, uint32_t nrows,
+static __device__ void mlp_tiles(const Params& P, const uint4* __restrict__ feats, float* __restrict__ y, uint32_t nrows,
                           uint32_t ntiles, uint8_t* smem, int* status) {
   __shared__ int s_err;
   const uint32_t tid = threadIdx.x;  // blockDim.x == 128

@@ -97,3 +97,58 @@ def test_batch_autotune_keeps_state_and_trajectory():
             o = _oracle(m, st, r, 0, 0, 2)
             o.run(0.2)
             _same(b, r, o, "after autotune")
+
+
+def _proposer_weights(seed=7):
+    from test_learned_gpu import random_weights
+    w = random_weights(seed, scale=2.0)
+    w[8960] = 1.0  # proposals well above the plain bound for many subvolumes
+    return w
+
+
+@pytest.mark.parametrize("family", ["schlogl", "brusselator"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_batch_with_a_proposer_matches_single_handles(family, precision):
+    """Learned tau in the batched form: every replica equals, bit for bit, a single handle with the
+    same proposer (mma.sync MLP), the same seed and its replica id."""
+    from pliscuda_b200 import Simulation, workloads
+    from pliscuda_b200.batch import Batch
+    if family == "schlogl":
+        reps = [workloads.schlogl(side) for side in (5, 8, 11)]
+    else:
+        reps = _replicas(4)
+    w = _proposer_weights()
+    with Batch.from_models([m for m, _ in reps], mode="corrected", precision=precision, seed=13) as b:
+        for i, (_, st) in enumerate(reps):
+            b.set_state(i, st)
+        b.set_proposer(w, 8.0)
+        b.step(25)
+        for r, (m, st) in enumerate(reps):
+            with Simulation(m, mode="corrected", precision=precision, seed=13, replica=r, learned_mlp="mma.sync") as s:
+                s.set_state(st)
+                s.set_proposer(w, 8.0)
+                s.step(25)
+                assert np.array_equal(b.get_state(r), s.get_state()), f"replica {r}"
+                gt, gf = b.taus(r)
+                et, ef = s.taus()
+                assert np.array_equal(gf, ef) and np.array_equal(bits(gt), bits(et)), f"replica {r}"
+                x, y = b.stats(r), s.stats()
+                assert (x.steps, x.rollbacks, x.events, x.exact_events) == (y.steps, y.rollbacks, y.events, y.exact_events)
+                assert bits(np.array([x.time]))[0] == bits(np.array([y.time]))[0]
+
+
+def test_batch_proposer_with_unit_clamp_is_the_plain_batch():
+    from pliscuda_b200.batch import Batch
+    reps = _replicas(3)
+    w = _proposer_weights()
+    out = []
+    for prop in (False, True):
+        with Batch.from_models([m for m, _ in reps], mode="corrected", seed=21) as b:
+            for i, (_, st) in enumerate(reps):
+                b.set_state(i, st)
+            if prop:
+                b.set_proposer(w, 1.0)
+            b.run(0.3)
+            out.append([(b.get_state(r).copy(), b.stats(r).steps, b.stats(r).events) for r in range(len(reps))])
+    for (x0, s0, e0), (x1, s1, e1) in zip(*out):
+        assert np.array_equal(x0, x1) and s0 == s1 and e0 == e1
