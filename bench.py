@@ -298,7 +298,8 @@ def learned_report():
     plain method's are admissible, the fastest of them is kept.  Measurement on Schlogl 128^3
     (2,097,152 subvolumes): plain and learned runs to t = 20 with checkpoints every 1.0; events/s and
     sim-time/s from CUDA-event device time; KS of the pooled subvolume counts at every checkpoint;
-    rollbacks among all attempts."""
+    rollbacks among all attempts.  The batched form (the persistent kernel) runs the same comparison
+    with the chosen proposer: plain batch against learned batch, KS against the plain run."""
     from pliscuda_b200 import workloads
     from pliscuda_b200.learned import _ks_per_checkpoint, _run_to_checkpoints, calibrate, train_proposer
     m64, s64 = workloads.schlogl(64)
@@ -326,7 +327,35 @@ def learned_report():
     out.update({"learned": lt, "ks": [round(k, 5) for k in ks], "ks_max": max(ks), "ks_bound": 0.02,
                 "speedup_events_per_s": lt["events_per_s"] / pt["events_per_s"],
                 "speedup_sim_time_per_s": lt["sim_time_per_s"] / pt["sim_time_per_s"]})
+    # the batched form (the persistent kernel, MLP by mma.sync) on the same workload: plain and learned
+    pbs, pb = _batch_to_checkpoints(m128, s128, cps, seed=13)
+    lbs, lb = _batch_to_checkpoints(m128, s128, cps, seed=14, weights=w, s_max=s_max)
+    ksb = _ks_per_checkpoint(ps, lbs)
+    out["batched_form"] = {"plain": pb, "learned": lb, "ks_max_vs_plain": max(ksb),
+                           "speedup_events_per_s": lb["events_per_s"] / pb["events_per_s"],
+                           "learned_vs_plain_multi_kernel": lb["events_per_s"] / pt["events_per_s"]}
     return out
+
+
+def _batch_to_checkpoints(model, state, checkpoints, *, seed, weights=None, s_max=0.0):
+    """One replica in the batched persistent kernel (corrected, FP64) to each checkpoint: counts at
+    each and the run's totals (CUDA-event device time)."""
+    from pliscuda_b200.batch import Batch
+    S, N = model.n_species, model.n_subvolumes
+    with Batch.from_models([model], mode="corrected", seed=seed) as b:
+        b.set_state(0, state)
+        if weights is not None:
+            b.set_proposer(weights, s_max)
+        snaps = []
+        for t in checkpoints:
+            b.run(float(t))
+            snaps.append(b.get_state(0).reshape(S, N).copy())
+        st = b.stats(0)
+        tot = {"steps": int(st.steps), "events": int(st.events), "rollbacks": int(st.rollbacks),
+               "device_ms": float(st.device_ms), "time": float(st.time)}
+    tot["events_per_s"] = tot["events"] / (tot["device_ms"] * 1e-3)
+    tot["sim_time_per_s"] = tot["time"] / (tot["device_ms"] * 1e-3)
+    return snaps, tot
 
 
 def batch_report(t0: float = 0.001, t1: float = 0.006):
