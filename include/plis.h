@@ -183,6 +183,39 @@ int plis_get_profile(plis_handle* h, plis_profile* out);
 /* Inspection: per-subvolume tau (binary64) and operation flags of the current state. */
 int plis_get_taus(plis_handle* h, double* tau, uint8_t* flags);
 
+/* Event log.  The reference's LOG build prints one line per event from inside its kernels
+ * (leap.cu:29-32, 58-62, 144-146, 196-198; ssa.cu:69-71, 96-98).  Here the kernels append one
+ * 32-byte record per event to a device buffer of the handle, read back on the host between calls.
+ * The records of one step come in no particular order.  Every attempt of a step is logged, the
+ * discarded ones included (their `attempt` is below the step's last), as the reference prints
+ * before its rollback check (driver.cu:292-315).  An event is a leap draw with count > 0 or one
+ * exact event that changed the state. */
+typedef struct plis_event_record {
+  double time;        /* simulated time at the start of the step */
+  uint64_t step;      /* number of the step (1 = the first step of the handle) */
+  uint32_t subvolume; /* where the event happened: the source of a diffusion */
+  uint32_t target;    /* destination subvolume of a diffusion; = subvolume for a reaction */
+  uint32_t count;     /* firings, or molecules moved (exact events: 1); saturated at 2^32-1 */
+  uint16_t channel;   /* reaction index, or species index of a diffusion */
+  uint8_t kind;       /* PLIS_EVENT_* */
+  uint8_t attempt;    /* rollback attempt of the step, 0 first (saturated at 255) */
+} plis_event_record;
+#define PLIS_EVENT_LEAP_REACTION 1      /* Poisson firings of one reaction (leap.cu:29-32) */
+#define PLIS_EVENT_LEAP_DIFFUSION 2     /* Poisson jumps of one species to one neighbour (leap.cu:58-62) */
+#define PLIS_EVENT_CRITICAL_REACTION 3  /* critical reaction of a LEAP_CR subvolume (leap.cu:144-146) */
+#define PLIS_EVENT_CRITICAL_DIFFUSION 4 /* critical jump of a LEAP_CR subvolume (leap.cu:196-198) */
+#define PLIS_EVENT_SSA_REACTION 5       /* exact reaction of the arg-min subvolume (ssa.cu:69-71) */
+#define PLIS_EVENT_SSA_DIFFUSION 6      /* exact jump of the arg-min subvolume (ssa.cu:96-98) */
+/* Room for `capacity` records on the device (0 turns the log off and frees it); the log starts
+ * empty.  Events past the capacity are counted, not stored. */
+int plis_set_event_log(plis_handle* h, uint64_t capacity);
+/* Copies min(stored, max_records) records, in the order they were appended, into out (may be NULL
+ * when max_records is 0); *n_records = records stored (<= capacity), *n_dropped = events not
+ * stored for lack of room since the log was last emptied.  clear != 0 empties the log afterwards.
+ * A handle without a log reports 0 and 0. */
+int plis_read_event_log(plis_handle* h, plis_event_record* out, uint64_t max_records, uint64_t* n_records,
+                        uint64_t* n_dropped, int clear);
+
 /* Arg-min of a device array of n taus (first index on ties) into *d_min_tau / *d_argmin, enqueued
  * on `stream` (a cudaStream_t, NULL for the default stream); the same global min-tau reduction the
  * step does internally.  No counterpart in the reference: it exists for callers that cannot allocate

@@ -71,8 +71,17 @@ def lib():
         L.oracle_get_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(Stats)]
         L.oracle_advance.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_uint64]
         L.oracle_advance.restype = ctypes.c_int
+        L.oracle_set_event_log.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.oracle_read_event_log.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64]
+        L.oracle_read_event_log.restype = ctypes.c_int64
         _lib = L
     return _lib
+
+
+# one logged event (oracle_event in plis_oracle.h; the library's plis_event_record)
+EVENT_DTYPE = np.dtype([("time", "<f8"), ("step", "<u8"), ("subvolume", "<u4"), ("target", "<u4"),
+                        ("count", "<u4"), ("channel", "<u2"), ("kind", "u1"), ("attempt", "u1")])
+assert EVENT_DTYPE.itemsize == 32
 
 
 def _p(a):
@@ -150,6 +159,17 @@ class Oracle:
         st = Stats()
         lib().oracle_get_stats(self._h, ctypes.byref(st))
         return st
+
+    def set_event_log(self, on=True):
+        """Record every event from now on (an empty log), or stop recording."""
+        lib().oracle_set_event_log(self._h, 1 if on else 0)
+
+    def read_event_log(self) -> np.ndarray:
+        """The events logged since the last read (EVENT_DTYPE records); empties the log."""
+        n = lib().oracle_read_event_log(self._h, None, 0)
+        out = np.zeros(n, EVENT_DTYPE)
+        lib().oracle_read_event_log(self._h, _p(out), n)
+        return out
 
 
 # ---------------------------------------------------------------------------------------------

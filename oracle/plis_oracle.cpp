@@ -104,6 +104,25 @@ struct Base {
   virtual int get_taus(double*, uint8_t*) = 0;
   virtual int advance(double, uint64_t) = 0;
   oracle_stats st{};
+  bool logging = false;
+  std::vector<oracle_event> log;
+  void note(uint64_t step, uint32_t attempt, uint32_t c, uint32_t target, int64_t count, uint32_t channel, int kind) {
+    if (!logging) return;
+    log.push_back(event(st.time, step, attempt, c, target, count, channel, kind));
+  }
+  static oracle_event event(double t, uint64_t step, uint32_t attempt, uint32_t c, uint32_t target, int64_t count,
+                            uint32_t channel, int kind) {
+    oracle_event e;
+    e.time = t;
+    e.step = step;
+    e.subvolume = c;
+    e.target = target;
+    e.count = count > 0xFFFFFFFFll ? 0xFFFFFFFFu : (uint32_t)count;
+    e.channel = (uint16_t)channel;
+    e.kind = (uint8_t)kind;
+    e.attempt = attempt > 255u ? (uint8_t)255 : (uint8_t)attempt;
+    return e;
+  }
 };
 
 template <typename Real>
@@ -119,6 +138,7 @@ struct Sim : Base {
   std::vector<uint8_t> leaped;            // leap: this cell marks its receivers
   std::vector<int64_t> evc;               // leap: events per cell
   std::vector<uint8_t> bigc;              // leap: a draw too large for 32-bit accumulation
+  std::vector<std::vector<oracle_event>> cell_log;  // leap: events per cell (event log on)
   uint8_t leap_big = 0;
   double ff_tau = 0.0;                    // fast-forward decrement (reference: min_tau, driver.cu:333)
   int64_t ff_argmin = -1;
@@ -387,12 +407,14 @@ struct Sim : Base {
     std::fill(own.begin(), own.end(), 0);
     std::fill(outk.begin(), outk.end(), 0);
     std::fill(leaped.begin(), leaped.end(), 0);
+    if (logging && cell_log.size() != N) cell_log.assign(N, {});
 #pragma omp parallel for schedule(dynamic, 64)
     for (int64_t ci = 0; ci < (int64_t)N; ++ci) {
       uint32_t c = (uint32_t)ci;
       int64_t ev = 0;
       evc[c] = 0;
       bigc[c] = 0;
+      if (logging) cell_log[c].clear();
       if (flag[c] == SSA || flag[c] == SSA_FF) continue;  // leap.cu:9-10
       uint8_t big = 0;
       for (uint32_t r = 0; r < R; ++r) {
@@ -409,6 +431,7 @@ struct Sim : Base {
           k = Ops::count(Ops::poisson(&sr, lam));
         }
         ev += k;
+        if (logging && k > 0) cell_log[c].push_back(event(st.time, step, attempt, c, c, k, r, 1));
         for (auto& e : rx[r].net) {
           int64_t v = k * e.second;
           if (v >= kBigDraw || v <= -kBigDraw) big = 1;
@@ -432,6 +455,7 @@ struct Sim : Base {
             k = Ops::count(Ops::poisson_shared(&sd, lam, em));
           }
           if (k >= kBigJump) big = 1;
+          if (logging && k > 0) cell_log[c].push_back(event(st.time, step, attempt, c, nbr[(size_t)c * 6 + j], k, s, 2));
           outk[((size_t)c * S + s) * 6 + j] = k;
           own[(size_t)c * S + s] -= k;
           ev += k;
@@ -449,6 +473,8 @@ struct Sim : Base {
     for (uint32_t c = 0; c < N; ++c) leap_big |= bigc[c];
     int64_t events = 0;
     for (uint32_t c = 0; c < N; ++c) events += evc[c];
+    if (logging)
+      for (uint32_t c = 0; c < N; ++c) log.insert(log.end(), cell_log[c].begin(), cell_log[c].end());
     // gather: next = curr + own + inflow; receivers SSA_FF -> SSA
 #pragma omp parallel for schedule(static)
     for (int64_t ci = 0; ci < (int64_t)N; ++ci) {
@@ -513,6 +539,7 @@ struct Sim : Base {
         if (!fire) continue;
         for (auto& e : rx[ri].net) delta.push_back({(size_t)e.first * N + c, (int64_t)e.second});
         ++events;
+        note(step, attempt, c, c, 1, ri, 3);
       } else {
         Real scaled = dsum * u;
         Real partial = (Real)0;
@@ -537,6 +564,7 @@ struct Sim : Base {
           delta.push_back({(size_t)spi * N + c, -1});
           delta.push_back({(size_t)spi * N + target, 1});
           ++events;
+          note(step, attempt, c, target, 1, spi, 4);
           uint32_t q = orig.empty() ? nbr[target] : orig[target];  // leap.cu:192-193
           flag_sets.push_back(q);
         }
@@ -575,6 +603,7 @@ struct Sim : Base {
         if (ri == (uint32_t)-1) ri = 0;
         for (auto& e : rx[ri].net) delta.push_back({(size_t)e.first * N + m, (int64_t)e.second});
         flag[m] = SSA;  // ssa.cu:295
+        note(step, attempt, m, m, 1, ri, 5);
         return 1;
       }
       if (!(dtot > (Real)0)) return 0;
@@ -593,6 +622,7 @@ struct Sim : Base {
       delta.push_back({(size_t)spi * N + m, -1});
       delta.push_back({(size_t)spi * N + target, 1});
       if (flag[target] == SSA_FF) flag[target] = SSA;
+      note(step, attempt, m, target, 1, spi, 6);
       return 1;
     }
     // corrected: channel rates
@@ -631,8 +661,10 @@ struct Sim : Base {
     if (chosen_r < 0 && chosen_s < 0) {  // rounding left the walk short: take the last channel
       if (last_s >= 0) chosen_s = last_s; else chosen_r = last_r;
     }
+    const int kind_r = critical_only ? 3 : 5;
     if (chosen_r >= 0) {
       for (auto& e : rx[chosen_r].net) delta.push_back({(size_t)e.first * N + m, (int64_t)e.second});
+      note(step, attempt, m, m, 1, (uint32_t)chosen_r, kind_r);
       return 1;
     }
     plis_stream sd = plis_stream_make(opt.seed, opt.replica, m, PLIS_PHASE_SSA, step, attempt, 1);
@@ -643,6 +675,7 @@ struct Sim : Base {
     delta.push_back({(size_t)chosen_s * N + m, -1});
     delta.push_back({(size_t)chosen_s * N + target, 1});
     if (flag[target] == SSA_FF) flag[target] = SSA;
+    note(step, attempt, m, target, 1, (uint32_t)chosen_s, kind_r + 1);
     return 1;
   }
 
@@ -764,6 +797,19 @@ int oracle_get_stats(void* h, oracle_stats* st) {
 }
 int oracle_advance(void* h, double t_end, uint64_t max_steps) {
   return static_cast<Base*>(h)->advance(t_end, max_steps);
+}
+void oracle_set_event_log(void* h, int on) {
+  Base* b = static_cast<Base*>(h);
+  b->logging = on != 0;
+  b->log.clear();
+}
+int64_t oracle_read_event_log(void* h, oracle_event* out, int64_t max) {
+  Base* b = static_cast<Base*>(h);
+  const int64_t n = (int64_t)b->log.size();
+  if (!out) return n;
+  for (int64_t i = 0; i < n && i < max; ++i) out[i] = b->log[(size_t)i];
+  b->log.clear();
+  return n;
 }
 
 }  // extern "C"

@@ -66,6 +66,22 @@ int oracle_get_stats(void* h, oracle_stats* st);
 // Advance: stop after max_steps accepted steps or once time >= t_end (reference loop condition
 // driver.cu:259), whichever first.  In corrected mode the last step is clamped to land on t_end.
 int oracle_advance(void* h, double t_end, uint64_t max_steps);
+// Event log: one record per event, the layout of the library's plis_event_record (the reference
+// prints these events under LOG: leap.cu:29-32, 58-62, 144-146, 196-198; ssa.cu:69-71, 96-98).
+typedef struct oracle_event {
+  double time;          // simulated time at the start of the step
+  uint64_t step;
+  uint32_t subvolume;
+  uint32_t target;
+  uint32_t count;
+  uint16_t channel;
+  uint8_t kind;         // 1 leap reaction, 2 leap diffusion, 3/4 critical reaction/diffusion, 5/6 SSA
+  uint8_t attempt;
+} oracle_event;
+void oracle_set_event_log(void* h, int on);  // on != 0: record from now on; the log starts empty
+// returns the number of records logged; with out != NULL it also copies min(logged, max) of them
+// into out and empties the log
+int64_t oracle_read_event_log(void* h, oracle_event* out, int64_t max);
 
 #ifdef __cplusplus
 }

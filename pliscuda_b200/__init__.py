@@ -28,14 +28,14 @@ from typing import Optional, Sequence, Tuple
 import numpy as np
 
 from . import _lib
-from ._lib import (LEAP_CR, LEAP_NOCR, MODE_CORRECTED, MODE_REFERENCE, PREC_FP32, PREC_FP64, SSA, SSA_FF,
-                   STOP_ERROR, STOP_NO_EVENT, STOP_NONE, STOP_STEPS, STOP_TIME, PlisError)
+from ._lib import (EVENT_DTYPE, EVENT_KINDS, LEAP_CR, LEAP_NOCR, MODE_CORRECTED, MODE_REFERENCE, PREC_FP32,
+                   PREC_FP64, SSA, SSA_FF, STOP_ERROR, STOP_NO_EVENT, STOP_NONE, STOP_STEPS, STOP_TIME, PlisError)
 
 __all__ = [
     "Model", "Simulation", "PlisError", "InvalidArgument", "load_configuration", "run_simulation",
     "canonical_neighbours", "write_snapshot", "read_snapshot", "parse_topology", "parse_state", "parse_reactions",
     "LEAP_CR", "LEAP_NOCR", "SSA", "SSA_FF", "MODE_REFERENCE", "MODE_CORRECTED", "PREC_FP64", "PREC_FP32",
-    "STOP_NONE", "STOP_TIME", "STOP_STEPS", "STOP_NO_EVENT", "STOP_ERROR", "library_path",
+    "STOP_NONE", "STOP_TIME", "STOP_STEPS", "STOP_NO_EVENT", "STOP_ERROR", "EVENT_DTYPE", "EVENT_KINDS", "library_path",
 ]
 
 library_path = _lib.LIB_PATH
@@ -211,6 +211,22 @@ class Simulation:
         if w.size != _lib.PROPOSER_WEIGHTS:
             raise InvalidArgument(1, f"proposer weights must hold {_lib.PROPOSER_WEIGHTS} floats, got {w.size}")
         _check(_lib.lib.plis_set_proposer(self._h, _c(w), float(s_max)))
+
+    # -- event log
+    def set_event_log(self, capacity: int) -> None:
+        """Keep room for `capacity` event records on the device (0 turns the log off).  Every event
+        of the following steps is appended: the events the reference's LOG build prints."""
+        _check(_lib.lib.plis_set_event_log(self._h, int(capacity)))
+
+    def read_event_log(self, clear: bool = True) -> Tuple[np.ndarray, int]:
+        """(records, dropped): the stored records (EVENT_DTYPE, in append order) and the number of
+        events not stored because the log was full.  clear empties the log."""
+        n, dropped = ctypes.c_uint64(), ctypes.c_uint64()
+        _check(_lib.lib.plis_read_event_log(self._h, None, 0, ctypes.byref(n), ctypes.byref(dropped), 0))
+        out = np.zeros(n.value, dtype=_lib.EVENT_DTYPE)
+        _check(_lib.lib.plis_read_event_log(self._h, _c(out) if n.value else None, n.value, ctypes.byref(n),
+                                            ctypes.byref(dropped), 1 if clear else 0))
+        return out, int(dropped.value)
 
     def kernel_profile(self) -> dict:
         """{kernel: (total ms, launches)} of profiled calls (profile=True)."""

@@ -79,6 +79,12 @@ import numpy as _np  # noqa: E402
 TRACE_DTYPE = _np.dtype([("features", "<f4", (8,)), ("tau_cao", "<f4"), ("tau_step", "<f4"), ("label", "<f4"),
                          ("subvolume", "<u4"), ("counts", "<i4", (4,))])
 assert TRACE_DTYPE.itemsize == 64
+# plis_event_record (32 bytes) and its kinds
+EVENT_DTYPE = _np.dtype([("time", "<f8"), ("step", "<u8"), ("subvolume", "<u4"), ("target", "<u4"),
+                         ("count", "<u4"), ("channel", "<u2"), ("kind", "u1"), ("attempt", "u1")])
+assert EVENT_DTYPE.itemsize == 32
+EVENT_KINDS = {1: "leap_reaction", 2: "leap_diffusion", 3: "critical_reaction", 4: "critical_diffusion",
+               5: "ssa_reaction", 6: "ssa_diffusion"}
 
 
 class ConfigView(ctypes.Structure):
@@ -110,6 +116,8 @@ def _load() -> ctypes.CDLL:
         "plis_step": (i32, [vp, u64]),
         "plis_get_stats": (i32, [vp, P(Stats)]),
         "plis_get_taus": (i32, [vp, vp, vp]),
+        "plis_set_event_log": (i32, [vp, u64]),
+        "plis_read_event_log": (i32, [vp, vp, u64, P(u64), P(u64), i32]),
         "plis_get_profile": (i32, [vp, P(Profile)]),
         "plis_tau_argmin_noalloc": (i32, [vp, u64, vp, vp, vp]),
         "plis_batch_create": (i32, [P(BatchDesc), P(Options), P(vp)]),

@@ -243,10 +243,11 @@ __global__ void __launch_bounds__(256, PLIS_BATCH_MIN_BLOCKS) k_batch(BatchArgs 
         L.flag = sA.b.flag[K->tf];
         L.step = K->step + 1;
         L.attempt = K->attempt;
+        L.t = K->t;
         const Real tl = (Real)K->tau_leap;
         long long ev;
         int big;
-        leap_tile<Real, MAXS>(sA, w - s_lp[r], L, tl, box, ev, big);
+        leap_tile<Real, MAXS, false>(sA, w - s_lp[r], L, tl, box, ev, big);
         ev = warp_sum(ev);  // events by warp, straight into the replica's counter (integer: order-free)
         if ((threadIdx.x & 31) == 0 && ev) atomicAdd(&K->ev_attempt, (unsigned long long)ev);
         if (big) atomicOr(&K->blocks_done, 0x80000000u);  // rare: an oversized draw forces a rollback
@@ -277,7 +278,7 @@ __global__ void __launch_bounds__(256, PLIS_BATCH_MIN_BLOCKS) k_batch(BatchArgs 
           if (cell_of(sA, item, cl) && flag[cl.c] == F_LEAP_CR) {
             Counts<MAXS> x;
             load_counts(sA.m, Xc, cl.c, x);
-            fired += critical_event_ref<Real>(sA, cl.c, x, Xt, step, attempt, sA.b.D, flag);
+            fired += critical_event_ref<Real, false>(sA, cl.c, x, Xt, step, attempt, sA.b.D, flag);
           }
         }
         if ((ex & 2u) && item == 0 && threadIdx.x == 0) {
@@ -287,11 +288,11 @@ __global__ void __launch_bounds__(256, PLIS_BATCH_MIN_BLOCKS) k_batch(BatchArgs 
           load_counts(sA.m, Xc, am, x);
           int32_t* dst = (ex & 1u) ? sA.b.D : Xt;
           if (sA.o.mode == 0) {
-            if (fa == F_SSA || fa == F_SSA_FF) fired += argmin_event<Real>(sA, am, x, step, attempt, dst, flag, false);
+            if (fa == F_SSA || fa == F_SSA_FF) fired += argmin_event<Real, false>(sA, am, x, step, attempt, dst, flag, false);
           } else if (fa == F_LEAP_CR) {
-            fired += argmin_event<Real>(sA, am, x, step, attempt, dst, flag, true);
+            fired += argmin_event<Real, false>(sA, am, x, step, attempt, dst, flag, true);
           } else if (fa == F_SSA || fa == F_SSA_FF) {
-            fired += argmin_event<Real>(sA, am, x, step, attempt, dst, flag, false);
+            fired += argmin_event<Real, false>(sA, am, x, step, attempt, dst, flag, false);
           }
         }
         if (fired) {  // exact events are rare: one atomic per firing thread

@@ -187,6 +187,21 @@ int plis_get_taus(plis_handle* h, double* tau, uint8_t* flags) {
   PLIS_GUARD_END
 }
 
+int plis_set_event_log(plis_handle* h, uint64_t capacity) {
+  PLIS_GUARD_BEGIN
+  if (!h) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return fail(h, h->eng.set_event_log(capacity));
+  PLIS_GUARD_END
+}
+
+int plis_read_event_log(plis_handle* h, plis_event_record* out, uint64_t max_records, uint64_t* n_records,
+                        uint64_t* n_dropped, int clear) {
+  PLIS_GUARD_BEGIN
+  if (!h || !n_records || !n_dropped) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return fail(h, h->eng.read_event_log(out, max_records, n_records, n_dropped, clear != 0));
+  PLIS_GUARD_END
+}
+
 // ---------------------------------------------------------------------------------------------- learned tau
 static int lfail(plis_learner* L, int rc) {
   if (rc != PLIS_OK) g_err = L->l.error();

@@ -41,6 +41,10 @@ Engine::~Engine() { release(); }
 void Engine::release() {
   if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
   graph_exec_ = nullptr;
+  if (d_evrec_) cudaFree(d_evrec_);
+  if (d_evhead_) cudaFree(d_evhead_);
+  d_evrec_ = nullptr;
+  d_evhead_ = nullptr;
   for (void* p : allocs_) cudaFree(p);
   allocs_.clear();
   if (h_ctrl_) cudaFreeHost(h_ctrl_);
@@ -422,6 +426,52 @@ int Engine::get_taus(double* tau, uint8_t* flags) {
   if (tau) PLIS_CU(cudaMemcpyAsync(tau, args_.b.tau[tf], (size_t)args_.m.N * 8, cudaMemcpyDeviceToHost, stream_));
   if (flags) PLIS_CU(cudaMemcpyAsync(flags, args_.b.flag[tf], args_.m.N, cudaMemcpyDeviceToHost, stream_));
   PLIS_CU(cudaStreamSynchronize(stream_));
+  return PLIS_OK;
+}
+
+int Engine::set_event_log(uint64_t capacity) {
+  if (capacity > (1ull << 36)) { err_ = "event log capacity above 2^36 records"; return PLIS_ERR_LIMIT; }
+  PLIS_CU(cudaSetDevice(opt_.device));
+  PLIS_CU(cudaStreamSynchronize(stream_));
+  if (d_evrec_) cudaFree(d_evrec_);
+  if (d_evhead_) cudaFree(d_evhead_);
+  d_evrec_ = nullptr;
+  d_evhead_ = nullptr;
+  args_.b.ev = EvLog{nullptr, nullptr, 0};
+  if (capacity) {
+    PLIS_CU(cudaMalloc((void**)&d_evrec_, capacity * sizeof(EvRec)));
+    PLIS_CU(cudaMalloc((void**)&d_evhead_, sizeof(unsigned long long)));
+    PLIS_CU(cudaMemsetAsync(d_evhead_, 0, sizeof(unsigned long long), stream_));
+    PLIS_CU(cudaStreamSynchronize(stream_));
+    args_.b.ev = EvLog{d_evrec_, d_evhead_, (unsigned long long)capacity};
+  }
+  if (graph_exec_) {  // the graph holds the kernel arguments by value
+    cudaGraphExecDestroy(graph_exec_);
+    graph_exec_ = nullptr;
+  }
+  return PLIS_OK;
+}
+
+int Engine::read_event_log(plis_event_record* out, uint64_t max_records, uint64_t* n_records, uint64_t* n_dropped,
+                           bool clear) {
+  static_assert(sizeof(plis_event_record) == sizeof(EvRec), "record layouts differ");
+  *n_records = 0;
+  *n_dropped = 0;
+  if (!d_evhead_) return PLIS_OK;
+  unsigned long long head = 0;
+  PLIS_CU(cudaMemcpyAsync(&head, d_evhead_, sizeof head, cudaMemcpyDeviceToHost, stream_));
+  PLIS_CU(cudaStreamSynchronize(stream_));
+  const uint64_t cap = args_.b.ev.cap;
+  const uint64_t stored = head < cap ? head : cap;
+  const uint64_t n = stored < max_records ? stored : max_records;
+  if (n) {
+    if (!out) { err_ = "null record buffer"; return PLIS_ERR_INVALID; }
+    PLIS_CU(cudaMemcpyAsync(out, d_evrec_, n * sizeof(EvRec), cudaMemcpyDeviceToHost, stream_));
+  }
+  if (clear) PLIS_CU(cudaMemsetAsync(d_evhead_, 0, sizeof(unsigned long long), stream_));
+  PLIS_CU(cudaStreamSynchronize(stream_));
+  *n_records = stored;
+  *n_dropped = head - stored;
   return PLIS_OK;
 }
 

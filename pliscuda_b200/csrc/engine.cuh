@@ -74,6 +74,22 @@ struct DevModel {
   const void* dr;   // Real [C][S]
 };
 
+// Event log of a handle (plis_set_event_log): records of 32 bytes, laid out as plis_event_record;
+// rec == null when the log is off (the batched kernel never logs).
+struct alignas(16) EvRec {
+  double time;
+  unsigned long long step;
+  uint32_t subvolume, target, count;
+  uint16_t channel;
+  uint8_t kind, attempt;
+};
+static_assert(sizeof(EvRec) == 32, "EvRec must match plis_event_record");
+struct EvLog {
+  EvRec* rec;
+  unsigned long long* head;  // events appended since the log was emptied (may exceed cap)
+  unsigned long long cap;
+};
+
 struct DevBufs {
   int32_t* X[3];
   double* tau[2];
@@ -90,6 +106,7 @@ struct DevBufs {
   uint8_t* pre_kind;       // 1: fast-forwarded, 2: leap bound computed
   float* ymlp;             // MLP output per subvolume
   Ctrl* ctrl;
+  EvLog ev;                // event log (rec == null: off)
 };
 
 struct DevOpts {

@@ -41,6 +41,10 @@ class Engine {
   // the labels of those records once a step has been taken (leap condition at label_eps, 0 = epsilon)
   int trace_features(TraceRec* out, uint32_t offset, uint32_t stride, uint32_t count);
   int trace_label(TraceRec* recs, uint32_t count, double tau_step, double label_eps);
+  // event log (plis_set_event_log / plis_read_event_log)
+  int set_event_log(uint64_t capacity);
+  int read_event_log(plis_event_record* out, uint64_t max_records, uint64_t* n_records, uint64_t* n_dropped,
+                     bool clear);
   int device() const { return opt_.device; }
   const std::string& error() const { return err_; }
   const Model& model() const { return model_; }
@@ -82,6 +86,8 @@ class Engine {
   double2* d_pre_ = nullptr;
   uint8_t* d_pre_kind_ = nullptr;
   float* d_ymlp_ = nullptr;
+  EvRec* d_evrec_ = nullptr;
+  unsigned long long* d_evhead_ = nullptr;
 };
 
 }  // namespace plis

@@ -24,6 +24,7 @@
 #ifndef PLIS_ENGINE_KERNELS_CUH_
 #define PLIS_ENGINE_KERNELS_CUH_
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include "../../include/plis.h"
@@ -44,6 +45,28 @@ namespace plis {
 __device__ __forceinline__ void pdl_entry() {
   asm volatile("griddepcontrol.wait;" ::: "memory");
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// One event record appended to the log.  The threads that reach this call together reserve their
+// slots with one atomic per warp; slots past the capacity are counted in the head but not written.
+__device__ __forceinline__ void ev_put(const EvLog& L, double t, uint64_t step, uint32_t attempt, uint32_t cell,
+                                    uint32_t target, long long count, int channel, int kind) {
+  namespace cg = cooperative_groups;
+  const cg::coalesced_group g = cg::coalesced_threads();
+  unsigned long long base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(L.head, (unsigned long long)g.size());
+  base = g.shfl(base, 0) + g.thread_rank();
+  if (base >= L.cap) return;
+  EvRec r;
+  r.time = t;
+  r.step = step;
+  r.subvolume = cell;
+  r.target = target;
+  r.count = count > 0xFFFFFFFFll ? 0xFFFFFFFFu : (uint32_t)count;
+  r.channel = (uint16_t)channel;
+  r.kind = (uint8_t)kind;
+  r.attempt = attempt > 255u ? (uint8_t)255 : (uint8_t)attempt;
+  L.rec[base] = r;
 }
 
 template <typename Kern, typename... Args>
@@ -700,11 +723,12 @@ struct LeapCtx {
   uint8_t* flag;
   uint64_t step;
   uint32_t attempt;
+  double t;  // simulated time at the start of the step (event log)
 };
 
 // Leap of one brick (or one 1-D block of a table topology) by the whole CTA; returns this thread's
 // events and guard flag.  leap_step, leap.cu:3-65.
-template <typename Real, int MAXS>
+template <typename Real, int MAXS, bool LOG>
 __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const LeapCtx& L, Real tl, const Box& box,
                                           long long& ev, int& big) {
   const DevModel& m = A.m;
@@ -778,6 +802,7 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
           if (r >= R) continue;
           const long long k = act[i] ? ks[i] : kk[i];
           ev += k;
+          if (LOG && k > 0) ev_put(A.b.ev, L.t, step, attempt, c, c, k, r, PLIS_EVENT_LEAP_REACTION);
           const int nn = m.n_net[r];
           for (int q = 0; q < nn; ++q) {
             const long long v = k * (long long)m.net_nu[r * 8 + q];
@@ -806,6 +831,7 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
             if (box.acc) atomicAdd_block(&box.acc[s * box.size + own + box_offset(box, q.dir[j])], (int)k);
             else atomicAdd(&Xt[(size_t)s * m.Npad + q.nb[j]], (int)k);
             if (mode == 1 && flag[q.nb[j]] == F_SSA_FF) flag[q.nb[j]] = F_SSA;
+            if (LOG) ev_put(A.b.ev, L.t, step, attempt, c, q.nb[j], k, s, PLIS_EVENT_LEAP_DIFFUSION);
           }
           out += k;
         }
@@ -862,7 +888,7 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
   }
 }
 
-template <typename Real, int MAXS>
+template <typename Real, int MAXS, bool LOG>
 __global__ void __launch_bounds__(256, PLIS_LEAP_MIN_BLOCKS) k_leap(KArgs A) {
   pdl_entry();
   Ctrl* K = A.b.ctrl;
@@ -877,6 +903,7 @@ __global__ void __launch_bounds__(256, PLIS_LEAP_MIN_BLOCKS) k_leap(KArgs A) {
   L.flag = A.b.flag[K->tf];
   L.step = K->step + 1;
   L.attempt = K->attempt;
+  L.t = K->t;
   const Real tl = (Real)K->tau_leap;
   Box box;
   box.acc = A.g.staged ? s_box : nullptr;
@@ -887,7 +914,7 @@ __global__ void __launch_bounds__(256, PLIS_LEAP_MIN_BLOCKS) k_leap(KArgs A) {
   __syncthreads();
   long long ev;
   int big;
-  leap_tile<Real, MAXS>(A, blockIdx.x, L, tl, box, ev, big);
+  leap_tile<Real, MAXS, LOG>(A, blockIdx.x, L, tl, box, ev, big);
   // events and guard flags of the CTA
   ev = warp_sum(ev);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -909,7 +936,7 @@ __global__ void __launch_bounds__(256, PLIS_LEAP_MIN_BLOCKS) k_leap(KArgs A) {
 // exact events
 // ------------------------------------------------------------------------------------------------
 // Reference critical event of one LEAP_CR subvolume (leap.cu:86-199).
-template <typename Real, int MAXS>
+template <typename Real, bool LOG, int MAXS>
 __device__ int critical_event_ref(const KArgs& A, uint32_t c, const Counts<MAXS>& x, const int32_t* Xt,
                                   uint64_t step, uint32_t attempt, int32_t* D, uint8_t* flag) {
   const DevModel& m = A.m;
@@ -947,6 +974,7 @@ __device__ int critical_event_ref(const KArgs& A, uint32_t c, const Counts<MAXS>
     if (!fire) return 0;
     for (int i = 0; i < m.n_net[ri]; ++i)
       atomicAdd(&D[(size_t)m.net_s[ri * 8 + i] * m.Npad + c], (int)m.net_nu[ri * 8 + i]);
+    if (LOG) ev_put(A.b.ev, A.b.ctrl->t, step, attempt, c, c, 1, ri, PLIS_EVENT_CRITICAL_REACTION);
     return 1;
   }
   const Real scaled = dsum * u;
@@ -973,12 +1001,13 @@ __device__ int critical_event_ref(const KArgs& A, uint32_t c, const Counts<MAXS>
   atomicAdd(&D[(size_t)spi * m.Npad + target], 1);
   const uint32_t q = flat_table_entry(m, target);  // leap.cu:192-193
   if (flag[q] == F_SSA_FF) flag[q] = F_SSA;
+  if (LOG) ev_put(A.b.ev, A.b.ctrl->t, step, attempt, c, target, 1, spi, PLIS_EVENT_CRITICAL_DIFFUSION);
   return 1;
 }
 
 // Exact event of the arg-min subvolume: reference ssa_step (ssa.cu:270-324), or in corrected mode
 // an SSA over the critical channels (LEAP_CR) or over every channel (SSA subvolumes).
-template <typename Real, int MAXS>
+template <typename Real, bool LOG, int MAXS>
 __device__ int argmin_event(const KArgs& A, uint32_t mcell, const Counts<MAXS>& x, uint64_t step, uint32_t attempt,
                             int32_t* dst, uint8_t* flag, bool critical_only) {
   const DevModel& m = A.m;
@@ -1006,6 +1035,7 @@ __device__ int argmin_event(const KArgs& A, uint32_t mcell, const Counts<MAXS>& 
       for (int i = 0; i < m.n_net[ri]; ++i)
         atomicAdd(&dst[(size_t)m.net_s[ri * 8 + i] * m.Npad + mcell], (int)m.net_nu[ri * 8 + i]);
       flag[mcell] = F_SSA;  // ssa.cu:295
+      if (LOG) ev_put(A.b.ev, A.b.ctrl->t, step, attempt, mcell, mcell, 1, ri, PLIS_EVENT_SSA_REACTION);
       return 1;
     }
     if (!(dtot > (Real)0)) return 0;
@@ -1027,6 +1057,7 @@ __device__ int argmin_event(const KArgs& A, uint32_t mcell, const Counts<MAXS>& 
     atomicAdd(&dst[(size_t)spi * m.Npad + mcell], -1);
     atomicAdd(&dst[(size_t)spi * m.Npad + target], 1);
     if (flag[target] == F_SSA_FF) flag[target] = F_SSA;
+    if (LOG) ev_put(A.b.ev, A.b.ctrl->t, step, attempt, mcell, target, 1, spi, PLIS_EVENT_SSA_DIFFUSION);
     return 1;
   }
   Real total = (Real)0;
@@ -1062,9 +1093,11 @@ __device__ int argmin_event(const KArgs& A, uint32_t mcell, const Counts<MAXS>& 
     if (last_s >= 0) chosen_s = last_s;
     else chosen_r = last_r;
   }
+  const int kind_r = critical_only ? PLIS_EVENT_CRITICAL_REACTION : PLIS_EVENT_SSA_REACTION;
   if (chosen_r >= 0) {
     for (int i = 0; i < m.n_net[chosen_r]; ++i)
       atomicAdd(&dst[(size_t)m.net_s[chosen_r * 8 + i] * m.Npad + mcell], (int)m.net_nu[chosen_r * 8 + i]);
+    if (LOG) ev_put(A.b.ev, A.b.ctrl->t, step, attempt, mcell, mcell, 1, chosen_r, kind_r);
     return 1;
   }
   plis_stream sd = plis_stream_make(A.o.seed, A.o.replica, mcell, PLIS_PHASE_SSA, step, attempt, 1);
@@ -1075,10 +1108,11 @@ __device__ int argmin_event(const KArgs& A, uint32_t mcell, const Counts<MAXS>& 
   atomicAdd(&dst[(size_t)chosen_s * m.Npad + mcell], -1);
   atomicAdd(&dst[(size_t)chosen_s * m.Npad + target], 1);
   if (flag[target] == F_SSA_FF) flag[target] = F_SSA;
+  if (LOG) ev_put(A.b.ev, A.b.ctrl->t, step, attempt, mcell, target, 1, chosen_s, kind_r + 1);
   return 1;
 }
 
-template <typename Real, int MAXS>
+template <typename Real, int MAXS, bool LOG>
 __global__ void __launch_bounds__(256) k_exact(KArgs A) {
   pdl_entry();
   Ctrl* K = A.b.ctrl;
@@ -1097,7 +1131,7 @@ __global__ void __launch_bounds__(256) k_exact(KArgs A) {
     if (c < m.N && flag[c] == F_LEAP_CR) {
       Counts<MAXS> x;
       load_counts(m, Xc, c, x);
-      fired += critical_event_ref<Real>(A, c, x, Xt, step, attempt, A.b.D, flag);
+      fired += critical_event_ref<Real, LOG>(A, c, x, Xt, step, attempt, A.b.D, flag);
     }
   }
   if ((ex & 2u) && blockIdx.x == 0 && threadIdx.x == 0) {
@@ -1107,10 +1141,10 @@ __global__ void __launch_bounds__(256) k_exact(KArgs A) {
     load_counts(m, Xc, am, x);
     int32_t* dst = (ex & 1u) ? A.b.D : Xt;
     if (A.o.mode == 0) {
-      if (fa == F_SSA || fa == F_SSA_FF) fired += argmin_event<Real>(A, am, x, step, attempt, dst, flag, false);
+      if (fa == F_SSA || fa == F_SSA_FF) fired += argmin_event<Real, LOG>(A, am, x, step, attempt, dst, flag, false);
     } else {
-      if (fa == F_LEAP_CR) fired += argmin_event<Real>(A, am, x, step, attempt, dst, flag, true);
-      else if (fa == F_SSA || fa == F_SSA_FF) fired += argmin_event<Real>(A, am, x, step, attempt, dst, flag, false);
+      if (fa == F_LEAP_CR) fired += argmin_event<Real, LOG>(A, am, x, step, attempt, dst, flag, true);
+      else if (fa == F_SSA || fa == F_SSA_FF) fired += argmin_event<Real, LOG>(A, am, x, step, attempt, dst, flag, false);
     }
   }
   if (fired) {  // exact events are rare: one atomic per firing thread
@@ -1348,11 +1382,20 @@ __global__ void k_fill_tau(double* t, uint8_t* f, uint32_t n) {
 // kernel launchers of each (precision, species capacity)
 template <typename Real, int MAXS>
 struct KernelSet {
-  static void leap(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) { launch_pdl(k_leap<Real, MAXS>, g, b, a.g.box_bytes, s, a); }
-  static cudaError_t leap_smem(int bytes) {
-    return cudaFuncSetAttribute(k_leap<Real, MAXS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  // the event-log variants (LOG = true) only when the handle's log is on: the plain path carries no logging code
+  static void leap(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) {
+    if (a.b.ev.rec) launch_pdl(k_leap<Real, MAXS, true>, g, b, a.g.box_bytes, s, a);
+    else launch_pdl(k_leap<Real, MAXS, false>, g, b, a.g.box_bytes, s, a);
   }
-  static void exact(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) { launch_pdl(k_exact<Real, MAXS>, g, b, 0, s, a); }
+  static cudaError_t leap_smem(int bytes) {
+    cudaError_t e = cudaFuncSetAttribute(k_leap<Real, MAXS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_leap<Real, MAXS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  }
+  static void exact(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) {
+    if (a.b.ev.rec) launch_pdl(k_exact<Real, MAXS, true>, g, b, 0, s, a);
+    else launch_pdl(k_exact<Real, MAXS, false>, g, b, 0, s, a);
+  }
   static void classify(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) { launch_pdl(k_classify<Real, MAXS>, g, b, 0, s, a); }
 };
 
