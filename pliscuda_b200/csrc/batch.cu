@@ -303,6 +303,7 @@ int BatchEngine::layout(const int tile[3]) {
     v.o.replica = ids_[r];
     v.g = geo_;
     v.g.ntx = rep[r].ntx; v.g.nty = rep[r].nty; v.g.ntz = rep[r].ntz;
+    geo_divisors(v.g);
     v.g.nblocks = rep[r].ntiles;
     for (int i = 0; i < 3; ++i) v.b.X[i] = d_X_[i] + coff_[r];
     for (int i = 0; i < 2; ++i) {

@@ -163,6 +163,7 @@ int Engine::create(const Model& model, const plis_options& opt) {
     g.nblocks = (dm.N + 255) / 256;
     g.ntx = g.nblocks; g.nty = g.ntz = 1;
   }
+  geo_divisors(g);
 
   // buffers
   const size_t cells = (size_t)M.S * dm.Npad;

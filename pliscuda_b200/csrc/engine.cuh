@@ -119,6 +119,23 @@ struct DevOpts {
   uint32_t replica;
 };
 
+// Division by a divisor fixed at set-up, as one multiply-high, two adds and two shifts: exact for
+// every 32-bit numerator (Granlund and Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994, section 4: m' = floor(2^32 (2^l - d) / d) + 1 with l = ceil(log2 d),
+// q = (t + ((n - t) >> min(l, 1))) >> max(l - 1, 0), t = mulhi(m', n)).
+struct FastDiv {
+  uint32_t mul, sh1, sh2;
+};
+inline FastDiv fastdiv_make(uint32_t d) {  // d >= 1
+  uint32_t l = 0;
+  while (l < 32 && (1ull << l) < d) ++l;
+  FastDiv f;
+  f.mul = (uint32_t)((((1ull << l) - d) << 32) / d + 1);
+  f.sh1 = l < 1 ? l : 1;
+  f.sh2 = l > 1 ? l - 1 : 0;
+  return f;
+}
+
 struct Geo {
   uint32_t tx, ty, tz;     // lattice brick per CTA
   uint32_t ntx, nty, ntz;  // bricks per dimension
@@ -126,7 +143,15 @@ struct Geo {
   uint32_t threads;        // threads per CTA
   uint32_t staged;         // 1: the leap stages the brick + halo in shared memory
   uint32_t box_bytes;      // dynamic shared memory of the staged leap
+  FastDiv dtx, dty, dntx, dnty;  // divisions by tx, ty, ntx, nty (geo_divisors)
 };
+// Sets the divisors of g from its tx, ty, ntx, nty.
+inline void geo_divisors(Geo& g) {
+  g.dtx = fastdiv_make(g.tx ? g.tx : 1);
+  g.dty = fastdiv_make(g.ty ? g.ty : 1);
+  g.dntx = fastdiv_make(g.ntx ? g.ntx : 1);
+  g.dnty = fastdiv_make(g.nty ? g.nty : 1);
+}
 
 struct KArgs {
   DevModel m;

@@ -263,14 +263,19 @@ struct Cell {
   uint32_t x, y, z;  // lattice coordinates (lattice topology only)
 };
 
+__device__ __forceinline__ uint32_t fdiv(uint32_t n, const FastDiv& f) {
+  const uint32_t t = __umulhi(f.mul, n);
+  return (t + ((n - t) >> f.sh1)) >> f.sh2;
+}
+
 __device__ __forceinline__ bool cell_of(const KArgs& A, uint32_t block, Cell& cl) {
   if (A.m.lattice) {
     const uint32_t b = block, t = threadIdx.x;
     if (t >= A.g.tx * A.g.ty * A.g.tz) return false;  // block rounded up to whole warps
-    const uint32_t bx = b % A.g.ntx, br = b / A.g.ntx;
-    const uint32_t by = br % A.g.nty, bz = br / A.g.nty;
-    const uint32_t lx = t % A.g.tx, tr = t / A.g.tx;
-    const uint32_t ly = tr % A.g.ty, lz = tr / A.g.ty;
+    const uint32_t br = fdiv(b, A.g.dntx), bx = b - br * A.g.ntx;
+    const uint32_t bz = fdiv(br, A.g.dnty), by = br - bz * A.g.nty;
+    const uint32_t tr = fdiv(t, A.g.dtx), lx = t - tr * A.g.tx;
+    const uint32_t lz = fdiv(tr, A.g.dty), ly = tr - lz * A.g.ty;
     cl.x = bx * A.g.tx + lx;
     cl.y = by * A.g.ty + ly;
     cl.z = bz * A.g.tz + lz;
