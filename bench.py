@@ -61,9 +61,29 @@ def _peaks():
 
 
 # dram__bytes_read.sum + dram__bytes_write.sum per launch of the dominant kernel, from the committed
-# ncu capture of the same kernel on the same workload (profiles/k_leap_schlogl64.md: 2.49 MB read,
-# 0.22 MB written).  Keyed by (workload, semantics, precision, kernel); absent keys report null.
-NCU_TRAFFIC = {("schlogl64", "reference", "fp64", "leap"): (2.49e6 + 0.22e6, "profiles/k_leap_schlogl64.md")}
+# ncu capture of the same kernel on the same workload (profiles/k_leap_schlogl64.md: 2.53 MB read,
+# 0.48 MB written, mean of three launches).  Keyed by (workload, semantics, precision, kernel); absent
+# keys report null.
+NCU_TRAFFIC = {("schlogl64", "reference", "fp64", "leap"): (2.53e6 + 0.48e6, "profiles/k_leap_schlogl64.md")}
+# smsp__inst_executed.sum per launch (warp instructions) of the same capture.  The kernel is bound by
+# instruction issue and dependent latency, not by DRAM, so the line also reports the achieved warp-
+# instruction rate against the issue peak (148 SMs x 4 schedulers x the SM clock sampled during the
+# timed region).  The count is that of steps 41-43 from the initial state; later steps of the bench
+# trajectory draw from similar Poisson means, so the rate is an estimate.
+NCU_WARP_INSTR = {("schlogl64", "reference", "fp64", "leap"): (27.8e6, "profiles/k_leap_schlogl64.md")}
+SM_COUNT, SCHEDULERS_PER_SM = 148, 4
+
+def issue_roofline(instr, ms_launch, clocks):
+    """Achieved warp-instruction issue rate of the dominant kernel against the issue peak."""
+    n, src = instr
+    mhz = (clocks or {}).get("sm_mhz")
+    if n is None or not mhz:
+        return None
+    achieved = n / (ms_launch / 1e3)
+    peak = SM_COUNT * SCHEDULERS_PER_SM * mhz * 1e6
+    return {"achieved": achieved, "peak": peak, "unit": "warp instructions/s", "frac": achieved / peak,
+            "warp_instructions_per_launch": n, "source": src, "sm_mhz": mhz}
+
 
 WORKLOADS = {
     "schlogl64": "Schlogl bistable model, 262144 subvolumes (64^3 reflective lattice), 1 species, 4 reactions",
@@ -503,6 +523,7 @@ def main(argv=None):
     peak, peak_kind = _peaks()
     shares = {k: round(v[0] / max(1e-12, sum(x[0] for x in per.values())), 4) for k, v in per.items()}
     traffic = NCU_TRAFFIC.get((args.workload, args.mode, args.precision, dom), (None, None))
+    instr = NCU_WARP_INSTR.get((args.workload, args.mode, args.precision, dom), (None, None))
 
     # end to end through the C ABI with host buffers
     e2e = None
@@ -551,7 +572,7 @@ def main(argv=None):
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic[0], "traffic_source": traffic[1],
                          "algorithmic_bytes_per_launch": algo_bytes[dom], "ms_per_launch": ms_launch,
-                         "kernel_share": shares},
+                         "kernel_share": shares, "issue": issue_roofline(instr, ms_launch, ck)},
             "e2e": e2e,
             "cpu_baseline": cpu,
             "clocks": ck,
