@@ -174,14 +174,20 @@ __device__ __forceinline__ uint32_t find_replica(const uint32_t* p, uint32_t n, 
   return lo;
 }
 
-// One kernel holds every phase, so it needs more registers than the leap alone.
+// One kernel holds every phase, so it wants more registers than the leap alone (124 plain, 128
+// learned).  Capped at 64 (4 CTAs of 256 threads per SM) it spills about 1.4 KB per thread, and is
+// still faster: twice the resident warps hide more of the latency-bound phases than the spills cost.
 #ifndef PLIS_BATCH_MIN_BLOCKS
-#define PLIS_BATCH_MIN_BLOCKS 2
+#define PLIS_BATCH_MIN_BLOCKS 4
+#endif
+#ifndef PLIS_BATCH_MIN_BLOCKS_LEARNED
+#define PLIS_BATCH_MIN_BLOCKS_LEARNED 4
 #endif
 // LEARNED: the classification phase takes learned tau proposals (learned_dev.cuh; corrected
 // semantics, every replica's view holds the proposer and its plain-min slots).
 template <typename Real, int MAXS, bool LEARNED>
-__global__ void __launch_bounds__(256, PLIS_BATCH_MIN_BLOCKS) k_batch(BatchArgs B) {
+__global__ void __launch_bounds__(256, LEARNED ? PLIS_BATCH_MIN_BLOCKS_LEARNED : PLIS_BATCH_MIN_BLOCKS)
+    k_batch(BatchArgs B) {
   extern __shared__ int32_t s_box[];
   const uint32_t nrep = B.nrep;
   // plan: prefix sums over replicas of the work items of each phase
