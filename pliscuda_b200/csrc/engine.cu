@@ -164,6 +164,13 @@ int Engine::create(const Model& model, const plis_options& opt) {
     g.ntx = g.nblocks; g.nty = g.ntz = 1;
   }
   geo_divisors(g);
+  {  // the exact-event and apply kernels stride over the subvolumes with a few CTAs per SM: on most
+     // steps they find nothing to do, and an early exit costs per CTA
+    int nsm = 0;
+    PLIS_CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, opt.device));
+    const uint32_t need = (dm.N + 255) / 256, cap = 2u * (uint32_t)(nsm > 0 ? nsm : 1);
+    exact_blocks_ = need < cap ? need : cap;
+  }
 
   // buffers
   const size_t cells = (size_t)M.S * dm.Npad;
@@ -217,7 +224,7 @@ void Engine::launch_classify() {
 
 void Engine::enqueue_step() {
   const dim3 gc(args_.g.nblocks), bc(args_.g.threads);
-  const dim3 gx((args_.m.N + 255) / 256), bx(256);
+  const dim3 gx(exact_blocks_), bx(256);
   launch_.leap(args_, gc, bc, stream_);
   launch_.exact(args_, gx, bx, stream_);
   if (opt_.mode == PLIS_MODE_REFERENCE) launch_pdl(k_apply, gx, bx, 0, stream_, args_);
@@ -227,7 +234,7 @@ void Engine::enqueue_step() {
 // Profiled step: the same four launches with CUDA events between them, accumulated per kernel.
 int Engine::enqueue_step_profiled() {
   const dim3 gc(args_.g.nblocks), bc(args_.g.threads);
-  const dim3 gx((args_.m.N + 255) / 256), bx(256);
+  const dim3 gx(exact_blocks_), bx(256);
   for (auto& e : pev_)
     if (!e) PLIS_CU(cudaEventCreate(&e));
   PLIS_CU(cudaEventRecord(pev_[0], stream_));

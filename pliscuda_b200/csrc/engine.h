@@ -70,6 +70,7 @@ class Engine {
   std::vector<void*> allocs_;
   std::string err_;
   int graph_steps_ = 32;
+  uint32_t exact_blocks_ = 1;  // CTAs of k_exact / k_apply
   int kernels_per_step_ = 4;
   uint64_t launches_ = 0;
   double device_ms_ = 0.0;

@@ -1131,9 +1131,9 @@ __global__ void __launch_bounds__(256) k_exact(KArgs A) {
   const uint64_t step = K->step + 1;
   const uint32_t attempt = K->attempt;
   int fired = 0;
-  if (ex & 1u) {  // reference: every LEAP_CR subvolume
-    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < m.N && flag[c] == F_LEAP_CR) {
+  if (ex & 1u) {  // reference: every LEAP_CR subvolume (grid-stride: the grid is a few CTAs per SM)
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < m.N; c += gridDim.x * blockDim.x) {
+      if (flag[c] != F_LEAP_CR) continue;
       Counts<MAXS> x;
       load_counts(m, Xc, c, x);
       fired += critical_event_ref<Real, LOG>(A, c, x, Xt, step, attempt, A.b.D, flag);
@@ -1165,14 +1165,14 @@ __global__ void __launch_bounds__(256) k_apply(KArgs A) {
   if (K->done || !(K->exact & 1u)) return;
   const DevModel& m = A.m;
   int32_t* Xt = A.b.X[K->tgt];
-  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= m.N) return;
-  for (uint32_t s = 0; s < m.S; ++s) {
-    const size_t i = (size_t)s * m.Npad + c;
-    const int32_t v = A.b.D[i];
-    if (v) {
-      Xt[i] += v;
-      A.b.D[i] = 0;
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < m.N; c += gridDim.x * blockDim.x) {
+    for (uint32_t s = 0; s < m.S; ++s) {
+      const size_t i = (size_t)s * m.Npad + c;
+      const int32_t v = A.b.D[i];
+      if (v) {
+        Xt[i] += v;
+        A.b.D[i] = 0;
+      }
     }
   }
 }
