@@ -308,7 +308,7 @@ int plis_batch_set_proposer(plis_batch* b, const float* weights, double s_max);
  * change of any propensity over the step relative to max(eps_L * a_j, c_j) (the Cao leap
  * condition at tolerance eps_L measured on the realised step), clamped to [log(1/16), log(64)].
  * plis_learner_train fits the MLP to a quantile of the label (pinball loss, Adam) with
- * hand-written CUDA kernels.  The accuracy of a proposer is judged against the plain method
+ * hand-written CUDA kernels.  The accuracy of a proposer is measured against the plain method
  * (KS distance of the marginals at checkpoints), which fixes s_max.
  * ------------------------------------------------------------------------------------------- */
 #define PLIS_PROPOSER_WEIGHTS 8977 /* 8961 parameters, then 8 feature means and 8 inverse deviations */

@@ -16,7 +16,7 @@ plis_set_proposer in include/plis.h).
         sim.set_proposer(weights, 16.0)
         sim.run(20.0)
 
-The plain method is the judge of a proposer's error: calibrate() runs the plain method and each
+The plain method is the measure of a proposer's error: calibrate() runs the plain method and each
 candidate (weights, s_max) side by side to the same checkpoints, admits the candidates whose
 marginal distributions stay within the KS bound, and picks the fastest of those.
 """
@@ -184,7 +184,7 @@ def train_proposer(model: Model, state: np.ndarray, *, label_epsilon: float, n_s
 def calibrate(model: Model, state: np.ndarray, candidates: Sequence[Tuple[np.ndarray, float, object]], *,
               checkpoints: Sequence[float] = (1.0, 2.0, 3.0, 4.0, 5.0), bound: float = 0.02, margin: float = 0.75,
               precision: str = "fp64", device: int = 0) -> Tuple[Optional[int], Dict]:
-    """The plain method judges each candidate (weights, s_max, tag): both run from the same state
+    """Each candidate (weights, s_max, tag) is measured against the plain method: both run from the same state
     to the checkpoints, and a candidate is admissible when the KS distance of every marginal at
     every checkpoint stays within margin * bound.  Returns the index of the admissible candidate
     with the shortest device time (None when none is admissible) and the table."""
