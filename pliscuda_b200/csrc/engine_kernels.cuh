@@ -509,7 +509,9 @@ __device__ __forceinline__ void cell_tau_parts(const KArgs& A, uint32_t c, const
     const Real d = drate<Real>(m, comp, s) * (Real)xs;
     if (mode == 0) {
       if (xs >= nc) { mu = mu + d; s2 = s2 + d; }
-      for (int j = 0; j < n; ++j) {
+#pragma unroll
+      for (int j = 0; j < 6; ++j) {  // unrolled: the neighbours' loads issue together
+        if (j >= n) break;
         const uint32_t b = q.nb[j];
         const Real db = drate<Real>(m, comp_of(m, b), s) * (Real)Xe[(size_t)s * m.Npad + b];
         const Real qd = db / (Real)q.nn[j];
@@ -522,7 +524,9 @@ __device__ __forceinline__ void cell_tau_parts(const KArgs& A, uint32_t c, const
         mu = mu - dout;
         s2 = s2 + dout;
       }
-      for (int j = 0; j < n; ++j) {
+#pragma unroll
+      for (int j = 0; j < 6; ++j) {
+        if (j >= n) break;
         const uint32_t b = q.nb[j];
         const int32_t xb = Xe[(size_t)s * m.Npad + b];
         if (xb >= nc) {
