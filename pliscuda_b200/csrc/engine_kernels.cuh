@@ -301,12 +301,32 @@ struct Nbr {
   uint8_t nn[6];
   uint8_t dir[6];  // lattice direction of each slot: 0..5 = -x,+x,-y,+y,-z,+z
   int n;
+  // lattice: the subvolume, its coordinates and neighbours per axis (for_each_nbr walks the
+  // directions from these; nbr_lite fills nothing else)
+  int lat;
+  uint32_t c, x, y, z;
+  int ax, ay, az;
 };
 
 __device__ __forceinline__ int axis_count(uint32_t v, uint32_t dim) { return (v > 0) + (v + 1 < dim); }
 
+__device__ __forceinline__ void nbr_scalars(const DevModel& m, const Cell& cl, Nbr& q) {
+  q.lat = (int)m.lattice;
+  q.c = cl.c;
+  q.x = cl.x;
+  q.y = cl.y;
+  q.z = cl.z;
+  if (m.lattice) {
+    q.ax = axis_count(cl.x, m.X);
+    q.ay = axis_count(cl.y, m.Y);
+    q.az = axis_count(cl.z, m.Z);
+    q.n = q.ax + q.ay + q.az;
+  }
+}
+
 __device__ __forceinline__ void nbr_info(const DevModel& m, const Cell& cl, Nbr& q) {
   const uint32_t c = cl.c;
+  nbr_scalars(m, cl, q);
   if (m.lattice) {
     const uint32_t X = m.X, Y = m.Y, Z = m.Z, XY = m.X * m.Y;
     const int ax = axis_count(cl.x, X), ay = axis_count(cl.y, Y), az = axis_count(cl.z, Z);
@@ -327,6 +347,46 @@ __device__ __forceinline__ void nbr_info(const DevModel& m, const Cell& cl, Nbr&
     q.nb[j] = m.canon[(size_t)c * 6 + j];
     q.nn[j] = j < q.n ? m.ncount[q.nb[j]] : 0;
     q.dir[j] = 0;
+  }
+}
+
+// The neighbours without the slot arrays on a lattice (they are walked by direction instead);
+// a neighbour table fills them as nbr_info does.
+__device__ __forceinline__ void nbr_lite(const DevModel& m, const Cell& cl, Nbr& q) {
+  if (m.lattice) nbr_scalars(m, cl, q);
+  else nbr_info(m, cl, q);
+}
+
+// Lattice neighbour in direction d (0..5 = -x,+x,-y,+y,-z,+z): false when absent, else its index and
+// its own neighbour count.
+__device__ __forceinline__ bool nbr_dir(const DevModel& m, const Nbr& q, int d, uint32_t& b, int& nn) {
+  switch (d) {
+    case 0: b = q.c - 1; nn = axis_count(q.x - 1, m.X) + q.ay + q.az; return q.x > 0;
+    case 1: b = q.c + 1; nn = axis_count(q.x + 1, m.X) + q.ay + q.az; return q.x + 1 < m.X;
+    case 2: b = q.c - m.X; nn = q.ax + axis_count(q.y - 1, m.Y) + q.az; return q.y > 0;
+    case 3: b = q.c + m.X; nn = q.ax + axis_count(q.y + 1, m.Y) + q.az; return q.y + 1 < m.Y;
+    case 4: b = q.c - m.X * m.Y; nn = q.ax + q.ay + axis_count(q.z - 1, m.Z); return q.z > 0;
+    default: b = q.c + m.X * m.Y; nn = q.ax + q.ay + axis_count(q.z + 1, m.Z); return q.z + 1 < m.Z;
+  }
+}
+
+// f(b, nn) for each neighbour in slot order (on a lattice: the present directions in order), fully
+// unrolled so that the neighbours' loads issue together.
+template <class F>
+__device__ __forceinline__ void for_each_nbr(const DevModel& m, const Nbr& q, F&& f) {
+  if (q.lat) {
+#pragma unroll
+    for (int d = 0; d < 6; ++d) {
+      uint32_t b;
+      int nn;
+      if (nbr_dir(m, q, d, b, nn)) f(b, nn);
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+      if (j >= q.n) break;
+      f(q.nb[j], (int)q.nn[j]);
+    }
   }
 }
 
@@ -509,32 +569,26 @@ __device__ __forceinline__ void cell_tau_parts(const KArgs& A, uint32_t c, const
     const Real d = drate<Real>(m, comp, s) * (Real)xs;
     if (mode == 0) {
       if (xs >= nc) { mu = mu + d; s2 = s2 + d; }
-#pragma unroll
-      for (int j = 0; j < 6; ++j) {  // unrolled: the neighbours' loads issue together
-        if (j >= n) break;
-        const uint32_t b = q.nb[j];
+      for_each_nbr(m, q, [&](uint32_t b, int nn) {
         const Real db = drate<Real>(m, comp_of(m, b), s) * (Real)Xe[(size_t)s * m.Npad + b];
-        const Real qd = db / (Real)q.nn[j];
+        const Real qd = db / (Real)nn;
         mu = mu - qd;
         s2 = s2 + qd;
-      }
+      });
     } else {
       if (xs >= nc && n > 0) {
         const Real dout = (Real)n * d;
         mu = mu - dout;
         s2 = s2 + dout;
       }
-#pragma unroll
-      for (int j = 0; j < 6; ++j) {
-        if (j >= n) break;
-        const uint32_t b = q.nb[j];
+      for_each_nbr(m, q, [&](uint32_t b, int) {
         const int32_t xb = Xe[(size_t)s * m.Npad + b];
         if (xb >= nc) {
           const Real qd = drate<Real>(m, comp_of(m, b), s) * (Real)xb;
           mu = mu + qd;
           s2 = s2 + qd;
         }
-      }
+      });
     }
     Real mm = ((Real)A.o.eps * (Real)xs) / g;
     if (!(mm > (Real)1)) mm = (Real)1;
@@ -1235,7 +1289,7 @@ __device__ __forceinline__ void classify_tile(const KArgs& A, uint32_t tile, con
       C.Xz[(size_t)s * m.Npad + c] = 0;
     }
   Nbr q;
-  nbr_info(m, cl, q);
+  nbr_lite(m, cl, q);
   classify_cell<Real>(A, c, q, x, C.Xe, C.tau_cur[c], C.flag_cur[c], C.step, C.attempt, C.ff, tn, fl);
   C.tau_new[c] = tn;
   C.flag_new[c] = (uint8_t)fl;
@@ -1367,7 +1421,12 @@ __device__ __forceinline__ void classify_control(const KArgs& A, Ctrl* K, uint32
 }
 
 template <typename Real, int MAXS>
-__global__ void __launch_bounds__(256) k_classify(KArgs A) {
+// 64 registers, 4 CTAs per SM: the classification is bound by load latency and needs the warps
+// (with the compiler's own choice of 80-88 registers it runs 12-60 % slower).
+#ifndef PLIS_CLASSIFY_MIN_BLOCKS
+#define PLIS_CLASSIFY_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(256, PLIS_CLASSIFY_MIN_BLOCKS) k_classify(KArgs A) {
   pdl_entry();
   Ctrl* K = A.b.ctrl;
   if (K->done) return;
