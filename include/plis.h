@@ -195,7 +195,8 @@ typedef struct plis_event_record {
   uint64_t step;      /* number of the step (1 = the first step of the handle) */
   uint32_t subvolume; /* where the event happened: the source of a diffusion */
   uint32_t target;    /* destination subvolume of a diffusion; = subvolume for a reaction */
-  uint32_t count;     /* firings, or molecules moved (exact events: 1); saturated at 2^32-1 */
+  uint32_t count;     /* firings, or molecules moved (exact events: 1); saturated at 2^32-1, and a
+                         leap jump at 2^27 (a jump that large always rolls the attempt back) */
   uint16_t channel;   /* reaction index, or species index of a diffusion */
   uint8_t kind;       /* PLIS_EVENT_* */
   uint8_t attempt;    /* rollback attempt of the step, 0 first (saturated at 255) */

@@ -455,7 +455,8 @@ struct Sim : Base {
             k = Ops::count(Ops::poisson_shared(&sd, lam, em));
           }
           if (k >= kBigJump) big = 1;
-          if (logging && k > 0) cell_log[c].push_back(event(st.time, step, attempt, c, nbr[(size_t)c * 6 + j], k, s, 2));
+          if (logging && k > 0)  // a jump of 2^27 or more (always rolled back) is logged as 2^27, as on the device
+            cell_log[c].push_back(event(st.time, step, attempt, c, nbr[(size_t)c * 6 + j], k < kBigJump ? k : kBigJump, s, 2));
           outk[((size_t)c * S + s) * 6 + j] = k;
           own[(size_t)c * S + s] -= k;
           ev += k;

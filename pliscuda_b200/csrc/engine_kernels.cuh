@@ -132,7 +132,7 @@ template <> struct DiffTraits<float> {
 
 template <typename Real>
 __device__ __forceinline__ void diffusion_draws(const KArgs& A, uint32_t c, int s, int n, Real lam, Real em,
-                                                uint64_t step, uint32_t attempt, long long k[6]) {
+                                                uint64_t step, uint32_t attempt, int32_t k[6]) {
   if (!(lam > (Real)0)) {
 #pragma unroll
     for (int j = 0; j < 6; ++j) k[j] = 0;
@@ -144,7 +144,8 @@ __device__ __forceinline__ void diffusion_draws(const KArgs& A, uint32_t c, int 
       k[j] = 0;
       if (j < n) {
         plis_stream st = plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_diff(s, j));
-        k[j] = plis_count_d(plis_poisson_d(&st, (double)lam));
+        const long long kj = plis_count_d(plis_poisson_d(&st, (double)lam));
+        k[j] = (int32_t)(kj < kBigJump ? kj : kBigJump);  // a jump of 2^27 or more rolls the attempt back
       }
     }
     return;
@@ -875,7 +876,8 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
         }
       }
       Nbr q;
-      nbr_info(m, cl, q);
+      if (m.lattice) nbr_scalars(m, cl, q);  // walked by direction below: no slot arrays
+      else nbr_info(m, cl, q);
       const int n = q.n;
       bool mark = false;
       for (int s = 0; s < S; ++s) {
@@ -884,26 +886,47 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
         if (mode == 0 && n > 0) mark = true;
         const Real lam = tl * (drate<Real>(m, comp, s) * (Real)xs);
         const Real em = RT<Real>::emlam(lam);  // one exp for the n draws of this species
-        long long kd[6];
+        int32_t kd[6];
         diffusion_draws<Real>(A, c, s, n, lam, em, step, attempt, kd);
         long long out = 0;
-        for (int j = 0; j < n; ++j) {
-          const long long k = kd[j];
+        auto jump = [&](long long k, uint32_t b, int dir) {
           if (k >= kBigJump) big = 1;
           if (k > 0) {
-            if (box.acc) atomicAdd_block(&box.acc[s * box.size + own + box_offset(box, q.dir[j])], (int)k);
-            else atomicAdd(&Xt[(size_t)s * m.Npad + q.nb[j]], (int)k);
-            if (mode == 1 && flag[q.nb[j]] == F_SSA_FF) flag[q.nb[j]] = F_SSA;
-            if (LOG) ev_put(A.b.ev, L.t, step, attempt, c, q.nb[j], k, s, PLIS_EVENT_LEAP_DIFFUSION);
+            if (box.acc) atomicAdd_block(&box.acc[s * box.size + own + box_offset(box, dir)], (int)k);
+            else atomicAdd(&Xt[(size_t)s * m.Npad + b], (int)k);
+            if (mode == 1 && flag[b] == F_SSA_FF) flag[b] = F_SSA;
+            if (LOG) ev_put(A.b.ev, L.t, step, attempt, c, b, k, s, PLIS_EVENT_LEAP_DIFFUSION);
           }
           out += k;
+        };
+        if (q.lat) {  // slot j is the j-th present direction; kd is read by constant index only
+          int j = 0;
+#pragma unroll
+          for (int d = 0; d < 6; ++d) {
+            uint32_t b;
+            int nb_n;
+            if (!nbr_dir(m, q, d, b, nb_n)) continue;
+            int32_t k = kd[0];
+#pragma unroll
+            for (int i = 1; i < 6; ++i)
+              if (j == i) k = kd[i];
+            ++j;
+            jump(k, b, d);
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 6; ++j) {
+            if (j >= n) break;
+            jump(kd[j], q.nb[j], 0);
+          }
         }
         dl.add(s, -out);
         ev += out;
       }
       if (mark) {  // leap.cu:54-56: every receiver leaves fast-forward
-        for (int j = 0; j < n; ++j)
-          if (flag[q.nb[j]] == F_SSA_FF) flag[q.nb[j]] = F_SSA;
+        for_each_nbr(m, q, [&](uint32_t b, int) {
+          if (flag[b] == F_SSA_FF) flag[b] = F_SSA;
+        });
       }
     }
 #pragma unroll
