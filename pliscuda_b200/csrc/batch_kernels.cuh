@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(256, LEARNED ? PLIS_BATCH_MIN_BLOCKS_LEARNED :
         const Real tl = (Real)K->tau_leap;
         long long ev;
         int big;
-        leap_tile<Real, MAXS, false>(sA, w - s_lp[r], L, tl, box, ev, big);
+        leap_tile<Real, MAXS, false, false>(sA, w - s_lp[r], L, tl, box, ev, big);
         ev = warp_sum(ev);  // events by warp, straight into the replica's counter (integer: order-free)
         if ((threadIdx.x & 31) == 0 && ev) atomicAdd(&K->ev_attempt, (unsigned long long)ev);
         if (big) atomicOr(&K->blocks_done, 0x80000000u);  // rare: an oversized draw forces a rollback
@@ -343,13 +343,13 @@ __global__ void __launch_bounds__(256, LEARNED ? PLIS_BATCH_MIN_BLOCKS_LEARNED :
       const ClassifyCtx C = classify_ctx(sA, K);
       const uint32_t tile = w - s_cp[r];
       if constexpr (LEARNED) {
-        if (learned_classify_tile<Real, MAXS>(sA, K, C, tile, sA.g.nblocks)) classify_control(sA, K, sA.g.nblocks);
+        if (learned_classify_tile<Real, MAXS, false>(sA, K, C, tile, sA.g.nblocks)) classify_control(sA, K, sA.g.nblocks);
       } else {
         double tn;
         long long ti;
         int fl, bad;
         bool valid;
-        classify_tile<Real, MAXS>(sA, tile, C, tn, ti, fl, bad, valid);
+        classify_tile<Real, MAXS, false>(sA, tile, C, tn, ti, fl, bad, valid);
         if (classify_slot(sA, K, tile, sA.g.nblocks, tn, ti, valid && fl == F_LEAP_CR, bad))
           classify_control(sA, K, sA.g.nblocks);
       }

@@ -526,7 +526,10 @@ __device__ __forceinline__ bool classify_ff(int mode, double tau_cur, uint8_t fl
 // The deterministic part of compute_taus (tau.cu:68-195): the Cao leap bound tau_ncr over the
 // species that enter it, and the rate whose exponential time is tau_cr (critical channels; in
 // corrected mode, all channels of a subvolume without a leap bound).
-template <typename Real, int MAXS>
+// WALK: the neighbour loops are unrolled (for_each_nbr); with WALK false they run to the run-time
+// count over nbr_info's slot arrays, which needs fewer registers where the kernel arguments live in
+// global memory (the batched kernel's per-replica views).
+template <typename Real, bool WALK = true, int MAXS>
 __device__ __forceinline__ void cell_tau_parts(const KArgs& A, uint32_t c, const Nbr& q, const Counts<MAXS>& x,
                                                const int32_t* Xe, Real& tau_ncr_out, Real& rate_cr_out) {
   const DevModel& m = A.m;
@@ -570,26 +573,30 @@ __device__ __forceinline__ void cell_tau_parts(const KArgs& A, uint32_t c, const
     const Real d = drate<Real>(m, comp, s) * (Real)xs;
     if (mode == 0) {
       if (xs >= nc) { mu = mu + d; s2 = s2 + d; }
-      for_each_nbr(m, q, [&](uint32_t b, int nn) {
+      auto term = [&](uint32_t b, int nn) {
         const Real db = drate<Real>(m, comp_of(m, b), s) * (Real)Xe[(size_t)s * m.Npad + b];
         const Real qd = db / (Real)nn;
         mu = mu - qd;
         s2 = s2 + qd;
-      });
+      };
+      if constexpr (WALK) for_each_nbr(m, q, term);
+      else for (int j = 0; j < n; ++j) term(q.nb[j], (int)q.nn[j]);
     } else {
       if (xs >= nc && n > 0) {
         const Real dout = (Real)n * d;
         mu = mu - dout;
         s2 = s2 + dout;
       }
-      for_each_nbr(m, q, [&](uint32_t b, int) {
+      auto term = [&](uint32_t b, int) {
         const int32_t xb = Xe[(size_t)s * m.Npad + b];
         if (xb >= nc) {
           const Real qd = drate<Real>(m, comp_of(m, b), s) * (Real)xb;
           mu = mu + qd;
           s2 = s2 + qd;
         }
-      });
+      };
+      if constexpr (WALK) for_each_nbr(m, q, term);
+      else for (int j = 0; j < n; ++j) term(q.nb[j], (int)q.nn[j]);
     }
     Real mm = ((Real)A.o.eps * (Real)xs) / g;
     if (!(mm > (Real)1)) mm = (Real)1;
@@ -647,13 +654,13 @@ __device__ __forceinline__ void cell_decide(double tn, double tcr, double& tau_o
 // ------------------------------------------------------------------------------------------------
 // classification of one subvolume (compute_taus, tau.cu:197-252)
 // ------------------------------------------------------------------------------------------------
-template <typename Real, int MAXS>
+template <typename Real, bool WALK = true, int MAXS>
 __device__ void classify_cell(const KArgs& A, uint32_t c, const Nbr& q, const Counts<MAXS>& x, const int32_t* Xe,
                               double tau_cur, uint8_t flag_cur, uint64_t step, uint32_t attempt,
                               double ff, double& tau_out, int& flag_out) {
   if (classify_ff(A.o.mode, tau_cur, flag_cur, step, ff, tau_out, flag_out)) return;
   Real tau_ncr, rate;
-  cell_tau_parts<Real>(A, c, q, x, Xe, tau_ncr, rate);
+  cell_tau_parts<Real, WALK>(A, c, q, x, Xe, tau_ncr, rate);
   const double tcr = cell_tau_cr<Real>(A, c, step, attempt, rate);
   cell_decide((double)tau_ncr, tcr, tau_out, flag_out);
 }
@@ -792,7 +799,7 @@ struct LeapCtx {
 
 // Leap of one brick (or one 1-D block of a table topology) by the whole CTA; returns this thread's
 // events and guard flag.  leap_step, leap.cu:3-65.
-template <typename Real, int MAXS, bool LOG>
+template <typename Real, int MAXS, bool LOG, bool WALK = true>
 __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const LeapCtx& L, Real tl, const Box& box,
                                           long long& ev, int& big) {
   const DevModel& m = A.m;
@@ -876,7 +883,7 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
         }
       }
       Nbr q;
-      if (m.lattice) nbr_scalars(m, cl, q);  // walked by direction below: no slot arrays
+      if (WALK && m.lattice) nbr_scalars(m, cl, q);  // walked by direction below: no slot arrays
       else nbr_info(m, cl, q);
       const int n = q.n;
       bool mark = false;
@@ -899,7 +906,7 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
           }
           out += k;
         };
-        if (q.lat) {  // slot j is the j-th present direction; kd is read by constant index only
+        if (WALK && q.lat) {  // slot j is the j-th present direction; kd is read by constant index only
           int j = 0;
 #pragma unroll
           for (int d = 0; d < 6; ++d) {
@@ -913,20 +920,24 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
             ++j;
             jump(k, b, d);
           }
-        } else {
+        } else if constexpr (WALK) {
 #pragma unroll
           for (int j = 0; j < 6; ++j) {
             if (j >= n) break;
             jump(kd[j], q.nb[j], 0);
           }
+        } else {
+          for (int j = 0; j < n; ++j) jump(kd[j], q.nb[j], q.dir[j]);
         }
         dl.add(s, -out);
         ev += out;
       }
       if (mark) {  // leap.cu:54-56: every receiver leaves fast-forward
-        for_each_nbr(m, q, [&](uint32_t b, int) {
+        auto leave_ff = [&](uint32_t b, int) {
           if (flag[b] == F_SSA_FF) flag[b] = F_SSA;
-        });
+        };
+        if constexpr (WALK) for_each_nbr(m, q, leave_ff);
+        else for (int j = 0; j < n; ++j) leave_ff(q.nb[j], 0);
       }
     }
 #pragma unroll
@@ -1291,7 +1302,7 @@ __device__ __forceinline__ ClassifyCtx classify_ctx(const KArgs& A, const Ctrl* 
 }
 
 // One thread's subvolume of one brick: negativity check, zeroing of the next target, classification.
-template <typename Real, int MAXS>
+template <typename Real, int MAXS, bool WALK = true>
 __device__ __forceinline__ void classify_tile(const KArgs& A, uint32_t tile, const ClassifyCtx& C, double& tn,
                                               long long& ti, int& fl, int& bad, bool& valid) {
   const DevModel& m = A.m;
@@ -1312,8 +1323,9 @@ __device__ __forceinline__ void classify_tile(const KArgs& A, uint32_t tile, con
       C.Xz[(size_t)s * m.Npad + c] = 0;
     }
   Nbr q;
-  nbr_lite(m, cl, q);
-  classify_cell<Real>(A, c, q, x, C.Xe, C.tau_cur[c], C.flag_cur[c], C.step, C.attempt, C.ff, tn, fl);
+  if constexpr (WALK) nbr_lite(m, cl, q);
+  else nbr_info(m, cl, q);
+  classify_cell<Real, WALK>(A, c, q, x, C.Xe, C.tau_cur[c], C.flag_cur[c], C.step, C.attempt, C.ff, tn, fl);
   C.tau_new[c] = tn;
   C.flag_new[c] = (uint8_t)fl;
   ti = c;

@@ -173,7 +173,7 @@ __device__ __forceinline__ bool classify_slot_learned(const KArgs& A, Ctrl* K, u
 // warp's MLP by mma.sync, decisions against the proposal and the plain bound), then its CTA slot
 // with the plain min-tau beside the proposed one; true in the CTA that reduces the last slot.  Every
 // thread of the CTA must call it (the MLP is warp-collective).
-template <typename Real, int MAXS>
+template <typename Real, int MAXS, bool WALK = true>
 __device__ __forceinline__ bool learned_classify_tile(const KArgs& A, Ctrl* K, const ClassifyCtx& C, uint32_t tile,
                                                       uint32_t nslots) {
   const LearnedParams* P = A.b.lp;
@@ -202,7 +202,7 @@ __device__ __forceinline__ bool learned_classify_tile(const KArgs& A, Ctrl* K, c
     nbr_info(m, cl, q);
     ff = classify_ff(A.o.mode, C.tau_cur[c], C.flag_cur[c], C.step, C.ff, tn, fl);
     if (!ff) {
-      cell_tau_parts<Real>(A, c, q, x, C.Xe, tau_ncr, rate);
+      cell_tau_parts<Real, WALK>(A, c, q, x, C.Xe, tau_ncr, rate);
       if (!plis_isinf_d((double)tau_ncr)) {
         cell_features<Real>(A, c, q, x, C.Xe, tau_ncr, f);
         normalise(P, f);
