@@ -12,9 +12,10 @@ trajectory: W warm-up intervals, then K timed ones.
 Metric: events/second (an event is one reaction firing or one molecule jump; a leap firing of k
 counts k), with simulated-time/second alongside.  `value` is device time from CUDA events on the
 library's stream around each interval with the state resident in HBM; L2 is flushed (a 512 MiB
-write) between timed intervals.  `e2e` is the same metric through the C ABI with host buffers:
-every interval uploads the state from pinned host memory (plis_set_state), runs, and reads the
-state back (plis_get_state).
+write) between timed intervals.  `e2e` is the same metric through the C ABI with host buffers over
+the same slice of the same trajectory: every interval uploads the counts from pinned host memory at
+the time and step count where the previous one left off (plis_set_state_at), runs to the same
+checkpoint as the device loop, and reads the counts back (plis_get_state).
 
 `batched` (rank 0, N = 1): the batched form on 256 Brusselator replicas of uneven sizes in one
 persistent launch against the same replicas as single handles (batch_report).
@@ -28,9 +29,9 @@ N > 1 (torchrun): each rank simulates its own independent replica (its rank is t
 the Philox key) on its own GPU; there is no data-path collective.  value = all ranks' events / the
 max over ranks of device time.
 
---impl reference: the reference has no CPU implementation of the step, so its CPU arm is the FP64
-host oracle (oracle/plis_oracle.cpp, OpenMP over subvolumes) on all host threads, on a bounded
-slice of the same workload.
+--impl reference: the reference has no CPU implementation of the step (it is CUDA only), so its CPU
+arm is the FP64 host oracle (oracle/plis_oracle.cpp, OpenMP over subvolumes) on all host threads,
+replaying the GPU arm's own trajectory: the same W warm-up and K timed intervals, the same events.
 """
 from __future__ import annotations
 
@@ -154,49 +155,74 @@ class Clocks:
                 "samples": len(sms)}
 
 
+SEED = 1000  # stream seed of the timed trajectory; rank r runs replica r (replicas.replica_options)
+
+
+def bench_config(args, world):
+    """The `config` object of both arms' lines (the same workload, slice and stream)."""
+    return {"workload": f"{args.workload}: {WORKLOADS[args.workload]}, {args.mode} semantics",
+            "step": f"one checkpoint interval of {INTERVAL} simulated time units of one trajectory (seed {SEED}, "
+                    f"replica = rank): W warm-up intervals from t = 0, then the K timed ones",
+            "l2": "flushed between timed steps (512 MiB write)", "parallelism": f"replicas x{world}",
+            "precision": args.precision}
+
+
 def run_reference(args):
-    """CPU arm: the FP64 host oracle on all host threads, bounded slice of the workload."""
+    """Reference arm.  The reference has no CPU implementation of the step (it is CUDA only), so its
+    CPU arm is the FP64 host oracle (oracle/plis_oracle.cpp, OpenMP over subvolumes) on all host
+    threads.  It replays exactly the trajectory of rank 0 of the GPU arm (same seed and replica:
+    the oracle is bit-exact with the CUDA step), W untimed intervals from t = 0, then K timed ones:
+    the same slice, the same events.  Inputs come from oracle/synth.py: this process loads no part
+    of the CUDA library."""
+    from oracle import synth
     from oracle.oracle import Oracle
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if int(os.environ.get("RANK", "0")) != 0:
         return 0
-    model, state = _workload(args.workload)
+    model, state = synth.WORKLOADS[args.workload]()
     threads = os.cpu_count() or 1
-    orc = Oracle.from_model(model, mode=0, precision=0, seed=1, threads=threads)
+    mode = {"reference": 0, "corrected": 1}[args.mode]
+    prec = {"fp64": 0, "fp32": 1}[args.precision]
+    orc = Oracle.from_model(model, mode=mode, precision=prec, seed=SEED, replica=0, threads=threads)
     orc.set_state(state)
-    # bounded sample: a slice of simulated time per step, sized so the whole run stays within minutes
-    slice_t = args.ref_slice
-    for _ in range(max(0, args.warmup if args.warmup < 1 else 1)):
-        orc.run(orc.stats().time + slice_t / 4)
+    t = 0.0
+    for _ in range(args.warmup):
+        t += INTERVAL
+        orc.run(t)
+    a = orc.stats()
     t0 = time.perf_counter()
-    ev0, st0, tt0 = orc.stats().events, orc.stats().steps, orc.stats().time
     for _ in range(args.steps):
-        orc.run(orc.stats().time + slice_t)
+        t += INTERVAL
+        orc.run(t)
     el = time.perf_counter() - t0
-    s = orc.stats()
-    ev = s.events - ev0
+    b = orc.stats()
+    ev = b.events - a.events
     value = ev / el
     out = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{args.workload} Schlogl, {model.n_subvolumes} subvolumes, reference semantics",
-                   "step": f"{slice_t} simulated time units per step (bounded CPU sample)"},
-        "sim_time_per_sec": (s.time - tt0) / el,
-        "leap_steps_per_sec": (s.steps - st0) / el,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32", "data": "synthetic",
+        "config": bench_config(args, world),
+        "sim_time_per_sec": (b.time - a.time) / el,
+        "leap_steps_per_sec": (b.steps - a.steps) / el,
+        "events": int(ev), "leap_steps": int(b.steps - a.steps), "t_start": a.time, "t_end": b.time,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} x {slice_t} sim-time units of the {args.workload} workload, "
-                                   f"FP64 host oracle (OpenMP, {threads} threads)"},
+                         "sample": f"the K timed intervals t = {a.time:.4f} -> {b.time:.4f} of the GPU arm's own "
+                                   f"trajectory (rank 0), FP64 host oracle, OpenMP {threads} threads"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))
     return 0
 
 
-def cpu_baseline_sample(model, state, threads, budget_s=12.0):
-    """Oracle events/s on a bounded slice (about budget_s of CPU work)."""
+def cpu_baseline_sample(workload, threads, mode=0, precision=0, budget_s=12.0):
+    """Oracle events/s on a bounded slice (about budget_s of CPU work) from t = 0 of the same
+    trajectory the GPU arm times (seed and replica of rank 0)."""
+    from oracle import synth
     from oracle.oracle import Oracle
-    orc = Oracle.from_model(model, mode=0, precision=0, seed=1, threads=threads)
+    model, state = synth.WORKLOADS[workload]()
+    orc = Oracle.from_model(model, mode=mode, precision=precision, seed=SEED, replica=0, threads=threads)
     orc.set_state(state)
     t0 = time.perf_counter()
     slice_t = 0.002
@@ -208,8 +234,8 @@ def cpu_baseline_sample(model, state, threads, budget_s=12.0):
         slice_t = min(slice_t * 2, 0.05)
     s = orc.stats()
     return {"value": s.events / el, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"first {s.time:.4f} sim-time units ({s.steps} leap steps) of the same workload, FP64 host "
-                      f"oracle, OpenMP {threads} threads, {el:.1f} s"}
+            "sample": f"first {s.time:.4f} sim-time units ({s.steps} leap steps) of the same trajectory, "
+                      f"{'FP64' if precision == 0 else 'FP32'} host oracle, OpenMP {threads} threads, {el:.1f} s"}
 
 
 def ncu_case(args):
@@ -430,7 +456,6 @@ def main(argv=None):
     ap.add_argument("--workload", default="schlogl64")
     ap.add_argument("--mode", default="reference", choices=["reference", "corrected"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
-    ap.add_argument("--ref-slice", type=float, default=0.01)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--ncu-case", action="store_true", help="run only the fixed ncu capture case")
@@ -471,7 +496,7 @@ def main(argv=None):
     dev = replicas.rank_device(dist, local)
 
     model, state = _workload(args.workload)
-    ropt = replicas.replica_options(rank)
+    ropt = replicas.replica_options(rank, seed=SEED)
     sim = Simulation(model, mode=args.mode, precision=args.precision, device=local, **ropt)
     sim.set_state(state)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")
@@ -481,6 +506,8 @@ def main(argv=None):
         t += INTERVAL
         sim.run(t)
     torch.cuda.synchronize()
+    t_w = t
+    start_state, start_stats = sim.get_state(), sim.stats()  # the e2e leg replays the timed slice
 
     clocks = Clocks(local)
     ev_tot, ms_tot, simt_tot, launches = 0, 0.0, 0.0, 0
@@ -509,11 +536,10 @@ def main(argv=None):
     value = ev_all / (ms_all / 1e3)
     sim_time_per_sec = simt_tot / (ms_tot / 1e3)
 
-    # per-kernel roofline from an event-instrumented replay of a slice of the same trajectory
-    cur = sim.get_state()
+    # per-kernel roofline from an event-instrumented replay of a quarter interval of the same slice
     with Simulation(model, mode=args.mode, precision=args.precision, device=local, profile=True, **ropt) as ps:
-        ps.set_state(cur)
-        ps.run(INTERVAL / 4)
+        ps.set_state(start_state, time=start_stats.time, steps=start_stats.steps)
+        ps.run(t_w + INTERVAL / 4)
         per = ps.kernel_profile()
     dom = max(per, key=lambda k: per[k][0])
     N, S = model.n_subvolumes, model.n_species
@@ -525,30 +551,40 @@ def main(argv=None):
     traffic = NCU_TRAFFIC.get((args.workload, args.mode, args.precision, dom), (None, None))
     instr = NCU_WARP_INSTR.get((args.workload, args.mode, args.precision, dom), (None, None))
 
-    # end to end through the C ABI with host buffers
+    # end to end through the C ABI with host buffers, over the same slice: every interval uploads the
+    # counts from pinned host memory at the time and step count it left off (plis_set_state_at),
+    # runs to the same checkpoint as the device loop, and reads the counts back
     e2e = None
     if not args.no_e2e:
-        host = torch.from_numpy(cur).pin_memory()
+        host = torch.from_numpy(start_state).pin_memory()
         hnp = host.numpy()
         out = torch.empty_like(host).pin_memory()
         onp = out.numpy()
-        e_ev, e_s = 0, 0.0
+        e_ev, e_s, e_simt = 0, 0.0, 0.0
+        te, ne = start_stats.time, start_stats.steps
+        target = t_w
         for i in range(args.steps):
+            flush.fill_(1)  # L2 flush between timed intervals, outside the timed region
             torch.cuda.synchronize()
+            target += INTERVAL
             w0 = time.perf_counter()
-            sim.set_state(hnp)
-            st = sim.run(INTERVAL)
+            sim.set_state(hnp, time=te, steps=ne)
+            st = sim.run(target)
             sim.get_state(onp)
             e_s += time.perf_counter() - w0
             e_ev += st.events
+            e_simt += st.time - te
+            te, ne = st.time, st.steps
             hnp[:] = onp
         ej = replicas.combine(dist, dev, max_keys={"s": e_s}, sum_keys={"events": float(e_ev)})
         e2e = {"value": ej["events"] / ej["s"], "unit": UNIT, "h2d_bytes_per_step": int(hnp.nbytes) * world,
-               "d2h_bytes_per_step": int(onp.nbytes) * world, "sim_time_per_sec": args.steps * INTERVAL / e_s}
+               "d2h_bytes_per_step": int(onp.nbytes) * world, "sim_time_per_sec": e_simt / e_s,
+               "slice": f"t = {start_stats.time:.4f} -> {te:.4f}, the device loop's slice"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample(model, state, os.cpu_count() or 1)
+        cpu = cpu_baseline_sample(args.workload, os.cpu_count() or 1, mode={"reference": 0, "corrected": 1}[args.mode],
+                                  precision={"fp64": 0, "fp32": 1}[args.precision])
     learned = None
     if rank == 0 and world == 1 and not args.no_learned:
         learned = learned_report()
@@ -562,10 +598,7 @@ def main(argv=None):
             "warmup": args.warmup, "ms_per_step": ms_all / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32",
             "data": "synthetic",
-            "config": {"workload": f"{args.workload}: {WORKLOADS[args.workload]}, {args.mode} semantics",
-                       "step": f"one checkpoint interval of {INTERVAL} simulated time units",
-                       "l2": "flushed between timed steps (512 MiB write)", "parallelism": f"replicas x{world}",
-                       "precision": args.precision},
+            "config": bench_config(args, world),
             "sim_time_per_sec": sim_time_per_sec,
             "leap_steps_per_sec": steps_tot / (ms_tot / 1e3),
             "gpu_launches": launches,

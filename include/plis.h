@@ -154,6 +154,12 @@ int plis_destroy(plis_handle* h);
  * the initial rates, taus and flags (driver.cu:221-234).  plis_get_state copies them back
  * (driver.cu:366, :391). */
 int plis_set_state(plis_handle* h, const uint32_t* counts);
+/* plis_set_state for a trajectory that continues from a host copy of its counts: the counts are at
+ * simulated time `time` after `steps` accepted steps.  The accepted-step counter keys the random
+ * stream, so the continued steps draw the numbers the same trajectory would have drawn on the device
+ * (the reference has no counterpart: its loop never leaves the device, driver.cu:259-376).  The
+ * statistics restart at zero; plis_get_stats reports steps from `steps` on. */
+int plis_set_state_at(plis_handle* h, const uint32_t* counts, double time, uint64_t steps);
 int plis_get_state(plis_handle* h, uint32_t* counts);
 int plis_set_time(plis_handle* h, double time);
 

@@ -67,6 +67,11 @@ def lib():
         for n in ("oracle_set_state", "oracle_get_state"):
             getattr(L, n).argtypes = [ctypes.c_void_p, ctypes.c_void_p]
             getattr(L, n).restype = ctypes.c_int
+        L.oracle_set_state_at.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_uint64]
+        L.oracle_set_state_at.restype = ctypes.c_int
+        L.oracle_canonical_neighbours.argtypes = [ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                  ctypes.c_void_p]
+        L.oracle_canonical_neighbours.restype = ctypes.c_int
         L.oracle_get_taus.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.oracle_get_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(Stats)]
         L.oracle_advance.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_uint64]
@@ -88,9 +93,24 @@ def _p(a):
     return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
 
 
+def canonical_neighbours(n, table=None, lattice=None):
+    """(canonical uint32[6n], lattice dims or zeros) built by the oracle's own code
+    (oracle_canonical_neighbours): non-self entries first, own index after them; a reflective lattice
+    in the direction order -x,+x,-y,+y,-z,+z."""
+    out = np.empty(6 * n, np.uint32)
+    dims = np.zeros(3, np.uint32)
+    tab = None if table is None else np.ascontiguousarray(table, np.uint32)
+    lat = None if lattice is None else np.ascontiguousarray(lattice, np.uint32)
+    if tab is None and lat is None:
+        raise ValueError("a topology needs a table or lattice dimensions")
+    if lib().oracle_canonical_neighbours(int(n), _p(tab), _p(lat), _p(out), _p(dims)):
+        raise ValueError("invalid topology (entry >= n, or dimensions that do not multiply to n)")
+    return out, tuple(int(v) for v in dims)
+
+
 class Oracle:
     """FP64 (precision=0) or FP32 (precision=1) host restatement of the step, same injected stream
-    as the CUDA step.  `nbr` is the canonical table (pliscuda_b200.canonical_neighbours)."""
+    as the CUDA step.  `nbr` is the canonical table (canonical_neighbours above)."""
 
     def __init__(self, n, s, r, nbr, reactants, products, reaction_rates, diffusion_rates, *,
                  n_compartments=1, compartment=None, orig=None, mode=0, precision=0, seed=1, replica=0,
@@ -110,8 +130,10 @@ class Oracle:
 
     @classmethod
     def from_model(cls, model, **kw):
-        """Build from a pliscuda_b200.Model (canonical table computed by the library's host helper)."""
-        from pliscuda_b200 import canonical_neighbours
+        """Build from any object with a model's fields (n_subvolumes, n_species, n_reactions,
+        reactants, products, reaction_rates, diffusion_rates, neighbours or lattice, n_compartments,
+        compartment): a pliscuda_b200.Model or an oracle.synth workload.  The canonical table is the
+        oracle's own (canonical_neighbours)."""
         canon, _ = canonical_neighbours(model.n_subvolumes, model.neighbours, model.lattice)
         return cls(model.n_subvolumes, model.n_species, model.n_reactions, canon, model.reactants,
                    model.products, model.reaction_rates, model.diffusion_rates,
@@ -129,9 +151,14 @@ class Oracle:
         except Exception:
             pass
 
-    def set_state(self, counts):
+    def set_state(self, counts, time=None, steps=0):
+        """Counts at time 0, or (with `time`) counts that continue a trajectory at that time after
+        `steps` accepted steps (oracle_set_state_at)."""
         c = np.ascontiguousarray(counts, np.uint32)
-        rc = lib().oracle_set_state(self._h, _p(c))
+        if time is None:
+            rc = lib().oracle_set_state(self._h, _p(c))
+        else:
+            rc = lib().oracle_set_state_at(self._h, _p(c), float(time), int(steps))
         if rc:
             raise ValueError(f"oracle_set_state failed ({rc})")
 

@@ -99,7 +99,7 @@ struct Base {
   std::vector<std::vector<std::pair<uint32_t, int>>> in_edges;  // per cell: (source cell, source slot)
   oracle_options opt;
   virtual ~Base() {}
-  virtual int set_state(const uint32_t*) = 0;
+  virtual int set_state(const uint32_t*, double t0, uint64_t step0) = 0;
   virtual int get_state(uint32_t*) = 0;
   virtual int get_taus(double*, uint8_t*) = 0;
   virtual int advance(double, uint64_t) = 0;
@@ -377,7 +377,7 @@ struct Sim : Base {
     for (int64_t ci = 0; ci < (int64_t)N; ++ci) classify((uint32_t)ci, step, attempt);
   }
 
-  int set_state(const uint32_t* counts) override {
+  int set_state(const uint32_t* counts, double t0, uint64_t step0) override {
     for (size_t i = 0; i < (size_t)S * N; ++i) {
       if (counts[i] >= (1u << 30)) return 8;
       x[i] = counts[i];
@@ -385,8 +385,10 @@ struct Sim : Base {
     std::fill(flag.begin(), flag.end(), (uint8_t)SSA_FF);  // driver.cu:213
     std::fill(tau.begin(), tau.end(), PLIS_INF_D);
     st = oracle_stats{};
+    st.time = t0;
+    st.steps = step0;
     ff_tau = 0.0;
-    classify_all(0, 0);
+    classify_all(step0, 0);
     return 0;
   }
   int get_state(uint32_t* counts) override {
@@ -789,7 +791,10 @@ void* oracle_create(const oracle_model* m, const oracle_options* o) {
   return make_sim<double>(m, o);
 }
 void oracle_destroy(void* h) { delete static_cast<Base*>(h); }
-int oracle_set_state(void* h, const uint32_t* c) { return static_cast<Base*>(h)->set_state(c); }
+int oracle_set_state(void* h, const uint32_t* c) { return static_cast<Base*>(h)->set_state(c, 0.0, 0); }
+int oracle_set_state_at(void* h, const uint32_t* c, double t0, uint64_t step0) {
+  return static_cast<Base*>(h)->set_state(c, t0, step0);
+}
 int oracle_get_state(void* h, uint32_t* c) { return static_cast<Base*>(h)->get_state(c); }
 int oracle_get_taus(void* h, double* t, uint8_t* f) { return static_cast<Base*>(h)->get_taus(t, f); }
 int oracle_get_stats(void* h, oracle_stats* st) {
@@ -819,6 +824,104 @@ int64_t oracle_read_event_log(void* h, oracle_event* out, int64_t max) {
 // Test hooks over the shared stream numerics (pliscuda_b200/csrc/plis_stream.h).
 // ---------------------------------------------------------------------------------------------
 extern "C" {
+
+// Canonical neighbour table of the oracle, built here rather than taken from the product so that a
+// fault in the product's slot order cannot hide from the parity tests.  The reference pads each
+// 6-wide row with the subvolume's own index (PLISCuda/include/cpp/Topology.hpp:176-184); its leap
+// and SSA draw a destination slot among the six (leap.cu:180-186, ssa.cu:89-106).  The canonical
+// row keeps the non-self entries in file order and pads with the own index after them.  A table that
+// is a reflective x-fastest lattice is rewritten in the fixed direction order -x,+x,-y,+y,-z,+z,
+// which is also the order of an implicit lattice (no table).  Lattice dimensions are read off row 0:
+// its sorted non-self entries are {} (one subvolume), {1} (a chain), {1, X} or {1, X, X*Y}; the
+// candidate is accepted when every row holds exactly that lattice's neighbours.  Unit dimensions are
+// moved to the back, since (1, Y, Z) linearises like (Y, Z, 1).
+static int lattice_nbrs(const uint32_t d[3], uint32_t c, uint32_t out[6]) {
+  const uint64_t X = d[0], XY = (uint64_t)d[0] * d[1];
+  const uint32_t x = (uint32_t)(c % X), y = (uint32_t)((c / X) % d[1]), z = (uint32_t)(c / XY);
+  int k = 0;
+  if (x >= 1) out[k++] = c - 1;
+  if (x + 1 < d[0]) out[k++] = c + 1;
+  if (y >= 1) out[k++] = (uint32_t)(c - X);
+  if (y + 1 < d[1]) out[k++] = (uint32_t)(c + X);
+  if (z >= 1) out[k++] = (uint32_t)(c - XY);
+  if (z + 1 < d[2]) out[k++] = (uint32_t)(c + XY);
+  return k;
+}
+
+static void units_last(uint32_t d[3]) {
+  uint32_t v[3] = {1, 1, 1};
+  int k = 0;
+  for (int i = 0; i < 3; ++i)
+    if (d[i] != 1) v[k++] = d[i];
+  d[0] = v[0]; d[1] = v[1]; d[2] = v[2];
+}
+
+int oracle_canonical_neighbours(uint32_t n, const uint32_t* table, const uint32_t* lattice, uint32_t* out,
+                                uint32_t* dims_out) {
+  if (n == 0 || !out) return 1;
+  uint32_t d[3] = {0, 0, 0};
+  bool is_lattice = false;
+  if (!table) {
+    if (!lattice || (uint64_t)lattice[0] * lattice[1] * lattice[2] != n) return 1;
+    d[0] = lattice[0]; d[1] = lattice[1]; d[2] = lattice[2];
+    units_last(d);
+    is_lattice = true;
+  } else {
+    std::vector<uint32_t> row0;
+    for (int j = 0; j < 6; ++j) {
+      const uint32_t b = table[j];
+      if (b >= n) return 1;
+      if (b != 0) row0.push_back(b);
+    }
+    std::sort(row0.begin(), row0.end());
+    uint32_t cand[3] = {0, 0, 0};
+    bool have = false;
+    if (row0.empty()) { cand[0] = 1; cand[1] = 1; cand[2] = 1; have = (n == 1); }
+    else if (row0[0] == 1 && row0.size() == 1) { cand[0] = n; cand[1] = 1; cand[2] = 1; have = true; }
+    else if (row0[0] == 1 && row0.size() == 2 && n % row0[1] == 0) {
+      cand[0] = row0[1]; cand[1] = n / row0[1]; cand[2] = 1; have = true;
+    } else if (row0[0] == 1 && row0.size() == 3 && row0[2] % row0[1] == 0 && n % row0[2] == 0) {
+      cand[0] = row0[1]; cand[1] = row0[2] / row0[1]; cand[2] = n / row0[2]; have = true;
+    }
+    if (have) {
+      is_lattice = true;
+      for (uint32_t c = 0; c < n && is_lattice; ++c) {
+        std::vector<uint32_t> got;
+        for (int j = 0; j < 6; ++j) {
+          const uint32_t b = table[(size_t)c * 6 + j];
+          if (b >= n) return 1;
+          if (b != c) got.push_back(b);
+        }
+        uint32_t want[6];
+        const int k = lattice_nbrs(cand, c, want);
+        std::sort(got.begin(), got.end());
+        std::sort(want, want + k);
+        is_lattice = (int)got.size() == k && std::equal(want, want + k, got.begin());
+      }
+      if (is_lattice) { d[0] = cand[0]; d[1] = cand[1]; d[2] = cand[2]; units_last(d); }
+    }
+  }
+  if (is_lattice) {
+    for (uint32_t c = 0; c < n; ++c) {
+      uint32_t row[6];
+      const int k = lattice_nbrs(d, c, row);
+      for (int j = 0; j < 6; ++j) out[(size_t)c * 6 + j] = j < k ? row[j] : c;
+    }
+  } else {
+    for (uint32_t c = 0; c < n; ++c) {
+      int k = 0;
+      for (int j = 0; j < 6; ++j) {
+        const uint32_t b = table[(size_t)c * 6 + j];
+        if (b >= n) return 1;
+        if (b != c) out[(size_t)c * 6 + k++] = b;
+      }
+      for (; k < 6; ++k) out[(size_t)c * 6 + k] = c;
+    }
+    d[0] = d[1] = d[2] = 0;
+  }
+  if (dims_out) { dims_out[0] = d[0]; dims_out[1] = d[1]; dims_out[2] = d[2]; }
+  return 0;
+}
 
 void oracle_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
   plis_u32x4 c = {ctr[0], ctr[1], ctr[2], ctr[3]};

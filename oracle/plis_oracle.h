@@ -60,6 +60,9 @@ typedef struct oracle_stats {
 void* oracle_create(const oracle_model* m, const oracle_options* o);
 void oracle_destroy(void* h);
 int oracle_set_state(void* h, const uint32_t* counts);   // [S*N] species-major; also recomputes taus (init)
+// the same for counts that continue a trajectory at time t0 after step0 accepted steps (the step
+// number keys the random stream); statistics restart from zero with steps = step0
+int oracle_set_state_at(void* h, const uint32_t* counts, double t0, uint64_t step0);
 int oracle_get_state(void* h, uint32_t* counts);
 int oracle_get_taus(void* h, double* tau, uint8_t* flags);
 int oracle_get_stats(void* h, oracle_stats* st);
@@ -82,6 +85,12 @@ void oracle_set_event_log(void* h, int on);  // on != 0: record from now on; the
 // returns the number of records logged; with out != NULL it also copies min(logged, max) of them
 // into out and empties the log
 int64_t oracle_read_event_log(void* h, oracle_event* out, int64_t max);
+// Canonical 6-wide neighbour rows (non-self entries first, own index after them; a reflective lattice
+// in the direction order -x,+x,-y,+y,-z,+z) from a topology table [6n] or, with table NULL, from
+// lattice dimensions.  dims_out: the lattice's dimensions (unit dimensions last), zeros otherwise.
+// Returns 0, or 1 for an entry >= n or dimensions that do not multiply to n.
+int oracle_canonical_neighbours(uint32_t n, const uint32_t* table, const uint32_t* lattice, uint32_t* out,
+                                uint32_t* dims_out);
 
 #ifdef __cplusplus
 }

@@ -165,11 +165,17 @@ class Simulation:
             pass
 
     # -- state
-    def set_state(self, counts: np.ndarray) -> None:
+    def set_state(self, counts: np.ndarray, time: Optional[float] = None, steps: int = 0) -> None:
+        """Counts uint32[S*N] species-major.  With `time`, the counts continue a trajectory at that
+        simulated time after `steps` accepted steps (plis_set_state_at): the step counter keys the
+        random stream, so continued steps do not repeat the draws of earlier ones."""
         c = np.ascontiguousarray(counts, dtype=np.uint32).reshape(-1)
         if c.size != self.n * self.s:
             raise InvalidArgument(1, f"state has {c.size} counts, expected S*N = {self.n * self.s}")
-        _check(_lib.lib.plis_set_state(self._h, _c(c)))
+        if time is None:
+            _check(_lib.lib.plis_set_state(self._h, _c(c)))
+        else:
+            _check(_lib.lib.plis_set_state_at(self._h, _c(c), float(time), int(steps)))
 
     def get_state(self, out: Optional[np.ndarray] = None) -> np.ndarray:
         if out is None:

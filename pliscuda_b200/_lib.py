@@ -112,6 +112,7 @@ def _load() -> ctypes.CDLL:
         "plis_set_state": (i32, [vp, vp]),
         "plis_get_state": (i32, [vp, vp]),
         "plis_set_time": (i32, [vp, f64]),
+        "plis_set_state_at": (i32, [vp, vp, f64, u64]),
         "plis_run": (i32, [vp, f64]),
         "plis_step": (i32, [vp, u64]),
         "plis_get_stats": (i32, [vp, P(Stats)]),

@@ -138,6 +138,14 @@ int plis_set_state(plis_handle* h, const uint32_t* counts) {
   PLIS_GUARD_END
 }
 
+int plis_set_state_at(plis_handle* h, const uint32_t* counts, double time, uint64_t steps) {
+  PLIS_GUARD_BEGIN
+  if (!h || !counts) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  if (!(time >= 0.0) || time == __builtin_inf()) { g_err = "time must be finite and >= 0"; return PLIS_ERR_INVALID; }
+  return fail(h, h->eng.set_state(counts, time, steps));
+  PLIS_GUARD_END
+}
+
 int plis_get_state(plis_handle* h, uint32_t* counts) {
   PLIS_GUARD_BEGIN
   if (!h || !counts) { g_err = "null argument"; return PLIS_ERR_INVALID; }

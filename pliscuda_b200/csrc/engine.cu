@@ -285,7 +285,7 @@ int Engine::read_ctrl() {
   return PLIS_OK;
 }
 
-int Engine::set_state(const uint32_t* counts) {
+int Engine::set_state(const uint32_t* counts, double t0, uint64_t step0) {
   const DevModel& dm = args_.m;
   for (size_t i = 0; i < (size_t)dm.S * dm.N; ++i)
     if (counts[i] >= (1u << 30)) {
@@ -309,6 +309,8 @@ int Engine::set_state(const uint32_t* counts) {
   k.argmin = -1;
   k.last_argmin = -1;
   k.t_end = 0.0;
+  k.t = t0;
+  k.step = step0;
   *h_ctrl_ = k;
   PLIS_CU(cudaMemcpyAsync(args_.b.ctrl, h_ctrl_, sizeof(Ctrl), cudaMemcpyHostToDevice, stream_));
   launch_classify();

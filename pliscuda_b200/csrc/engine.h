@@ -28,7 +28,9 @@ class Engine {
   Engine();
   ~Engine();
   int create(const Model& model, const plis_options& opt);
-  int set_state(const uint32_t* counts);
+  // t0, step0: simulated time and accepted-step counter the state is at (0, 0 for a new run); the
+  // step counter keys the random stream, so a trajectory continued from a host copy draws fresh numbers
+  int set_state(const uint32_t* counts, double t0 = 0.0, uint64_t step0 = 0);
   int get_state(uint32_t* counts);
   int set_time(double t);
   int get_taus(double* tau, uint8_t* flags);

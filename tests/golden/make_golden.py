@@ -43,7 +43,11 @@ def dump(conf_dir: str) -> dict:
     }
 
 
-def main(reference="/root/reference"):
+def main(reference=None):
+    reference = reference or os.environ.get("PLIS_REFERENCE")
+    if not reference:
+        print("usage: make_golden.py <reference tree> (or set PLIS_REFERENCE)")
+        return 1
     if not os.path.exists(REFDUMP):
         print("build oracle/_ref/refdump first (python oracle/ref_build.py)")
         return 1

@@ -7,6 +7,17 @@ import numpy as np
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 REF_FIXTURES = os.path.join(GOLDEN, "ref_fixtures")
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def reference_root():
+    """The reference tree, when it is present: PLIS_REFERENCE, else the tree oracle/ref_build.py
+    last built from (oracle/_ref/reference_root.txt).  None elsewhere (the GPU box has no tree)."""
+    cand = os.environ.get("PLIS_REFERENCE")
+    rec = os.path.join(ROOT, "oracle", "_ref", "reference_root.txt")
+    if not cand and os.path.exists(rec):
+        cand = open(rec).read().strip()
+    return cand if cand and os.path.isdir(os.path.join(cand, "PLISCuda")) else None
 
 
 def ref_fixture(name: str):

@@ -6,11 +6,12 @@ import os
 import numpy as np
 import pytest
 
-from helpers import REF_FIXTURES, ref_fixture, write_reference_files
+from helpers import REF_FIXTURES, ref_fixture, reference_root, write_reference_files
 
 import pliscuda_b200 as plis
 
-REFERENCE = "/root/reference/PLISCuda"
+_ROOT = reference_root()
+REFERENCE = os.path.join(_ROOT, "PLISCuda") if _ROOT else None
 FIXTURES = sorted(f[:-4] for f in os.listdir(REF_FIXTURES) if f.endswith(".npz"))
 
 
@@ -27,7 +28,7 @@ def _same_model(a, state_a, b, state_b):
         np.testing.assert_array_equal(a.compartment, b.compartment)
 
 
-@pytest.mark.skipif(not os.path.isdir(REFERENCE), reason="reference tree not present")
+@pytest.mark.skipif(REFERENCE is None, reason="reference tree not present")
 @pytest.mark.parametrize("name", FIXTURES)
 def test_loader_matches_reference_parsers(name):
     """plis_config_load on the reference's own input files gives exactly what the reference's
@@ -166,7 +167,7 @@ def test_snapshot_format(tmp_path):
     assert open(p).read() == "subvolumes=3\nspecies=2\ntime=10.002600\n\n1 40 \n2 50 \n3 60 \n"
 
 
-@pytest.mark.skipif(not os.path.isdir(REFERENCE), reason="reference tree not present")
+@pytest.mark.skipif(REFERENCE is None, reason="reference tree not present")
 @pytest.mark.parametrize("fixture", ["react-9", "diff-41"])
 def test_snapshot_bytes_match_reference_golden(fixture, tmp_path):
     """Writing the golden end state back gives the golden endstate.dat byte for byte."""

@@ -92,3 +92,25 @@ def test_staged_halo_leap_matches(name, mode):
     sim.run(t_end)
     orc.run(t_end)
     assert_same(sim, orc, "final run")
+
+
+@pytest.mark.parametrize("mode", [0, 1], ids=["ref", "corr"])
+def test_state_at_continues_a_trajectory(mode):
+    """plis_set_state_at: counts copied to the host at (t, steps) and set on a new handle continue
+    the trajectory with the same stream counters as the oracle continued from the same point."""
+    from oracle.oracle import Oracle
+    from pliscuda_b200 import Simulation, workloads
+    model, state = workloads.schlogl(12)
+    with Simulation(model, mode=mode, seed=5) as a:
+        a.set_state(state)
+        st = a.run(0.3)
+        mid, t1, n1 = a.get_state(), st.time, st.steps
+    with Simulation(model, mode=mode, seed=5) as b:
+        b.set_state(mid, time=t1, steps=n1)
+        orc = Oracle.from_model(model, mode=mode, seed=5)
+        orc.set_state(mid, time=t1, steps=n1)
+        assert_same(b, orc, "continued state")
+        b.run(0.6)
+        orc.run(0.6)
+        assert_same(b, orc, "continued run")
+        assert b.stats().steps > n1 + 10
