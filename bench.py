@@ -37,6 +37,8 @@ from __future__ import annotations
 
 import argparse
 import json
+
+import numpy as np
 import os
 import tempfile
 import statistics
@@ -287,7 +289,7 @@ def ncu_batch_case(args):
     return 0
 
 
-def precision_report(args):
+def precision_report(side=128, report_steps=200):
     """FP32 form vs binary64 on the precision configuration: the seeded random 10-species,
     20-reaction network (orders 0-2) on a 128^3 lattice.  The binary64 GPU step is bit-identical to
     the FP64 host oracle, so its runs are the oracle's distribution.  The network is stiff (Cao tau
@@ -299,13 +301,12 @@ def precision_report(args):
     import numpy as np
     from scipy import stats as st_
     from pliscuda_b200 import Simulation, workloads
-    side = args.report_side
     model, state = workloads.random_network(side)
     S, N = model.n_species, model.n_subvolumes
     x0 = state.reshape(S, N).astype(np.int64)
     with Simulation(model, mode="corrected", precision="fp64", seed=76) as sim:
         sim.set_state(state)
-        t_end = sim.step(args.report_steps).time
+        t_end = sim.step(report_steps).time
     res = {}
     for prec in ("fp64", "fp32"):
         with Simulation(model, mode="corrected", precision=prec, seed=77 if prec == "fp64" else 78) as sim:
@@ -329,9 +330,10 @@ def precision_report(args):
            "events_per_s_fp64": res["fp64"]["events"] / (res["fp64"]["ms"] * 1e-3),
            "events_per_s_fp32": res["fp32"]["events"] / (res["fp32"]["ms"] * 1e-3),
            "ms_per_step_fp64": res["fp64"]["ms"] / res["fp64"]["steps"],
-           "ms_per_step_fp32": res["fp32"]["ms"] / res["fp32"]["steps"], "per_species": per}
-    print(json.dumps(out))
-    return 0
+           "ms_per_step_fp32": res["fp32"]["ms"] / res["fp32"]["steps"], "per_species": per,
+           "max_rel_error": max(p["rel_error"] for p in per), "max_abs_z": max(abs(p["z"]) for p in per),
+           "max_ks": max(p["ks_delta"] for p in per)}
+    return out
 
 
 def learned_report():
@@ -347,7 +349,8 @@ def learned_report():
     rollbacks among all attempts.  The batched form (the persistent kernel) runs the same comparison
     with the chosen proposer: plain batch against learned batch, KS against the plain run."""
     from pliscuda_b200 import workloads
-    from pliscuda_b200.learned import _ks_per_checkpoint, _run_to_checkpoints, calibrate, train_proposer
+    from pliscuda_b200.learned import (_ks_per_checkpoint, _moment_z_per_checkpoint, _run_to_checkpoints, calibrate,
+                                       train_proposer)
     m64, s64 = workloads.schlogl(64)
     cands, training = [], []
     for eps_l in (0.4, 0.8, 1.6):
@@ -369,8 +372,10 @@ def learned_report():
     w, s_max, tag = cands[best]
     ls, lt = _run_to_checkpoints(m128, s128, cps, seed=12, precision="fp64", device=0, weights=w, s_max=s_max)
     ks = _ks_per_checkpoint(ps, ls)
+    zs = _moment_z_per_checkpoint(ps, ls)
     lt.update(tag)
     out.update({"learned": lt, "ks": [round(k, 5) for k in ks], "ks_max": max(ks), "ks_bound": 0.02,
+                "z_mean": [round(z[0], 3) for z in zs], "z_var": [round(z[1], 3) for z in zs],
                 "speedup_events_per_s": lt["events_per_s"] / pt["events_per_s"],
                 "speedup_sim_time_per_s": lt["sim_time_per_s"] / pt["sim_time_per_s"]})
     # the batched form (the persistent kernel, MLP by mma.sync) on the same workload: plain and learned
@@ -438,13 +443,185 @@ def batch_report(t0: float = 0.001, t1: float = 0.006):
             y = sim.stats()
             s_ms += y.device_ms - x.device_ms
             s_ev += y.events - x.events
+    peak, peak_kind = _peaks()
+    sv_steps = int((steps * cells).sum())
+    achieved = sv_steps * 8 * 2 / (ms * 1e-3) / 1e9  # counts of both species read and written per subvolume-step
     return {"workload": f"brusselator x{n}: {int(cells.sum())} subvolumes, sides 8..48, reference semantics, FP64, "
                         f"slice t = {t0} -> {t1}",
+            "roofline": {"bound": "hbm", "kernel": "batch (persistent, all phases)", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                         "algorithmic_bytes_per_subvolume_step": 16},
             "tuning": tune, "events": ev, "device_ms": ms, "events_per_s": ev / (ms * 1e-3),
             "sim_time_per_s": (t1 - t0) / (ms * 1e-3), "subvolume_steps": int((steps * cells).sum()),
             "steps_per_replica_q0_50_100": [int(np.quantile(steps, q)) for q in (0, 0.5, 1)],
             "single_handles": {"device_ms": s_ms, "events": int(s_ev), "events_per_s": s_ev / (s_ms * 1e-3)},
             "speedup_vs_single_handles": s_ms / ms}
+
+
+def configs_report():
+    """The other configurations on this GPU, each on its own handle (CUDA events on the library's stream):
+
+    * small_ab 10^3 (1,000 subvolumes, 2 species, 3 reactions), reference semantics, FP64, t = 0 -> 10
+      as configured (state dumped every 1.0);
+    * the random network on 128^3 (2,097,152 subvolumes, 10 species, 20 reactions of order 0-2,
+      80 MB of counts per buffer), reference semantics, FP64 and FP32: 200 steps after 20 warm-up
+      steps (Cao tau ~1e-10 at these counts: t = 2 is out of reach of any tau-leaping step), with the
+      HBM roofline of its dominant kernel from an event-instrumented replay of 40 more steps:
+      8 S N bytes per leap launch (counts read and written), 4 S N + 9 N + 4 S N per classification."""
+    from pliscuda_b200 import Simulation, workloads
+    out = {}
+    m, st = workloads.small_ab(10)
+    with Simulation(m, mode="reference", precision="fp64", seed=SEED) as sim:
+        sim.set_state(st)
+        for t in range(1, 11):
+            r = sim.run(float(t))
+            sim.get_state()
+        out["small_ab10"] = {"workload": "small_ab 10^3, reference semantics, FP64, t = 0 -> 10, dumps every 1.0",
+                             "events": int(r.events), "steps": int(r.steps), "device_ms": float(r.device_ms),
+                             "events_per_s": r.events / (r.device_ms * 1e-3), "sim_time_per_s": r.time / (r.device_ms * 1e-3),
+                             "us_per_step": r.device_ms * 1e3 / max(1, r.steps)}
+    peak, peak_kind = _peaks()
+    m, st = workloads.random_network(128)
+    N, S = m.n_subvolumes, m.n_species
+    algo = {"leap": 8 * S * N, "classify": 8 * S * N + 9 * N, "exact": 0, "apply": 8 * S * N}
+    for prec in ("fp64", "fp32"):
+        with Simulation(m, mode="reference", precision=prec, seed=SEED) as sim:
+            sim.set_state(st)
+            sim.step(20)
+            a = sim.stats()
+            b = sim.step(200)
+            cur = sim.get_state()
+            tb = b.time
+            nb = b.steps
+        ms = b.device_ms - a.device_ms
+        with Simulation(m, mode="reference", precision=prec, seed=SEED, profile=True) as ps:
+            ps.set_state(cur, time=tb, steps=nb)
+            ps.step(40)
+            per = ps.kernel_profile()
+        dom = max(per, key=lambda k: per[k][0])
+        ms_launch = per[dom][0] / max(1, per[dom][1])
+        achieved = algo[dom] / (ms_launch * 1e-3) / 1e9
+        shares = {k: round(v[0] / max(1e-12, sum(x[0] for x in per.values())), 4) for k, v in per.items()}
+        out[f"random128_{prec}"] = {
+            "workload": f"random network S=10 R=20 on 128^3, reference semantics, {prec.upper()}, 200 steps after 20",
+            "events": int(b.events - a.events), "steps": int(b.steps - a.steps), "device_ms": ms,
+            "events_per_s": (b.events - a.events) / (ms * 1e-3), "sim_time_per_s": (b.time - a.time) / (ms * 1e-3),
+            "ms_per_step": ms / max(1, b.steps - a.steps), "kernel_share": shares,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind, "algorithmic_bytes_per_launch": algo[dom],
+                         "ms_per_launch": ms_launch,
+                         "hbm_frac_per_kernel": {k: (algo[k] / (v[0] / max(1, v[1]) * 1e-3) / 1e9) / peak
+                                                 for k, v in per.items() if v[1] and algo[k]}}}
+    return out
+
+
+REF_BINARY = os.path.join(ROOT, "oracle", "_ref", "pliscuda")
+
+
+def standin_schlogl(side: int = 64):
+    """A bimolecular stand-in of the Schlogl workload that the reference's CUDA build can express (it
+    has no trimolecular or zero-order channels, PLISCuda/src/rates.cu:3-40): species X and a constant
+    source species K (1 per subvolume, no diffusion); 2X -> 3X (k 0.01993), 2X -> X (k 0.03),
+    K -> K + X (k 3909), X -> 0 (k 3.5); X jump rate 1.0; X = 100 for x < side/2, 600 above.  At
+    X = 600 its channels fire at about the Schlogl rates (3582, 5391, 3909 and 2100 per unit time)
+    and X = 600 is its stable state.  It is labelled as a stand-in wherever it is reported."""
+    from pliscuda_b200 import Model
+    re = np.zeros((2, 4), np.int32)
+    pr = np.zeros((2, 4), np.int32)
+    re[0, 0], pr[0, 0] = 2, 3
+    re[0, 1], pr[0, 1] = 2, 1
+    re[1, 2], pr[1, 2], pr[0, 2] = 1, 1, 1
+    re[0, 3] = 1
+    n = side ** 3
+    m = Model(n_subvolumes=n, n_species=2, n_reactions=4, reactants=re.reshape(-1), products=pr.reshape(-1),
+              reaction_rates=[0.01993, 0.03, 3909.0, 3.5], diffusion_rates=[1.0, 0.0], lattice=(side, side, side))
+    x = np.arange(n) % side
+    state = np.concatenate([np.where(x < side // 2, 100, 600), np.ones(n, np.int64)]).astype(np.uint32)
+    return m, state
+
+
+def _replicated_fixture(name, copies):
+    """copies of one of the reference's fixtures (the arrays its own parsers produced, committed
+    under tests/golden/ref_fixtures) side by side in one topology"""
+    from pliscuda_b200 import Model
+    z = np.load(os.path.join(ROOT, "tests", "golden", "ref_fixtures", name + ".npz"))
+    n, s, r, c = (int(v) for v in z["dims"])
+    nb = z["neighbours"].reshape(n, 6).astype(np.int64)
+    big = np.concatenate([nb + k * n for k in range(copies)]).astype(np.uint32).reshape(-1)
+    st = np.tile(z["state"].reshape(s, n), (1, copies)).reshape(-1).astype(np.uint32)
+    m = Model(n_subvolumes=n * copies, n_species=s, n_reactions=r, reactants=z["reactants"], products=z["products"],
+              reaction_rates=z["rrc"].astype(np.float64), diffusion_rates=z["drc"].astype(np.float64), neighbours=big)
+    return m, st
+
+
+def _run_reference_binary(d, t_end):
+    """One run of the reference binary on the configuration in d to t_end: (wall s, steps, final time)."""
+    conf = os.path.join(d, "conf.txt")
+    lines = [(f"endTime={t_end}" if l.startswith("endTime=") else l) for l in open(conf).read().splitlines()]
+    with open(conf, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    for old in os.listdir(d):
+        if old.startswith("sim") and old.endswith(".dat"):
+            os.remove(os.path.join(d, old))
+    w0 = time.perf_counter()
+    r = subprocess.run([REF_BINARY, "conf.txt"], cwd=d, capture_output=True, text=True, timeout=600)
+    wall = time.perf_counter() - w0
+    if r.returncode != 0 or "Simulation Complete" not in r.stdout:
+        raise RuntimeError(f"reference binary failed ({r.returncode}): {r.stdout[-500:]} {r.stderr[-500:]}")
+    steps = tfin = None
+    for l in r.stdout.splitlines():
+        if "simulation steps:" in l:
+            steps = int(l.split(":")[1])
+        if "final simulation time:" in l:
+            tfin = float(l.split(":")[1].strip().rstrip("s"))
+    return wall, steps, tfin
+
+
+def reference_cuda_report():
+    """The reference's own CUDA build (oracle/_ref/pliscuda: its sources compiled for sm_100a by
+    oracle/ref_build.py --cuda) beside the new step, on the same GPU, on inputs both can express: the
+    bimolecular Schlogl stand-in on 64^3 (standin_schlogl) and replicated copies of the reference's own
+    react-64 and diff-64 fixtures.  The reference times its loop with std::clock (CPU time,
+    driver.cu:249, 386), so it is timed here by the wall clock around two whole runs to t1 and t2 of
+    the same input: (t2' - t1') / (wall2 - wall1) removes start-up and parsing, leaving sim-time/s and
+    steps/s of its loop.  It counts no events; its events/s is estimated as the new step's events per
+    unit of simulated time on the same input and interval (both run reference semantics, whose
+    ensembles agree statistically) times its sim-time/s.  The new step runs the same input (parsed from
+    the same files) in reference semantics, FP64: device time, and wall time of the run call."""
+    import tempfile
+    from pliscuda_b200 import Simulation, load_configuration, write_configuration
+    if not os.path.exists(REF_BINARY):
+        return {"unavailable": "oracle/_ref/pliscuda not built (needs the reference tree at build time)"}
+    cases = [("standin_schlogl64 (bimolecular stand-in of Schlogl 64^3, 262144 subvolumes)", standin_schlogl(64), 0.25, 1.25),
+             ("react-64 x 200 copies (12800 subvolumes)", _replicated_fixture("test_react-64", 200), 0.5, 2.0),
+             ("diff-64 x 100 copies (6400 subvolumes)", _replicated_fixture("test_diff-64", 100), 0.1, 0.5)]
+    rows = []
+    for name, (model, state), t1, t2 in cases:
+        with tempfile.TemporaryDirectory() as d:
+            write_configuration(d, model, state, end_time=t1)
+            fm, fs, _, _ = load_configuration(os.path.join(d, "conf.txt"))
+            _run_reference_binary(d, t1)  # warm-up: context creation, file cache
+            w1, n1, f1 = _run_reference_binary(d, t1)
+            w2, n2, f2 = _run_reference_binary(d, t2)
+        ref = {"sim_time_per_s": (f2 - f1) / (w2 - w1), "steps_per_s": (n2 - n1) / (w2 - w1),
+               "wall_s": [w1, w2], "steps": [n1, n2], "final_time": [f1, f2]}
+        with Simulation(fm, mode="reference", precision="fp64", seed=17) as sim:
+            sim.set_state(fs)
+            sim.run(t1)
+            a = sim.stats()
+            w0 = time.perf_counter()
+            b = sim.run(t2)
+            wall = time.perf_counter() - w0
+        dev_s = (b.device_ms - a.device_ms) / 1e3
+        ours = {"sim_time_per_s": (b.time - a.time) / dev_s, "steps_per_s": (b.steps - a.steps) / dev_s,
+                "events_per_s": (b.events - a.events) / dev_s, "sim_time_per_s_wall": (b.time - a.time) / wall,
+                "events_per_s_wall": (b.events - a.events) / wall, "steps": int(b.steps - a.steps)}
+        ev_per_t = (b.events - a.events) / max(1e-300, b.time - a.time)
+        ref["events_per_s_estimated"] = ev_per_t * ref["sim_time_per_s"]
+        rows.append({"input": name, "interval": [t1, t2], "reference_cuda": ref, "new_step": ours,
+                     "speedup_sim_time_per_s": ours["sim_time_per_s"] / ref["sim_time_per_s"],
+                     "speedup_sim_time_per_s_wall": ours["sim_time_per_s_wall"] / ref["sim_time_per_s"]})
+    return {"binary": "oracle/_ref/pliscuda (reference sources, sm_100a, release -O3, clock-seeded)", "cases": rows}
 
 
 def main(argv=None):
@@ -464,8 +641,13 @@ def main(argv=None):
     ap.add_argument("--precision-report", action="store_true", help="FP32 form vs binary64 on the precision config")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-tau comparison")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-replicas measurement")
+    ap.add_argument("--no-configs", action="store_true", help="skip the other configurations and the precision report")
+    ap.add_argument("--configs-report", action="store_true", help="print only the other configurations")
     ap.add_argument("--batch-report", action="store_true", help="print only the batched-replicas measurement")
     ap.add_argument("--learned-report", action="store_true", help="print only the learned-tau comparison")
+    ap.add_argument("--reference-cuda-report", action="store_true",
+                    help="print only the reference CUDA build against the new step on shared inputs")
+    ap.add_argument("--no-reference-cuda", action="store_true", help="skip the reference CUDA build comparison")
     ap.add_argument("--report-side", type=int, default=128)
     ap.add_argument("--report-steps", type=int, default=200)
     args = ap.parse_args(argv)
@@ -478,12 +660,19 @@ def main(argv=None):
     if args.ncu_batch_case:
         return ncu_batch_case(args)
     if args.precision_report:
-        return precision_report(args)
+        print(json.dumps(precision_report(args.report_side, args.report_steps)))
+        return 0
     if args.learned_report:
         print(json.dumps(learned_report()))
         return 0
     if args.batch_report:
         print(json.dumps(batch_report()))
+        return 0
+    if args.reference_cuda_report:
+        print(json.dumps(reference_cuda_report()))
+        return 0
+    if args.configs_report:
+        print(json.dumps(configs_report()))
         return 0
 
     import numpy as np
@@ -591,6 +780,16 @@ def main(argv=None):
     batched = None
     if rank == 0 and world == 1 and not args.no_batch:
         batched = batch_report()
+    configs = precision = None
+    if rank == 0 and world == 1 and not args.no_configs:
+        configs = configs_report()
+        precision = precision_report(args.report_side, args.report_steps)
+    ref_cuda = None
+    if rank == 0 and world == 1 and not args.no_reference_cuda:
+        try:
+            ref_cuda = reference_cuda_report()
+        except Exception as e:  # the comparison must not take the bench line down with it
+            ref_cuda = {"error": str(e)[:300]}
 
     if rank == 0:
         line = {
@@ -611,6 +810,9 @@ def main(argv=None):
             "clocks": ck,
             "learned": learned,
             "batched": batched,
+            "reference_cuda": ref_cuda,
+            "configs": configs,
+            "precision_report": precision,
         }
         print(json.dumps(line))
     replicas.finish(dist)

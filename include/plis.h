@@ -108,6 +108,10 @@ typedef struct plis_options {
   int32_t profile;            /* 1 = launch phase kernels one by one with CUDA events around each (plis_get_profile) */
   int32_t stage_halo;         /* lattice leap: 1 = stage brick + halo in shared memory, 0 = global atomics (default) */
   int32_t learned_mlp;        /* learned tau MLP: 0 = tcgen05.mma with TMEM accumulators (default), 1 = mma.sync */
+  uint64_t wait_polls;        /* polls after which a device-side wait gives up with PLIS_ERR_TIMEOUT: the grid
+                               * barrier of the persistent batched kernel (>= 32 ns per poll) and the mbarrier
+                               * waits of the tcgen05 MLP; 0 = defaults (2^26 and 2^22 polls).  The reference
+                               * has no device waits (its host loop synchronises, driver.cu:259-376). */
 } plis_options;
 
 /* Per-kernel device time accumulated while plis_options.profile is set (CUDA events recorded on the
@@ -229,9 +233,12 @@ int plis_read_event_log(plis_handle* h, plis_event_record* out, uint64_t max_rec
  * device memory (a host whose own allocator owns the device memory, or a latency-critical loop in
  * which cudaMalloc may synchronise the device).  It allocates nothing: inputs and outputs are the
  * caller's device buffers, and its 16 KiB of per-CTA partials live in a fixed array inside the
- * library, held on every device that loads the library until exit.  The first call on a device,
- * made with that device current, looks up that array's device address; make it before any stream
- * capture.  Calls share the array, so calls that overlap on the GPU race.  n must be in
+ * library, held on every device that loads the library until exit.  Each call looks up that array's
+ * device address in the context current on the calling thread (the runtime's context of the current
+ * device, also after cudaDeviceReset); the first call on a device may load the library's device code
+ * there, so make it before any stream capture.  Calls share the array, so calls that overlap on the
+ * GPU race.  NaN taus are skipped (they compare below nothing): NaNs only give (+inf, -1), NaNs among
+ * numbers give the arg-min of the numbers; +inf only gives (+inf, 0).  n must be in
  * 1..PLIS_NOALLOC_MAX_TAUS, else PLIS_ERR_LIMIT. */
 #define PLIS_NOALLOC_MAX_TAUS 2147483647u
 int plis_tau_argmin_noalloc(const double* d_tau, uint64_t n, double* d_min_tau, int64_t* d_argmin, void* stream);

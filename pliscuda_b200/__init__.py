@@ -34,6 +34,7 @@ from ._lib import (EVENT_DTYPE, EVENT_KINDS, LEAP_CR, LEAP_NOCR, MODE_CORRECTED,
 __all__ = [
     "Model", "Simulation", "PlisError", "InvalidArgument", "load_configuration", "run_simulation",
     "canonical_neighbours", "write_snapshot", "read_snapshot", "parse_topology", "parse_state", "parse_reactions",
+    "write_configuration",
     "LEAP_CR", "LEAP_NOCR", "SSA", "SSA_FF", "MODE_REFERENCE", "MODE_CORRECTED", "PREC_FP64", "PREC_FP32",
     "STOP_NONE", "STOP_TIME", "STOP_STEPS", "STOP_NO_EVENT", "STOP_ERROR", "EVENT_DTYPE", "EVENT_KINDS", "library_path",
 ]
@@ -128,7 +129,7 @@ class Simulation:
                  seed: int = 1, replica: int = 0, device: int = 0, critical_threshold: int = 10,
                  epsilon: float = 0.05, max_rollbacks: int = 64, steps_per_launch: int = 0,
                  tile: Optional[Sequence[int]] = None, profile: bool = False, stage_halo: bool = False,
-                 learned_mlp: str = "tcgen05"):
+                 learned_mlp: str = "tcgen05", wait_polls: int = 0):
         if isinstance(mode, str):
             mode = {"reference": MODE_REFERENCE, "corrected": MODE_CORRECTED}[mode]
         if isinstance(precision, str):
@@ -138,7 +139,7 @@ class Simulation:
         kw = dict(mode=mode, precision=precision, seed=seed, replica=replica, device=device,
                   critical_threshold=critical_threshold, epsilon=epsilon, max_rollbacks=max_rollbacks,
                   steps_per_launch=steps_per_launch, profile=int(bool(profile)), stage_halo=int(bool(stage_halo)),
-                  learned_mlp={"tcgen05": 0, "mma.sync": 1}[learned_mlp])
+                  learned_mlp={"tcgen05": 0, "mma.sync": 1}[learned_mlp], wait_polls=int(wait_polls))
         if tile is not None:
             kw["tile"] = tile
         self.options = _lib.default_options(**kw)
@@ -271,6 +272,54 @@ def load_configuration(conf_path: str) -> Tuple[Model, np.ndarray, float, float]
         return model, state, float(v.end_time), float(v.log_freq)
     finally:
         _lib.lib.plis_config_free(h)
+
+
+def write_configuration(d: str, model: Model, state: np.ndarray, end_time: float = 1.0, log_freq: float = 0.0) -> str:
+    """Write a model and its initial counts in the reference's input formats under directory d
+    (conf.txt with topology, reactions, state and constants files, and the compartments file when
+    there are several: spec/*.md, Configuration.hpp:27-144), the inverse of load_configuration.
+    A lattice model's topology is written as its neighbour table.  Rates are written as the
+    reference reads them, in binary32.  Returns the path of conf.txt."""
+    N, S, R, C = model.n_subvolumes, model.n_species, model.n_reactions, model.n_compartments
+    nb = model.neighbours if model.neighbours is not None else canonical_neighbours(N, None, model.lattice)[0]
+    nb = np.asarray(nb, np.int64).reshape(N, 6)
+    with open(os.path.join(d, "topology.txt"), "w") as f:
+        f.write(f"subvolumes: {N}\n\n")
+        own = np.arange(N)[:, None]
+        for c in range(N):
+            row = nb[c][nb[c] != own[c]]
+            f.write(f"{c}: " + "".join(f"{b} " for b in row.tolist()) + "\n")
+    st = np.asarray(state).reshape(S, N)
+    with open(os.path.join(d, "state.txt"), "w") as f:
+        f.write(f"subvolumes: {N}\nspecies: {S}\n\n")
+        nz = np.nonzero(st.any(axis=0))[0]
+        cols = st[:, nz].T.tolist()
+        f.write("".join(f"{c}: " + " ".join(map(str, v)) + "\n" for c, v in zip(nz.tolist(), cols)))
+    re = model.reactants.reshape(S, R)
+    pr = model.products.reshape(S, R)
+    with open(os.path.join(d, "reactions.txt"), "w") as f:
+        f.write(f"reactions: {R}\nspecies: {S}\n\n")
+        for r in range(R):
+            f.write(" ".join(str(int(v)) for v in re[:, r]) + " -> " + " ".join(str(int(v)) for v in pr[:, r]) + "\n")
+    consts = []
+    for k in range(C):
+        p = f"constants{k + 1}.txt"
+        with open(os.path.join(d, p), "w") as f:
+            f.write(" ".join(repr(float(np.float32(v))) for v in model.reaction_rates[k * R:(k + 1) * R]) + "\n")
+            f.write(" ".join(repr(float(np.float32(v))) for v in model.diffusion_rates[k * S:(k + 1) * S]) + "\n")
+        consts.append(p)
+    lines = ["topology=topology.txt", "reactions=reactions.txt", "initialState=state.txt",
+             f"endTime={end_time}", f"logFreq={log_freq}", f"compartments={C}"]
+    if C > 1:
+        with open(os.path.join(d, "subvc.txt"), "w") as f:
+            for c in range(N):
+                f.write(f"{c}: {int(model.compartment[c])}\n")
+        lines.append("compartmentsFile=subvc.txt")
+    lines += [f"constants={p}" for p in consts]
+    path = os.path.join(d, "conf.txt")
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    return path
 
 
 def parse_topology(path: str) -> Tuple[int, np.ndarray]:

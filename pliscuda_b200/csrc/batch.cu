@@ -372,8 +372,10 @@ int BatchEngine::launch(uint32_t max_iters) {
   BatchArgs B = make_args(dm_, dopt_, geo_, d_views_, d_rep_, nrep_, R_, S_, d_rr_, d_dr_, d_ctrl_, d_X_, d_tau_,
                           d_flag_, d_D_, d_slot_tau_, d_slot_idx_, d_slot_cr_, d_slot_bad_, d_work_, d_bar_, d_err_,
                           max_iters);
+  if (opt_.wait_polls) B.spin_limit = opt_.wait_polls;
   PLIS_CU(cudaMemsetAsync(d_work_, 0, 12 * sizeof(unsigned), stream_));
   PLIS_CU(cudaMemsetAsync(d_bar_, 0, 2 * sizeof(unsigned), stream_));
+  PLIS_CU(cudaMemsetAsync(d_err_, 0, sizeof(int), stream_));  // a timed-out launch does not poison the next
   void* args[] = {&B};
   PLIS_CU(cudaLaunchCooperativeKernel(launch_.kernel, dim3(grid_), dim3(geo_.threads), args,
                                       batch_dyn_smem(geo_.box_bytes, nrep_), stream_));

@@ -191,6 +191,7 @@ int Engine::create(const Model& model, const plis_options& opt) {
   PLIS_CU(cudaMemset(b.ctrl, 0, sizeof(Ctrl)));
 
   DevOpts& o = args_.o;
+  o.mlp_wait = opt.wait_polls > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)opt.wait_polls;
   o.mode = opt.mode;
   o.nc = opt.critical_threshold;
   o.max_rollbacks = opt.max_rollbacks;

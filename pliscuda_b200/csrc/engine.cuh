@@ -113,7 +113,7 @@ struct DevOpts {
   int32_t mode;
   int32_t nc;
   int32_t max_rollbacks;
-  int32_t pad_;
+  uint32_t mlp_wait;  // polls of each mbarrier wait of the tcgen05 MLP before it gives up (0: the default)
   double eps;
   unsigned long long seed;
   uint32_t replica;

@@ -124,11 +124,11 @@ __global__ void __launch_bounds__(256) k_learned_pre(KArgs A) {
 
 __global__ void __launch_bounds__(128) k_mlp_tc(const Ctrl* __restrict__ K, const LearnedParams* __restrict__ P,
                                                 const uint4* __restrict__ feats, float* __restrict__ y, uint32_t nrows,
-                                                uint32_t ntiles, int* status) {
+                                                uint32_t ntiles, int* status, uint32_t wait_limit) {
   extern __shared__ __align__(128) uint8_t tsm[];
   pdl_entry();
   if (K && K->done) return;
-  tc::mlp_tiles(tc_params(P), feats, y, nrows, ntiles, tsm, status);
+  tc::mlp_tiles(tc_params(P), feats, y, nrows, ntiles, tsm, status, wait_limit);
 }
 
 template <typename Real, int MAXS>
@@ -258,7 +258,8 @@ struct LearnedSet {
     launch_pdl(k_learned_pre<Real, MAXS>, g, b, 0, s, a);
     const uint32_t ntiles = a.m.Npad / 128u + ((a.m.Npad % 128u) ? 1u : 0u);
     launch_pdl(k_mlp_tc, dim3(mlp_grid(ntiles)), dim3(128), tc::kPSmemBytes, s, (const Ctrl*)a.b.ctrl,
-               (const LearnedParams*)a.b.lp, (const uint4*)a.b.feat, a.b.ymlp, a.m.Npad, ntiles, (int*)&a.b.ctrl->status);
+               (const LearnedParams*)a.b.lp, (const uint4*)a.b.feat, a.b.ymlp, a.m.Npad, ntiles, (int*)&a.b.ctrl->status,
+               a.o.mlp_wait);
     launch_pdl(k_learned_post<Real, MAXS>, g, b, 0, s, a);
   }
   static void features(const KArgs& a, TraceRec* out, uint32_t offset, uint32_t stride, uint32_t count,
@@ -890,7 +891,7 @@ int Learner::predict(const float* features, uint64_t n, float* y, int mlp_kernel
       if (e == cudaSuccess) {
         k_feat_rows<<<(unsigned)((ntiles * 128 + 255) / 256), 256, 0, stream_>>>(packed_, d_f, n, ntiles * 128, d_rows);
         k_mlp_tc<<<mlp_grid((uint32_t)ntiles), 128, tc::kPSmemBytes, stream_>>>(nullptr, packed_, d_rows, d_y,
-                                                                                (uint32_t)n, (uint32_t)ntiles, d_st);
+                                                                                (uint32_t)n, (uint32_t)ntiles, d_st, 0u);
         e = cudaStreamSynchronize(stream_);
       }
       if (d_rows) cudaFree(d_rows);

@@ -9,14 +9,21 @@
 // library keeps until the process exits.
 //
 // Host code cannot pass the array's name to a kernel (on the host it is only a stand-in for the
-// device symbol), so its device address is looked up with cudaGetSymbolAddress once per device, on
-// the first call made while that device is current, and cached.  Make that first call before any
-// stream capture.  All calls share the array and it keeps the last call's contents; nothing in it
-// needs to start at zero (every partial a call reads was written by the same call).  Two calls whose
-// kernels overlap on the GPU (different streams, or different host threads) race on the array.
+// device symbol), so every call looks up its device address in the context current on the calling
+// thread with cudaGetSymbolAddress, checks the result, and passes that address to the kernels.  The
+// lookup allocates nothing and is cheap; doing it on every call (rather than caching an address per
+// device ordinal) keeps it right after cudaDeviceReset and for whichever context the runtime has
+// current.  The first call on a device may load the library's device code there (lazy module
+// loading), so make it before any stream capture.  All calls share the array and it keeps the last
+// call's contents; nothing in it needs to start at zero (every partial a call reads was written by
+// the same call).  Two calls whose kernels overlap on the GPU (different streams, or different host
+// threads) race on the array.
+//
+// NaN taus never compare below anything, so they are skipped: an input of NaNs only gives
+// (+inf, -1), and NaNs mixed with numbers give the arg-min of the numbers.  An input of +inf only
+// gives (+inf, 0): the first index wins the tie.
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <string>
 
 #include "../../include/plis.h"
@@ -29,7 +36,6 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kMaxPartials = 1024;  // CTAs of the first pass = entries of the scratch array
-constexpr int kMaxDevices = 64;
 
 struct Partial {
   double tau;
@@ -37,9 +43,6 @@ struct Partial {
 };
 
 static __device__ __align__(256) Partial g_argmin_scratch[kMaxPartials];
-
-std::mutex g_mu;
-Partial* g_scratch_ptr[kMaxDevices] = {};
 
 __device__ __forceinline__ void min_pair(double& t, long long& i, double t2, long long i2) {
   if (t2 < t || (t2 == t && i2 < i)) { t = t2; i = i2; }
@@ -105,28 +108,11 @@ extern "C" int plis_tau_argmin_noalloc(const double* d_tau, uint64_t n, double* 
     plis::set_error("plis_tau_argmin_noalloc: n must be in 1.." + std::to_string((unsigned long long)PLIS_NOALLOC_MAX_TAUS));
     return PLIS_ERR_LIMIT;
   }
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) {
-    plis::set_error(std::string("plis_tau_argmin_noalloc: cudaGetDevice: ") + cudaGetErrorString(e));
+  Partial* scratch = nullptr;  // the array's device address in the current context
+  cudaError_t e = cudaGetSymbolAddress((void**)&scratch, g_argmin_scratch);
+  if (e != cudaSuccess || !scratch) {
+    plis::set_error(std::string("plis_tau_argmin_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
     return e == cudaErrorNoDevice ? PLIS_ERR_NO_DEVICE : PLIS_ERR_CUDA;
-  }
-  if (dev < 0 || dev >= kMaxDevices) {
-    plis::set_error("plis_tau_argmin_noalloc: device ordinal out of range");
-    return PLIS_ERR_INVALID;
-  }
-  Partial* scratch = nullptr;
-  {
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_scratch_ptr[dev]) {  // first call on this device: resolve the array's device address
-      e = cudaGetSymbolAddress((void**)&scratch, g_argmin_scratch);
-      if (e != cudaSuccess) {
-        plis::set_error(std::string("plis_tau_argmin_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        return PLIS_ERR_CUDA;
-      }
-      g_scratch_ptr[dev] = scratch;
-    }
-    scratch = g_scratch_ptr[dev];
   }
   const long long nn = (long long)n;
   long long blocks = (nn + kThreads - 1) / kThreads;

@@ -94,8 +94,8 @@ __device__ __forceinline__ uint32_t canon(uint32_t row, uint32_t k, uint32_t chu
 }
 
 // wait for the mbarrier phase `parity`; false (and *err set) when the limit ran out
-__device__ __forceinline__ bool wait_phase(uint32_t bar, uint32_t parity, volatile int* err) {
-  for (uint32_t i = 0; i < kWaitLimit; ++i) {
+__device__ __forceinline__ bool wait_phase(uint32_t bar, uint32_t parity, volatile int* err, uint32_t limit) {
+  for (uint32_t i = 0; i < limit; ++i) {
     if (try_wait(bar, parity)) return true;
     if (*err) return false;
   }
@@ -127,7 +127,8 @@ static_assert(kPSmemBytes * 6 > 228 * 1024, "at most 5 CTAs per SM");
 // readable) with the MLP on tcgen05.  Tiles are taken round robin; every CTA loads the weights once.
 // A wait that runs out sets *status and the CTA stops; TMEM is always freed.
 static __device__ void mlp_tiles(const Params& P, const uint4* __restrict__ feats, float* __restrict__ y, uint32_t nrows,
-                          uint32_t ntiles, uint8_t* smem, int* status) {
+                          uint32_t ntiles, uint8_t* smem, int* status, uint32_t wait_limit = 0) {
+  if (wait_limit == 0) wait_limit = kWaitLimit;
   __shared__ int s_err;
   const uint32_t tid = threadIdx.x;  // blockDim.x == 128
   const uint32_t warp = tid >> 5;
@@ -183,7 +184,7 @@ static __device__ void mlp_tiles(const Params& P, const uint4* __restrict__ feat
         }
         commit(bar);
       }
-      bool got = !*err && wait_phase(bar, phase & 1u, (volatile int*)err);
+      bool got = !*err && wait_phase(bar, phase & 1u, (volatile int*)err, wait_limit);
       phase += 1;
       fence_after();
       ok = __syncthreads_and(got && !*err) != 0;

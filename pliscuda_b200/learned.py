@@ -154,6 +154,27 @@ def _ks_per_checkpoint(a, b) -> list:
     return [max(ks_distance(x[s], y[s]) for s in range(x.shape[0])) for x, y in zip(a, b)]
 
 
+def _moment_z_per_checkpoint(a, b) -> list:
+    """Per checkpoint (z of the mean, z of the variance) of the pooled subvolume counts, the species
+    with the largest |z| each, standard errors as for independent samples (var/n for the mean,
+    (m4 - var^2)/n for the variance).  Neighbouring subvolumes are correlated, so these are
+    descriptive: the replica-based test (tests/test_learned_stats_gpu.py) is the statistical check."""
+    out = []
+    for x, y in zip(a, b):
+        zm = zv = 0.0
+        for s in range(x.shape[0]):
+            u, v = x[s].astype(np.float64), y[s].astype(np.float64)
+            se = np.sqrt(u.var() / u.size + v.var() / v.size)
+            z1 = (v.mean() - u.mean()) / se if se > 0 else 0.0
+            m4u, m4v = np.mean((u - u.mean()) ** 4), np.mean((v - v.mean()) ** 4)
+            sev = np.sqrt(max(m4u - u.var() ** 2, 0) / u.size + max(m4v - v.var() ** 2, 0) / v.size)
+            z2 = (v.var() - u.var()) / sev if sev > 0 else 0.0
+            zm = z1 if abs(z1) > abs(zm) else zm
+            zv = z2 if abs(z2) > abs(zv) else zv
+        out.append((float(zm), float(zv)))
+    return out
+
+
 def compare(model: Model, state: np.ndarray, weights: np.ndarray, s_max: float, checkpoints: Sequence[float], *,
             precision: str = "fp64", seeds: Tuple[int, int] = (101, 202), device: int = 0) -> Dict:
     """Plain method and proposer (corrected mode, independent seeds) from the same state to each

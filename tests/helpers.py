@@ -102,44 +102,7 @@ def assert_same(sim, orc, where=""):
 
 
 def write_reference_files(d, model, state, end_time=1.0, log_freq=0.0):
-    """Write a model in the reference's input formats (spec/*.md, Configuration.hpp:27-144) under
-    directory d; returns the conf.txt path."""
-    import os
-    N, S, R, C = model.n_subvolumes, model.n_species, model.n_reactions, model.n_compartments
-    nb = model.neighbours.reshape(N, 6)
-    with open(os.path.join(d, "topology.txt"), "w") as f:
-        f.write(f"subvolumes: {N}\n\n")
-        for c in range(N):
-            row = [int(b) for b in nb[c] if b != c]
-            f.write(f"{c}: " + "".join(f"{b} " for b in row) + "\n")
-    st = np.asarray(state).reshape(S, N)
-    with open(os.path.join(d, "state.txt"), "w") as f:
-        f.write(f"subvolumes: {N}\nspecies: {S}\n\n")
-        for c in range(N):
-            if st[:, c].any():
-                f.write(f"{c}: " + " ".join(str(int(v)) for v in st[:, c]) + "\n")
-    re = model.reactants.reshape(S, R)
-    pr = model.products.reshape(S, R)
-    with open(os.path.join(d, "reactions.txt"), "w") as f:
-        f.write(f"reactions: {R}\nspecies: {S}\n\n")
-        for r in range(R):
-            f.write(" ".join(str(int(v)) for v in re[:, r]) + " -> " + " ".join(str(int(v)) for v in pr[:, r]) + "\n")
-    consts = []
-    for k in range(C):
-        p = f"constants{k + 1}.txt"
-        with open(os.path.join(d, p), "w") as f:
-            f.write(" ".join(repr(float(np.float32(v))) for v in model.reaction_rates[k * R:(k + 1) * R]) + "\n")
-            f.write(" ".join(repr(float(np.float32(v))) for v in model.diffusion_rates[k * S:(k + 1) * S]) + "\n")
-        consts.append(p)
-    lines = ["topology=topology.txt", "reactions=reactions.txt", "initialState=state.txt",
-             f"endTime={end_time}", f"logFreq={log_freq}", f"compartments={C}"]
-    if C > 1:
-        with open(os.path.join(d, "subvc.txt"), "w") as f:
-            for c in range(N):
-                f.write(f"{c}: {int(model.compartment[c])}\n")
-        lines.append("compartmentsFile=subvc.txt")
-    lines += [f"constants={p}" for p in consts]
-    path = os.path.join(d, "conf.txt")
-    with open(path, "w") as f:
-        f.write("\n".join(lines) + "\n")
-    return path
+    """Write a model in the reference's input formats under directory d; returns the conf.txt path
+    (pliscuda_b200.write_configuration)."""
+    from pliscuda_b200 import write_configuration
+    return write_configuration(d, model, state, end_time=end_time, log_freq=log_freq)

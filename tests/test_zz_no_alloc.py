@@ -61,7 +61,37 @@ def test_noalloc_argmin_edge_cases():
     assert _noalloc(_lib.lib, inf, 10, out_t, out_i, stream) == 0
     torch.cuda.synchronize()
     assert out_t.item() == float("inf") and out_i.item() == 0
+    # NaNs compare below nothing: NaNs only give (+inf, -1); NaNs among numbers are skipped
+    nan = torch.full((1000,), float("nan"), dtype=torch.float64, device="cuda")
+    assert _noalloc(_lib.lib, nan, 1000, out_t, out_i, stream) == 0
+    torch.cuda.synchronize()
+    assert out_t.item() == float("inf") and out_i.item() == -1
+    nan[::3] = torch.arange(334, dtype=torch.float64, device="cuda")[: nan[::3].numel()] + 2.0
+    nan[500] = 0.5
+    nan[501] = 0.5
+    assert _noalloc(_lib.lib, nan, 1000, out_t, out_i, stream) == 0
+    torch.cuda.synchronize()
+    assert (out_t.item(), out_i.item()) == (0.5, 500)
     # sizes beyond the stated maximum and empty inputs are rejected before any launch
     assert _noalloc(_lib.lib, tau, 0, out_t, out_i, stream) == 9
     assert _noalloc(_lib.lib, tau, 2**31, out_t, out_i, stream) == 9
     assert b"1..2147483647" in _lib.lib.plis_last_error()
+
+
+def test_noalloc_argmin_on_a_caller_stream():
+    """Both kernels are enqueued on the stream the caller passes: a non-default stream, synchronised
+    alone, holds the result."""
+    import torch
+
+    from pliscuda_b200 import _lib
+    rng = np.random.default_rng(11)
+    host = rng.exponential(1.0, size=300_001)
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        tau = torch.from_numpy(host).to("cuda", non_blocking=False)
+        out_t = torch.full((1,), -1.0, dtype=torch.float64, device="cuda")
+        out_i = torch.full((1,), -7, dtype=torch.int64, device="cuda")
+        for _ in range(2):
+            assert _noalloc(_lib.lib, tau, host.size, out_t, out_i, side.cuda_stream) == 0
+    side.synchronize()
+    assert (out_t.item(), out_i.item()) == (float(host.min()), int(np.argmin(host)))
