@@ -6,6 +6,8 @@ reports PLIS_ERR_TIMEOUT.  With a limit of two polls (about 64 ns) the first CTA
 give up long before the last ones arrive, so the run ends with PLIS_ERR_TIMEOUT.  Nothing spins
 without a bound here: the test only makes the bound short.  Afterwards the handle still answers and
 the CUDA context is intact: a batch with the default limit on the same device matches the oracle.
+A state set after a timeout is accepted; the first classification that runs on it waits at the same
+barriers, so with the same limit it gives up the same way.
 (The reference has no device-side waits: its host loop synchronises after every kernel,
 driver.cu:259-376.)"""
 import numpy as np
@@ -33,9 +35,11 @@ def test_batch_grid_barrier_gives_up_and_the_context_survives():
             b.step(5)
         assert e.value.status == 6, e.value  # PLIS_ERR_TIMEOUT
         assert "timed out" in str(e.value)
-        # the handle still answers
+        # the handle still answers: a new state is accepted, and the next run gives up the same way
         b.set_state(0, reps[0][1])
-        b.stats(0)
+        with pytest.raises(PlisError) as e:
+            b.step(1)
+        assert e.value.status == 6
     with Batch.from_models([m for m, _ in reps[:3]], seed=2) as b:
         for r, (_, st) in enumerate(reps[:3]):
             b.set_state(r, st)
