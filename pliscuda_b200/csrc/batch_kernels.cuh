@@ -250,6 +250,7 @@ __global__ void __launch_bounds__(256, LEARNED ? PLIS_BATCH_MIN_BLOCKS_LEARNED :
         L.step = K->step + 1;
         L.attempt = K->attempt;
         L.t = K->t;
+        L.ff_free = K->ff_free != 0;
         const Real tl = (Real)K->tau_leap;
         long long ev;
         int big;
@@ -350,7 +351,7 @@ __global__ void __launch_bounds__(256, LEARNED ? PLIS_BATCH_MIN_BLOCKS_LEARNED :
         int fl, bad;
         bool valid;
         classify_tile<Real, MAXS, false>(sA, tile, C, tn, ti, fl, bad, valid);
-        if (classify_slot(sA, K, tile, sA.g.nblocks, tn, ti, valid && fl == F_LEAP_CR, bad))
+        if (classify_slot(sA, K, tile, sA.g.nblocks, tn, ti, valid && fl == F_LEAP_CR, bad, valid && fl == F_SSA_FF))
           classify_control(sA, K, sA.g.nblocks);
       }
       __syncthreads();

@@ -36,7 +36,7 @@ struct Ctrl {
   uint32_t phase;        // 0: initial classification pending, 1: stepping
   int32_t done, status, stop_reason;
   uint32_t blocks_done;
-  uint32_t pad_;
+  uint32_t ff_free;      // 1: the classification behind the current flags left no SSA_FF subvolume (0: unknown)
   unsigned long long events, exact_events, rollbacks;
   unsigned long long ev_attempt, ex_attempt;
   // learned tau proposals (corrected mode): attempt 0 leaps with the arg-min of the proposed taus,

@@ -140,13 +140,15 @@ __device__ __forceinline__ void diffusion_draws(const KArgs& A, uint32_t c, int 
   }
   if (!(lam < (Real)10)) {
 #pragma unroll
-    for (int j = 0; j < 6; ++j) {
-      k[j] = 0;
-      if (j < n) {
-        plis_stream st = plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_diff(s, j));
-        const long long kj = plis_count_d(plis_poisson_d(&st, (double)lam));
-        k[j] = (int32_t)(kj < kBigJump ? kj : kBigJump);  // a jump of 2^27 or more rolls the attempt back
-      }
+    for (int j = 0; j < 6; ++j) k[j] = 0;
+#pragma unroll 1
+    for (int j = 0; j < n; ++j) {  // one inlined PTRS for the n slots
+      plis_stream st = plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_diff(s, j));
+      const long long kj = plis_count_d(plis_poisson_d(&st, (double)lam));
+      const int32_t v = (int32_t)(kj < kBigJump ? kj : kBigJump);  // a jump of 2^27 or more rolls the attempt back
+#pragma unroll
+      for (int t = 0; t < 6; ++t)
+        if (t == j) k[t] = v;
     }
     return;
   }
@@ -529,15 +531,38 @@ __device__ __forceinline__ bool classify_ff(int mode, double tau_cur, uint8_t fl
 // WALK: the neighbour loops are unrolled (for_each_nbr); with WALK false they run to the run-time
 // count over nbr_info's slot arrays, which needs fewer registers where the kernel arguments live in
 // global memory (the batched kernel's per-replica views).
-template <typename Real, bool WALK = true, int MAXS>
+// CACHE: every propensity and criticality of the subvolume is evaluated once, the propensities
+// into the thread's column of `pc` (shared memory, pc[r * stride], R <= kPropCache) and the critical
+// flags into a bit mask, and the loops below read them back; without it each loop evaluates them
+// again (the batched and learned kernels, and models with more reactions).  Same values either way.
+constexpr int kPropCache = 20;  // 20 x 256 threads x 8 B = 40 KB: under the 48 KB a launch gets without opting in
+template <typename Real, bool WALK = true, bool CACHE = false, int MAXS>
 __device__ __forceinline__ void cell_tau_parts(const KArgs& A, uint32_t c, const Nbr& q, const Counts<MAXS>& x,
-                                               const int32_t* Xe, Real& tau_ncr_out, Real& rate_cr_out) {
+                                               const int32_t* Xe, Real& tau_ncr_out, Real& rate_cr_out,
+                                               Real* pc = nullptr, uint32_t stride = 0) {
   const DevModel& m = A.m;
   const int mode = A.o.mode;
   const int nc = A.o.nc;
   const int comp = comp_of(m, c);
   const int n = q.n;
   const int S = (int)m.S, R = (int)m.R;
+  uint32_t critm = 0;
+  if constexpr (CACHE) {
+    for (int r = 0; r < R; ++r) {
+      const Real a = prop<Real>(m, x, r, comp);
+      pc[r * stride] = a;
+      const bool cr = (mode == 0) ? crit_ref(m, x, r, nc) : crit_fix(m, x, r, a, nc);
+      critm |= (uint32_t)cr << r;
+    }
+  }
+  auto propensity = [&](int r) -> Real {
+    if constexpr (CACHE) return pc[r * stride];
+    else return prop<Real>(m, x, r, comp);
+  };
+  auto critical = [&](int r, Real a) -> bool {  // crit_ref in reference mode, crit_fix in corrected mode
+    if constexpr (CACHE) return ((critm >> r) & 1u) != 0u;
+    else return (mode == 0) ? crit_ref(m, x, r, nc) : crit_fix(m, x, r, a, nc);
+  };
   Real tau_ncr = RT<Real>::inf();
   for (int s = 0; s < S; ++s) {
     const int32_t xs = x.get(s);
@@ -545,14 +570,14 @@ __device__ __forceinline__ void cell_tau_parts(const KArgs& A, uint32_t c, const
     const int r0 = m.sr_off[s], r1 = m.sr_off[s + 1];
     if (mode == 0) {
       bool skip_r = false;
-      for (int i = r0; i < r1 && !skip_r; ++i) skip_r = crit_ref(m, x, m.sr_r[i], nc);
+      for (int i = r0; i < r1 && !skip_r; ++i) skip_r = critical(m.sr_r[i], (Real)0);
       include = !(skip_r && xs < nc);  // tau.cu:165
     } else {
       include = false;
       for (int i = r0; i < r1 && !include; ++i) {
         const int r = m.sr_r[i];
-        const Real a = prop<Real>(m, x, r, comp);
-        include = (a > (Real)0) && !crit_fix(m, x, r, a, nc);
+        const Real a = propensity(r);
+        include = (a > (Real)0) && !critical(r, a);
       }
       if (!include && xs >= nc && drate<Real>(m, comp, s) > (Real)0 && n > 0) include = true;
     }
@@ -564,8 +589,8 @@ __device__ __forceinline__ void cell_tau_parts(const KArgs& A, uint32_t c, const
     for (int i = p0; i < p1; ++i) {
       const int r = m.sp_r[i];
       const int nu = m.sp_nu[i];
-      const Real a = prop<Real>(m, x, r, comp);
-      const bool ncrit = (mode == 0) ? !crit_ref(m, x, r, nc) : ((a > (Real)0) && !crit_fix(m, x, r, a, nc));
+      const Real a = propensity(r);
+      const bool ncrit = (mode == 0) ? !critical(r, a) : ((a > (Real)0) && !critical(r, a));
       if (!ncrit) continue;
       mu = mu + (Real)nu * a;
       s2 = s2 + (Real)(nu * nu) * a;
@@ -610,9 +635,8 @@ __device__ __forceinline__ void cell_tau_parts(const KArgs& A, uint32_t c, const
   const bool ncr_inf = plis_isinf_d((double)tau_ncr);
   if (mode == 0 || !ncr_inf) {
     for (int r = 0; r < R; ++r) {
-      const Real a = prop<Real>(m, x, r, comp);
-      const bool cr = (mode == 0) ? crit_ref(m, x, r, nc) : crit_fix(m, x, r, a, nc);
-      if (cr) rsum = rsum + a;
+      const Real a = propensity(r);
+      if (critical(r, a)) rsum = rsum + a;
     }
     for (int s = 0; s < S; ++s) {
       const int32_t xs = x.get(s);
@@ -622,7 +646,7 @@ __device__ __forceinline__ void cell_tau_parts(const KArgs& A, uint32_t c, const
       }
     }
   } else {
-    for (int r = 0; r < R; ++r) rsum = rsum + prop<Real>(m, x, r, comp);
+    for (int r = 0; r < R; ++r) rsum = rsum + propensity(r);
     for (int s = 0; s < S; ++s) dsum = dsum + (Real)n * (drate<Real>(m, comp, s) * (Real)x.get(s));
   }
   tau_ncr_out = tau_ncr;
@@ -654,13 +678,13 @@ __device__ __forceinline__ void cell_decide(double tn, double tcr, double& tau_o
 // ------------------------------------------------------------------------------------------------
 // classification of one subvolume (compute_taus, tau.cu:197-252)
 // ------------------------------------------------------------------------------------------------
-template <typename Real, bool WALK = true, int MAXS>
+template <typename Real, bool WALK = true, bool CACHE = false, int MAXS>
 __device__ void classify_cell(const KArgs& A, uint32_t c, const Nbr& q, const Counts<MAXS>& x, const int32_t* Xe,
                               double tau_cur, uint8_t flag_cur, uint64_t step, uint32_t attempt,
-                              double ff, double& tau_out, int& flag_out) {
+                              double ff, double& tau_out, int& flag_out, Real* pc = nullptr, uint32_t stride = 0) {
   if (classify_ff(A.o.mode, tau_cur, flag_cur, step, ff, tau_out, flag_out)) return;
   Real tau_ncr, rate;
-  cell_tau_parts<Real, WALK>(A, c, q, x, Xe, tau_ncr, rate);
+  cell_tau_parts<Real, WALK, CACHE>(A, c, q, x, Xe, tau_ncr, rate, pc, stride);
   const double tcr = cell_tau_cr<Real>(A, c, step, attempt, rate);
   cell_decide((double)tau_ncr, tcr, tau_out, flag_out);
 }
@@ -795,6 +819,7 @@ struct LeapCtx {
   uint64_t step;
   uint32_t attempt;
   double t;  // simulated time at the start of the step (event log)
+  bool ff_free;  // no subvolume is SSA_FF: the receivers' flag updates are no-ops and are skipped
 };
 
 // Leap of one brick (or one 1-D block of a table topology) by the whole CTA; returns this thread's
@@ -837,7 +862,7 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
         Real u[4], lam[4];
         bool act[4];
         long long kk[4];
-        uint32_t need = 0;
+        uint32_t need = 0, big_mean = 0;
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
           const int r = r0 + i;
@@ -854,11 +879,23 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
                 act[i] = true;  // inversion search: its single uniform comes from the group's blocks
                 need |= 1u << i;
               } else {
-                plis_stream st = plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_react(r));
-                kk[i] = RT<Real>::count(RT<Real>::poisson(&st, lam[i]));
+                big_mean |= 1u << i;  // PTRS below, one sampler for the group
               }
             }
           }
+        }
+        while (big_mean) {  // draws with means >= 10, one at a time through a single inlined PTRS
+          const int i = __ffs(big_mean) - 1;
+          big_mean &= big_mean - 1u;
+          Real li = lam[0];
+#pragma unroll
+          for (int j = 1; j < 4; ++j)
+            if (i == j) li = lam[j];
+          plis_stream st = plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_react(r0 + i));
+          const long long kv = RT<Real>::count(RT<Real>::poisson(&st, li));
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if (i == j) kk[j] = kv;
         }
         if (need) {
           const plis_stream g =
@@ -901,7 +938,7 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
           if (k > 0) {
             if (box.acc) atomicAdd_block(&box.acc[s * box.size + own + box_offset(box, dir)], (int)k);
             else atomicAdd(&Xt[(size_t)s * m.Npad + b], (int)k);
-            if (mode == 1 && flag[b] == F_SSA_FF) flag[b] = F_SSA;
+            if (mode == 1 && !L.ff_free && flag[b] == F_SSA_FF) flag[b] = F_SSA;
             if (LOG) ev_put(A.b.ev, L.t, step, attempt, c, b, k, s, PLIS_EVENT_LEAP_DIFFUSION);
           }
           out += k;
@@ -932,7 +969,7 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
         dl.add(s, -out);
         ev += out;
       }
-      if (mark) {  // leap.cu:54-56: every receiver leaves fast-forward
+      if (mark && !L.ff_free) {  // leap.cu:54-56: every receiver leaves fast-forward
         auto leave_ff = [&](uint32_t b, int) {
           if (flag[b] == F_SSA_FF) flag[b] = F_SSA;
         };
@@ -1001,6 +1038,7 @@ __global__ void __launch_bounds__(256, PLIS_LEAP_MIN_BLOCKS) k_leap(KArgs A) {
   L.step = K->step + 1;
   L.attempt = K->attempt;
   L.t = K->t;
+  L.ff_free = K->ff_free != 0;
   const Real tl = (Real)K->tau_leap;
   Box box;
   box.acc = A.g.staged ? s_box : nullptr;
@@ -1302,9 +1340,9 @@ __device__ __forceinline__ ClassifyCtx classify_ctx(const KArgs& A, const Ctrl* 
 }
 
 // One thread's subvolume of one brick: negativity check, zeroing of the next target, classification.
-template <typename Real, int MAXS, bool WALK = true>
+template <typename Real, int MAXS, bool WALK = true, bool CACHE = false>
 __device__ __forceinline__ void classify_tile(const KArgs& A, uint32_t tile, const ClassifyCtx& C, double& tn,
-                                              long long& ti, int& fl, int& bad, bool& valid) {
+                                              long long& ti, int& fl, int& bad, bool& valid, Real* pc = nullptr) {
   const DevModel& m = A.m;
   Cell cl;
   valid = cell_of(A, tile, cl);
@@ -1325,7 +1363,8 @@ __device__ __forceinline__ void classify_tile(const KArgs& A, uint32_t tile, con
   Nbr q;
   if constexpr (WALK) nbr_lite(m, cl, q);
   else nbr_info(m, cl, q);
-  classify_cell<Real, WALK>(A, c, q, x, C.Xe, C.tau_cur[c], C.flag_cur[c], C.step, C.attempt, C.ff, tn, fl);
+  classify_cell<Real, WALK, CACHE>(A, c, q, x, C.Xe, C.tau_cur[c], C.flag_cur[c], C.step, C.attempt, C.ff, tn, fl,
+                                   CACHE ? pc + threadIdx.x : nullptr, blockDim.x);
   C.tau_new[c] = tn;
   C.flag_new[c] = (uint8_t)fl;
   ti = c;
@@ -1334,11 +1373,12 @@ __device__ __forceinline__ void classify_tile(const KArgs& A, uint32_t tile, con
 // CTA reduction of one brick into slot `slot` (min tau with arg-min, #LEAP_CR, negative flag), then
 // the count of finished bricks; true in the CTA that finished last of `nslots`.
 __device__ __forceinline__ bool classify_slot(const KArgs& A, Ctrl* K, uint32_t slot, uint32_t nslots, double tn,
-                                              long long ti, bool is_cr, int bad) {
+                                              long long ti, bool is_cr, int bad, bool is_ff) {
   __shared__ double s_t[32];
   __shared__ long long s_i[32];
   __shared__ bool s_last;
   const int ncr = __syncthreads_count(is_cr);
+  const int nff = __syncthreads_count(is_ff);
   const int nbad = __syncthreads_or(bad);
   warp_min_pair(tn, ti);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -1351,7 +1391,7 @@ __device__ __forceinline__ bool classify_slot(const KArgs& A, Ctrl* K, uint32_t 
     for (int w = 1; w < nw; ++w) min_pair(bt, bi, s_t[w], s_i[w]);
     A.b.slot_tau[slot] = bt;
     A.b.slot_idx[slot] = bi;
-    A.b.slot_cr[slot] = (uint32_t)ncr;
+    A.b.slot_cr[slot] = (uint32_t)ncr | ((uint32_t)nff << 16);  // #LEAP_CR | #SSA_FF << 16 (<= 1024 each)
     A.b.slot_bad[slot] = nbad ? 1u : 0u;
     __threadfence();
     const uint32_t prev = atomicAdd(&K->blocks_done, 1u);
@@ -1367,6 +1407,7 @@ __device__ __forceinline__ void classify_control(const KArgs& A, Ctrl* K, uint32
   __shared__ double s_t[32];
   __shared__ long long s_i[32];
   __shared__ unsigned long long s_cr[32];
+  __shared__ unsigned long long s_ff[32];
   __shared__ uint32_t s_bad[32];
   __shared__ double s_p[32];
   __threadfence();
@@ -1375,32 +1416,37 @@ __device__ __forceinline__ void classify_control(const KArgs& A, Ctrl* K, uint32
   const uint8_t* flag_new = A.b.flag[tf ^ 1u];
   double gt = PLIS_INF_D;
   long long gi = 0x7FFFFFFFFFFFFFFFll;
-  unsigned long long gcr = 0;
+  unsigned long long gcr = 0, gff = 0;
   uint32_t gbad = 0;
   double gp = PLIS_INF_D;  // learned classification: min of the plain taus
   const double* sp = A.b.slot_tau_plain;
   for (uint32_t b = threadIdx.x; b < nslots; b += blockDim.x) {
     min_pair(gt, gi, __ldcg(&A.b.slot_tau[b]), __ldcg(&A.b.slot_idx[b]));
-    gcr += __ldcg(&A.b.slot_cr[b]);
+    const uint32_t sc = __ldcg(&A.b.slot_cr[b]);
+    gcr += sc & 0xFFFFu;
+    gff += sc >> 16;
     gbad |= __ldcg(&A.b.slot_bad[b]);
     if (sp) gp = fmin(gp, __ldcg(&sp[b]));
   }
   warp_min_pair(gt, gi);
   gcr = (unsigned long long)warp_sum((long long)gcr);
+  gff = (unsigned long long)warp_sum((long long)gff);
   gbad = __reduce_or_sync(0xffffffffu, gbad);
   if (sp) gp = warp_min_d(gp);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  if (lane == 0) { s_t[wid] = gt; s_i[wid] = gi; s_cr[wid] = gcr; s_bad[wid] = gbad; s_p[wid] = gp; }
+  if (lane == 0) { s_t[wid] = gt; s_i[wid] = gi; s_cr[wid] = gcr; s_ff[wid] = gff; s_bad[wid] = gbad; s_p[wid] = gp; }
   __syncthreads();
   if (wid == 0) {
     const int nw = (blockDim.x + 31) >> 5;
     gt = lane < nw ? s_t[lane] : PLIS_INF_D;
     gi = lane < nw ? s_i[lane] : 0x7FFFFFFFFFFFFFFFll;
     gcr = lane < nw ? s_cr[lane] : 0ull;
+    gff = lane < nw ? s_ff[lane] : 0ull;
     gbad = lane < nw ? s_bad[lane] : 0u;
     gp = lane < nw ? s_p[lane] : PLIS_INF_D;
     warp_min_pair(gt, gi);
     gcr = (unsigned long long)warp_sum((long long)gcr);
+    gff = (unsigned long long)warp_sum((long long)gff);
     gbad = __reduce_or_sync(0xffffffffu, gbad);
     if (sp) gp = warp_min_d(gp);
   }
@@ -1415,6 +1461,7 @@ __device__ __forceinline__ void classify_control(const KArgs& A, Ctrl* K, uint32
       K->tau_min_plain = gp;
       K->argmin = gi;
       K->n_leap_cr = (uint32_t)gcr;
+      K->ff_free = gff == 0 ? 1u : 0u;
       K->argmin_flag = gi >= 0 ? __ldcg(&flag_new[gi]) : F_SSA_FF;
       K->tf = tf ^ 1u;
       K->phase = 1;
@@ -1449,19 +1496,21 @@ __device__ __forceinline__ void classify_control(const KArgs& A, Ctrl* K, uint32
       K->tau_min_plain = gp;
       K->argmin = gi;
       K->n_leap_cr = (uint32_t)gcr;
+      K->ff_free = gff == 0 ? 1u : 0u;
       K->argmin_flag = gi >= 0 ? __ldcg(&flag_new[gi]) : F_SSA_FF;
       prepare_step(K, mode);
     }
   }
 }
 
-template <typename Real, int MAXS>
 // 64 registers, 4 CTAs per SM: the classification is bound by load latency and needs the warps
 // (with the compiler's own choice of 80-88 registers it runs 12-60 % slower).
 #ifndef PLIS_CLASSIFY_MIN_BLOCKS
 #define PLIS_CLASSIFY_MIN_BLOCKS 4
 #endif
+template <typename Real, int MAXS, bool CACHE>
 __global__ void __launch_bounds__(256, PLIS_CLASSIFY_MIN_BLOCKS) k_classify(KArgs A) {
+  extern __shared__ __align__(16) unsigned char s_prop[];  // CACHE: R x blockDim propensities
   pdl_entry();
   Ctrl* K = A.b.ctrl;
   if (K->done) return;
@@ -1470,8 +1519,8 @@ __global__ void __launch_bounds__(256, PLIS_CLASSIFY_MIN_BLOCKS) k_classify(KArg
   long long ti;
   int fl, bad;
   bool valid;
-  classify_tile<Real, MAXS>(A, blockIdx.x, C, tn, ti, fl, bad, valid);
-  if (classify_slot(A, K, blockIdx.x, gridDim.x, tn, ti, valid && fl == F_LEAP_CR, bad))
+  classify_tile<Real, MAXS, true, CACHE>(A, blockIdx.x, C, tn, ti, fl, bad, valid, reinterpret_cast<Real*>(s_prop));
+  if (classify_slot(A, K, blockIdx.x, gridDim.x, tn, ti, valid && fl == F_LEAP_CR, bad, valid && fl == F_SSA_FF))
     classify_control(A, K, gridDim.x);
 }
 
@@ -1499,7 +1548,14 @@ struct KernelSet {
     if (a.b.ev.rec) launch_pdl(k_exact<Real, MAXS, true>, g, b, 0, s, a);
     else launch_pdl(k_exact<Real, MAXS, false>, g, b, 0, s, a);
   }
-  static void classify(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) { launch_pdl(k_classify<Real, MAXS>, g, b, 0, s, a); }
+  static void classify(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) {
+    // the cache pays once the grid fills the GPU; on a grid of a few CTAs its extra pass only
+    // lengthens each thread's chain (measured: 57 -> 62 us per step on 1,000 subvolumes)
+    if (a.m.R <= (uint32_t)kPropCache && g.x >= 148u)
+      launch_pdl(k_classify<Real, MAXS, true>, g, b, (size_t)a.m.R * b.x * sizeof(Real), s, a);
+    else
+      launch_pdl(k_classify<Real, MAXS, false>, g, b, 0, s, a);
+  }
 };
 
 template <typename Real>

@@ -162,7 +162,8 @@ __global__ void __launch_bounds__(256) k_learned_post(KArgs A) {
     ti = c;
   }
   const int bad = threadIdx.x == 0 ? (int)A.b.slot_bad[blockIdx.x] : 0;
-  if (classify_slot_learned(A, K, blockIdx.x, gridDim.x, tn, ti, tp, valid && fl == F_LEAP_CR, bad))
+  if (classify_slot_learned(A, K, blockIdx.x, gridDim.x, tn, ti, tp, valid && fl == F_LEAP_CR, bad,
+                            valid && fl == F_SSA_FF))
     classify_control(A, K, gridDim.x);
 }
 

@@ -136,12 +136,14 @@ __device__ __forceinline__ void normalise(const LearnedParams* __restrict__ P, f
 // classification with proposals
 // ------------------------------------------------------------------------------------------------
 __device__ __forceinline__ bool classify_slot_learned(const KArgs& A, Ctrl* K, uint32_t slot, uint32_t nslots,
-                                                      double tn, long long ti, double tp, bool is_cr, int bad) {
+                                                      double tn, long long ti, double tp, bool is_cr, int bad,
+                                                      bool is_ff) {
   __shared__ double s_t[32];
   __shared__ long long s_i[32];
   __shared__ double s_p[32];
   __shared__ bool s_last;
   const int ncr = __syncthreads_count(is_cr);
+  const int nff = __syncthreads_count(is_ff);
   const int nbad = __syncthreads_or(bad);
   warp_min_pair(tn, ti);
   tp = warp_min_d(tp);
@@ -159,7 +161,7 @@ __device__ __forceinline__ bool classify_slot_learned(const KArgs& A, Ctrl* K, u
     A.b.slot_tau[slot] = bt;
     A.b.slot_idx[slot] = bi;
     A.b.slot_tau_plain[slot] = bp;
-    A.b.slot_cr[slot] = (uint32_t)ncr;
+    A.b.slot_cr[slot] = (uint32_t)ncr | ((uint32_t)nff << 16);  // #LEAP_CR | #SSA_FF << 16
     A.b.slot_bad[slot] = nbad ? 1u : 0u;
     __threadfence();
     const uint32_t prev = atomicAdd(&K->blocks_done, 1u);
@@ -227,7 +229,7 @@ __device__ __forceinline__ bool learned_classify_tile(const KArgs& A, Ctrl* K, c
     C.flag_new[c] = (uint8_t)fl;
     ti = c;
   }
-  return classify_slot_learned(A, K, tile, nslots, tn, ti, tp, valid && fl == F_LEAP_CR, bad);
+  return classify_slot_learned(A, K, tile, nslots, tn, ti, tp, valid && fl == F_LEAP_CR, bad, valid && fl == F_SSA_FF);
 }
 
 }  // namespace plis
