@@ -153,11 +153,35 @@ inline void geo_divisors(Geo& g) {
   g.dnty = fastdiv_make(g.nty ? g.nty : 1);
 }
 
+// The tables of a small model (at most kSmallR reactions and kSmallS species, one set of rate
+// constants for every subvolume), held in the kernel arguments.  The step kernels built for small
+// models read them from the constant bank the arguments live in, with compile-time offsets once
+// their reaction and species loops are unrolled, instead of loading DevModel's tables from global
+// memory for every subvolume.  The values are those of the DevModel tables (same propensities, same
+// criticality, same order of summation).
+constexpr int kSmallR = 4, kSmallS = 4;
+struct SmallModel {
+  uint32_t on;                   // 1: the model fits and the tables below are filled
+  uint8_t nreac[kSmallR];        // distinct reactant species of reaction r
+  uint8_t rs[kSmallR][3];        // reactant species, increasing
+  uint8_t rm[kSmallR][3];        // their multiplicities (1..3)
+  int8_t rnu[kSmallR][3];        // their net change (the reference's criticality test)
+  int8_t nu[kSmallR][kSmallS];   // net change of every species (0 for species >= S and reactions >= R)
+  uint8_t hor[kSmallS], hmult[kSmallS];
+  uint8_t rmask[kSmallS];        // bit r: species s is a reactant of reaction r
+  double inv_denom[kSmallR];
+  double rate_d[kSmallR];
+  float rate_f[kSmallR];
+  double drate_d[kSmallS];
+  float drate_f[kSmallS];
+};
+
 struct KArgs {
   DevModel m;
   DevBufs b;
   DevOpts o;
   Geo g;
+  SmallModel sm;
 };
 
 }  // namespace plis

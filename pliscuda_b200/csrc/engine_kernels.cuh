@@ -500,6 +500,60 @@ __device__ __forceinline__ Real gfun(int hor, int hmult, int32_t x) {
   }
 }
 
+// Small models (SmallModel in the kernel arguments): the same propensity, criticality and rate
+// constants as prop / crit_ref / crit_fix / drate above, from the argument tables.  The product of
+// falling factorials is formed in the same order (reactant species increasing, x, x-1, x-2).
+template <typename Real> __device__ __forceinline__ Real sm_rate(const SmallModel& t, int r);
+template <> __device__ __forceinline__ double sm_rate<double>(const SmallModel& t, int r) { return t.rate_d[r]; }
+template <> __device__ __forceinline__ float sm_rate<float>(const SmallModel& t, int r) { return t.rate_f[r]; }
+template <typename Real> __device__ __forceinline__ Real sm_drate(const SmallModel& t, int s);
+template <> __device__ __forceinline__ double sm_drate<double>(const SmallModel& t, int s) { return t.drate_d[s]; }
+template <> __device__ __forceinline__ float sm_drate<float>(const SmallModel& t, int s) { return t.drate_f[s]; }
+
+template <typename Real, int MAXS>
+__device__ __forceinline__ Real prop_sm(const SmallModel& t, const Counts<MAXS>& x, int r) {
+  Real prod = (Real)1;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    if (i < t.nreac[r]) {
+      const Real xs = (Real)x.get(t.rs[r][i]);
+      const int mu = t.rm[r][i];
+      prod = prod * xs;
+      if (mu > 1) prod = prod * (xs - (Real)1);
+      if (mu > 2) prod = prod * (xs - (Real)2);
+    }
+  }
+  return (sm_rate<Real>(t, r) * prod) * (Real)t.inv_denom[r];
+}
+
+template <int MAXS>
+__device__ __forceinline__ bool crit_ref_sm(const SmallModel& t, const Counts<MAXS>& x, int r, int nc) {
+  const int lim = t.nreac[r] < 2 ? t.nreac[r] : 2;
+  bool crit = false;
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    if (i < lim) {
+      const int32_t xs = x.get(t.rs[r][i]);
+      if (xs == 0) return true;
+      const int nu = t.rnu[r][i];
+      if (nu < 0 && (long long)(-nu) * nc > xs) crit = true;
+    }
+  }
+  return crit;
+}
+
+template <typename Real, int MAXS>
+__device__ __forceinline__ bool crit_fix_sm(const SmallModel& t, const Counts<MAXS>& x, int r, Real a, int nc) {
+  if (!(a > (Real)0)) return false;
+  bool crit = false;
+#pragma unroll
+  for (int s = 0; s < MAXS; ++s) {
+    const int nu = t.nu[r][s];
+    if (nu < 0 && x.v[s] < (long long)(-nu) * nc) crit = true;
+  }
+  return crit;
+}
+
 template <int MAXS>
 __device__ __forceinline__ void load_counts(const DevModel& m, const int32_t* X, uint32_t c, Counts<MAXS>& x) {
 #pragma unroll
@@ -536,6 +590,10 @@ __device__ __forceinline__ bool classify_ff(int mode, double tau_cur, uint8_t fl
 // flags into a bit mask, and the loops below read them back; without it each loop evaluates them
 // again (the batched and learned kernels, and models with more reactions).  Same values either way.
 constexpr int kPropCache = 20;  // 20 x 256 threads x 8 B = 40 KB: under the 48 KB a launch gets without opting in
+template <typename Real, bool WALK = true, int MAXS>
+__device__ __forceinline__ void cell_tau_parts_sm(const KArgs& A, const Nbr& q, const Counts<MAXS>& x,
+                                                  const int32_t* Xe, Real& tau_ncr_out, Real& rate_cr_out);
+
 template <typename Real, bool WALK = true, bool CACHE = false, int MAXS>
 __device__ __forceinline__ void cell_tau_parts(const KArgs& A, uint32_t c, const Nbr& q, const Counts<MAXS>& x,
                                                const int32_t* Xe, Real& tau_ncr_out, Real& rate_cr_out,
@@ -653,6 +711,120 @@ __device__ __forceinline__ void cell_tau_parts(const KArgs& A, uint32_t c, const
   rate_cr_out = (rsum == (Real)0 && dsum == (Real)0) ? (Real)0 : rsum + dsum;
 }
 
+// cell_tau_parts for a small model (SmallModel in the kernel arguments): the same quantities in the
+// same order, with the species and reaction loops unrolled to the tables' compile-time sizes.
+template <typename Real, bool WALK, int MAXS>
+__device__ __forceinline__ void cell_tau_parts_sm(const KArgs& A, const Nbr& q, const Counts<MAXS>& x,
+                                                  const int32_t* Xe, Real& tau_ncr_out, Real& rate_cr_out) {
+  static_assert(MAXS <= kSmallS, "small-model tables hold kSmallS species");
+  const DevModel& m = A.m;
+  const SmallModel& t = A.sm;
+  const int mode = A.o.mode;
+  const int nc = A.o.nc;
+  const int n = q.n;
+  const int S = (int)m.S, R = (int)m.R;
+  Real tau_ncr = RT<Real>::inf();
+#pragma unroll
+  for (int s = 0; s < MAXS; ++s) {
+    if (s >= S) continue;
+    const int32_t xs = x.v[s];
+    bool include;
+    if (mode == 0) {
+      bool skip_r = false;
+#pragma unroll
+      for (int r = 0; r < kSmallR; ++r)
+        if ((t.rmask[s] >> r) & 1u) skip_r = skip_r || crit_ref_sm(t, x, r, nc);
+      include = !(skip_r && xs < nc);  // tau.cu:165
+    } else {
+      include = false;
+#pragma unroll
+      for (int r = 0; r < kSmallR; ++r)
+        if ((t.rmask[s] >> r) & 1u) {
+          const Real a = prop_sm<Real>(t, x, r);
+          include = include || ((a > (Real)0) && !crit_fix_sm(t, x, r, a, nc));
+        }
+      if (!include && xs >= nc && sm_drate<Real>(t, s) > (Real)0 && n > 0) include = true;
+    }
+    if (!include) continue;
+    const Real g = gfun<Real>(t.hor[s], t.hmult[s], xs);
+    Real mu = (Real)0, s2 = (Real)0;
+#pragma unroll
+    for (int r = 0; r < kSmallR; ++r) {
+      const int nu = t.nu[r][s];  // 0 for reactions >= R
+      if (nu == 0) continue;
+      const Real a = prop_sm<Real>(t, x, r);
+      const bool ncrit = (mode == 0) ? !crit_ref_sm(t, x, r, nc) : ((a > (Real)0) && !crit_fix_sm(t, x, r, a, nc));
+      if (!ncrit) continue;
+      mu = mu + (Real)nu * a;
+      s2 = s2 + (Real)(nu * nu) * a;
+    }
+    const Real dr = sm_drate<Real>(t, s);
+    const Real d = dr * (Real)xs;
+    if (mode == 0) {
+      if (xs >= nc) { mu = mu + d; s2 = s2 + d; }
+      auto term = [&](uint32_t b, int nn) {
+        const Real db = dr * (Real)Xe[(size_t)s * m.Npad + b];
+        const Real qd = db / (Real)nn;
+        mu = mu - qd;
+        s2 = s2 + qd;
+      };
+      if constexpr (WALK) for_each_nbr(m, q, term);
+      else for (int j = 0; j < n; ++j) term(q.nb[j], (int)q.nn[j]);
+    } else {
+      if (xs >= nc && n > 0) {
+        const Real dout = (Real)n * d;
+        mu = mu - dout;
+        s2 = s2 + dout;
+      }
+      auto term = [&](uint32_t b, int) {
+        const int32_t xb = Xe[(size_t)s * m.Npad + b];
+        if (xb >= nc) {
+          const Real qd = dr * (Real)xb;
+          mu = mu + qd;
+          s2 = s2 + qd;
+        }
+      };
+      if constexpr (WALK) for_each_nbr(m, q, term);
+      else for (int j = 0; j < n; ++j) term(q.nb[j], (int)q.nn[j]);
+    }
+    Real mm = ((Real)A.o.eps * (Real)xs) / g;
+    if (!(mm > (Real)1)) mm = (Real)1;
+    const Real t1 = mm / fabs(mu);
+    const Real t2 = (mm * mm) / s2;
+    const Real ts = t1 < t2 ? t1 : t2;
+    if (ts < tau_ncr) tau_ncr = ts;
+  }
+  Real rsum = (Real)0, dsum = (Real)0;
+  const bool ncr_inf = plis_isinf_d((double)tau_ncr);
+  if (mode == 0 || !ncr_inf) {
+#pragma unroll
+    for (int r = 0; r < kSmallR; ++r) {
+      if (r >= R) continue;
+      const Real a = prop_sm<Real>(t, x, r);
+      const bool cr = (mode == 0) ? crit_ref_sm(t, x, r, nc) : crit_fix_sm(t, x, r, a, nc);
+      if (cr) rsum = rsum + a;
+    }
+#pragma unroll
+    for (int s = 0; s < MAXS; ++s) {
+      if (s >= S) continue;
+      const int32_t xs = x.v[s];
+      if (xs < nc) {
+        const Real d = sm_drate<Real>(t, s) * (Real)xs;
+        dsum = dsum + (mode == 0 ? d : (Real)n * d);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < kSmallR; ++r)
+      if (r < R) rsum = rsum + prop_sm<Real>(t, x, r);
+#pragma unroll
+    for (int s = 0; s < MAXS; ++s)
+      if (s < S) dsum = dsum + (Real)n * (sm_drate<Real>(t, s) * (Real)x.v[s]);
+  }
+  tau_ncr_out = tau_ncr;
+  rate_cr_out = (rsum == (Real)0 && dsum == (Real)0) ? (Real)0 : rsum + dsum;
+}
+
 // tau_cr: exponential time of the critical rate (inf when it is zero), tau.cu:193.
 template <typename Real>
 __device__ __forceinline__ double cell_tau_cr(const KArgs& A, uint32_t c, uint64_t step, uint32_t attempt, Real rate) {
@@ -678,13 +850,14 @@ __device__ __forceinline__ void cell_decide(double tn, double tcr, double& tau_o
 // ------------------------------------------------------------------------------------------------
 // classification of one subvolume (compute_taus, tau.cu:197-252)
 // ------------------------------------------------------------------------------------------------
-template <typename Real, bool WALK = true, bool CACHE = false, int MAXS>
+template <typename Real, bool WALK = true, bool CACHE = false, bool SM = false, int MAXS>
 __device__ void classify_cell(const KArgs& A, uint32_t c, const Nbr& q, const Counts<MAXS>& x, const int32_t* Xe,
                               double tau_cur, uint8_t flag_cur, uint64_t step, uint32_t attempt,
                               double ff, double& tau_out, int& flag_out, Real* pc = nullptr, uint32_t stride = 0) {
   if (classify_ff(A.o.mode, tau_cur, flag_cur, step, ff, tau_out, flag_out)) return;
   Real tau_ncr, rate;
-  cell_tau_parts<Real, WALK, CACHE>(A, c, q, x, Xe, tau_ncr, rate, pc, stride);
+  if constexpr (SM) cell_tau_parts_sm<Real, WALK>(A, q, x, Xe, tau_ncr, rate);
+  else cell_tau_parts<Real, WALK, CACHE>(A, c, q, x, Xe, tau_ncr, rate, pc, stride);
   const double tcr = cell_tau_cr<Real>(A, c, step, attempt, rate);
   cell_decide((double)tau_ncr, tcr, tau_out, flag_out);
 }
@@ -824,9 +997,12 @@ struct LeapCtx {
 
 // Leap of one brick (or one 1-D block of a table topology) by the whole CTA; returns this thread's
 // events and guard flag.  leap_step, leap.cu:3-65.
-template <typename Real, int MAXS, bool LOG, bool WALK = true>
+// SM: a small model whose tables are in A.sm (SmallModel): the reaction and species loops run to
+// the tables' compile-time sizes, so every table read is a constant-bank operand.
+template <typename Real, int MAXS, bool LOG, bool WALK = true, bool SM = false>
 __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const LeapCtx& L, Real tl, const Box& box,
                                           long long& ev, int& big) {
+  static_assert(!SM || MAXS <= kSmallS, "small-model tables hold kSmallS species");
   const DevModel& m = A.m;
   const int mode = A.o.mode, nc = A.o.nc;
   const int32_t* Xc = L.Xc;
@@ -855,9 +1031,9 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
     for (int s = 0; s < MAXS; ++s) dl.v[s] = 0;
     const uint8_t f = flag[c];
     if (f == F_LEAP_CR || f == F_LEAP_NOCR) {  // leap.cu:9-10
-      const int comp = comp_of(m, c);
+      const int comp = SM ? 0 : comp_of(m, c);
       const int S = (int)m.S, R = (int)m.R;
-      for (int r0 = 0; r0 < R; r0 += 4) {
+      auto reaction_group = [&](const int r0) {
         // reactions r0..r0+3: means >= 10 go through PTRS one by one, the rest in lockstep
         Real u[4], lam[4];
         bool act[4];
@@ -871,8 +1047,15 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
           u[i] = (Real)0;
           kk[i] = 0;
           if (r < R) {
-            const Real a = prop<Real>(m, x, r, comp);
-            const bool fire = (mode == 0) ? !crit_ref(m, x, r, nc) : ((a > (Real)0) && !crit_fix(m, x, r, a, nc));
+            Real a;
+            bool fire;
+            if constexpr (SM) {
+              a = prop_sm<Real>(A.sm, x, r);
+              fire = (mode == 0) ? !crit_ref_sm(A.sm, x, r, nc) : ((a > (Real)0) && !crit_fix_sm(A.sm, x, r, a, nc));
+            } else {
+              a = prop<Real>(m, x, r, comp);
+              fire = (mode == 0) ? !crit_ref(m, x, r, nc) : ((a > (Real)0) && !crit_fix(m, x, r, a, nc));
+            }
             lam[i] = fire ? tl * a : (Real)0;
             if (lam[i] > (Real)0) {
               if (lam[i] < (Real)10) {
@@ -911,24 +1094,46 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
           const long long k = act[i] ? ks[i] : kk[i];
           ev += k;
           if (LOG && k > 0) ev_put(A.b.ev, L.t, step, attempt, c, c, k, r, PLIS_EVENT_LEAP_REACTION);
-          const int nn = m.n_net[r];
-          for (int q = 0; q < nn; ++q) {
-            const long long v = k * (long long)m.net_nu[r * 8 + q];
-            if (v >= kBigDraw || v <= -kBigDraw) big = 1;
-            dl.add(m.net_s[r * 8 + q], v);
+          if constexpr (SM) {
+#pragma unroll
+            for (int sp = 0; sp < MAXS; ++sp) {
+              const int nu = A.sm.nu[r][sp];
+              if (nu != 0) {
+                const long long v = k * (long long)nu;
+                if (v >= kBigDraw || v <= -kBigDraw) big = 1;
+                dl.v[sp] += v;
+              }
+            }
+          } else {
+            const int nn = m.n_net[r];
+            for (int q = 0; q < nn; ++q) {
+              const long long v = k * (long long)m.net_nu[r * 8 + q];
+              if (v >= kBigDraw || v <= -kBigDraw) big = 1;
+              dl.add(m.net_s[r * 8 + q], v);
+            }
           }
         }
+      };
+      if constexpr (SM) {
+#pragma unroll
+        for (int r0 = 0; r0 < kSmallR; r0 += 4)
+          if (r0 < R) reaction_group(r0);
+      } else {
+        for (int r0 = 0; r0 < R; r0 += 4) reaction_group(r0);
       }
       Nbr q;
       if (WALK && m.lattice) nbr_scalars(m, cl, q);  // walked by direction below: no slot arrays
       else nbr_info(m, cl, q);
       const int n = q.n;
       bool mark = false;
-      for (int s = 0; s < S; ++s) {
+      auto species_jumps = [&](const int s) {
         const int32_t xs = x.get(s);
-        if (xs < nc) continue;  // is_critical_diffusion, tau.cu:42-45
+        if (xs < nc) return;  // is_critical_diffusion, tau.cu:42-45
         if (mode == 0 && n > 0) mark = true;
-        const Real lam = tl * (drate<Real>(m, comp, s) * (Real)xs);
+        Real dr;
+        if constexpr (SM) dr = sm_drate<Real>(A.sm, s);
+        else dr = drate<Real>(m, comp, s);
+        const Real lam = tl * (dr * (Real)xs);
         const Real em = RT<Real>::emlam(lam);  // one exp for the n draws of this species
         int32_t kd[6];
         diffusion_draws<Real>(A, c, s, n, lam, em, step, attempt, kd);
@@ -968,6 +1173,13 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
         }
         dl.add(s, -out);
         ev += out;
+      };
+      if constexpr (SM) {
+#pragma unroll
+        for (int s = 0; s < MAXS; ++s)
+          if (s < S) species_jumps(s);
+      } else {
+        for (int s = 0; s < S; ++s) species_jumps(s);
       }
       if (mark && !L.ff_free) {  // leap.cu:54-56: every receiver leaves fast-forward
         auto leave_ff = [&](uint32_t b, int) {
@@ -1022,7 +1234,7 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
   }
 }
 
-template <typename Real, int MAXS, bool LOG>
+template <typename Real, int MAXS, bool LOG, bool SM>
 __global__ void __launch_bounds__(256, PLIS_LEAP_MIN_BLOCKS) k_leap(KArgs A) {
   pdl_entry();
   Ctrl* K = A.b.ctrl;
@@ -1049,7 +1261,7 @@ __global__ void __launch_bounds__(256, PLIS_LEAP_MIN_BLOCKS) k_leap(KArgs A) {
   __syncthreads();
   long long ev;
   int big;
-  leap_tile<Real, MAXS, LOG>(A, blockIdx.x, L, tl, box, ev, big);
+  leap_tile<Real, MAXS, LOG, true, SM>(A, blockIdx.x, L, tl, box, ev, big);
   // events and guard flags of the CTA
   ev = warp_sum(ev);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -1340,7 +1552,7 @@ __device__ __forceinline__ ClassifyCtx classify_ctx(const KArgs& A, const Ctrl* 
 }
 
 // One thread's subvolume of one brick: negativity check, zeroing of the next target, classification.
-template <typename Real, int MAXS, bool WALK = true, bool CACHE = false>
+template <typename Real, int MAXS, bool WALK = true, bool CACHE = false, bool SM = false>
 __device__ __forceinline__ void classify_tile(const KArgs& A, uint32_t tile, const ClassifyCtx& C, double& tn,
                                               long long& ti, int& fl, int& bad, bool& valid, Real* pc = nullptr) {
   const DevModel& m = A.m;
@@ -1363,8 +1575,8 @@ __device__ __forceinline__ void classify_tile(const KArgs& A, uint32_t tile, con
   Nbr q;
   if constexpr (WALK) nbr_lite(m, cl, q);
   else nbr_info(m, cl, q);
-  classify_cell<Real, WALK, CACHE>(A, c, q, x, C.Xe, C.tau_cur[c], C.flag_cur[c], C.step, C.attempt, C.ff, tn, fl,
-                                   CACHE ? pc + threadIdx.x : nullptr, blockDim.x);
+  classify_cell<Real, WALK, CACHE, SM>(A, c, q, x, C.Xe, C.tau_cur[c], C.flag_cur[c], C.step, C.attempt, C.ff, tn, fl,
+                                       CACHE ? pc + threadIdx.x : nullptr, blockDim.x);
   C.tau_new[c] = tn;
   C.flag_new[c] = (uint8_t)fl;
   ti = c;
@@ -1508,7 +1720,7 @@ __device__ __forceinline__ void classify_control(const KArgs& A, Ctrl* K, uint32
 #ifndef PLIS_CLASSIFY_MIN_BLOCKS
 #define PLIS_CLASSIFY_MIN_BLOCKS 4
 #endif
-template <typename Real, int MAXS, bool CACHE>
+template <typename Real, int MAXS, bool CACHE, bool SM>
 __global__ void __launch_bounds__(256, PLIS_CLASSIFY_MIN_BLOCKS) k_classify(KArgs A) {
   extern __shared__ __align__(16) unsigned char s_prop[];  // CACHE: R x blockDim propensities
   pdl_entry();
@@ -1519,7 +1731,7 @@ __global__ void __launch_bounds__(256, PLIS_CLASSIFY_MIN_BLOCKS) k_classify(KArg
   long long ti;
   int fl, bad;
   bool valid;
-  classify_tile<Real, MAXS, true, CACHE>(A, blockIdx.x, C, tn, ti, fl, bad, valid, reinterpret_cast<Real*>(s_prop));
+  classify_tile<Real, MAXS, true, CACHE, SM>(A, blockIdx.x, C, tn, ti, fl, bad, valid, reinterpret_cast<Real*>(s_prop));
   if (classify_slot(A, K, blockIdx.x, gridDim.x, tn, ti, valid && fl == F_LEAP_CR, bad, valid && fl == F_SSA_FF))
     classify_control(A, K, gridDim.x);
 }
@@ -1534,27 +1746,48 @@ __global__ void k_fill_tau(double* t, uint8_t* f, uint32_t n) {
 // kernel launchers of each (precision, species capacity)
 template <typename Real, int MAXS>
 struct KernelSet {
+  static constexpr bool kSmallOk = MAXS <= kSmallS;  // small-model kernels exist for these species counts
   // the event-log variants (LOG = true) only when the handle's log is on: the plain path carries no logging code
   static void leap(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) {
-    if (a.b.ev.rec) launch_pdl(k_leap<Real, MAXS, true>, g, b, a.g.box_bytes, s, a);
-    else launch_pdl(k_leap<Real, MAXS, false>, g, b, a.g.box_bytes, s, a);
+    if constexpr (kSmallOk) {
+      if (a.sm.on) {
+        if (a.b.ev.rec) launch_pdl(k_leap<Real, MAXS, true, true>, g, b, a.g.box_bytes, s, a);
+        else launch_pdl(k_leap<Real, MAXS, false, true>, g, b, a.g.box_bytes, s, a);
+        return;
+      }
+    }
+    if (a.b.ev.rec) launch_pdl(k_leap<Real, MAXS, true, false>, g, b, a.g.box_bytes, s, a);
+    else launch_pdl(k_leap<Real, MAXS, false, false>, g, b, a.g.box_bytes, s, a);
   }
   static cudaError_t leap_smem(int bytes) {
-    cudaError_t e = cudaFuncSetAttribute(k_leap<Real, MAXS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_leap<Real, MAXS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaError_t e = cudaFuncSetAttribute(k_leap<Real, MAXS, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_leap<Real, MAXS, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if constexpr (kSmallOk) {
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_leap<Real, MAXS, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_leap<Real, MAXS, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    }
+    return e;
   }
   static void exact(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) {
     if (a.b.ev.rec) launch_pdl(k_exact<Real, MAXS, true>, g, b, 0, s, a);
     else launch_pdl(k_exact<Real, MAXS, false>, g, b, 0, s, a);
   }
   static void classify(const KArgs& a, dim3 g, dim3 b, cudaStream_t s) {
+    if constexpr (kSmallOk) {
+      if (a.sm.on) {  // the small-model tables make a propensity cheap: no cache
+        launch_pdl(k_classify<Real, MAXS, false, true>, g, b, 0, s, a);
+        return;
+      }
+    }
     // the cache pays once the grid fills the GPU; on a grid of a few CTAs its extra pass only
     // lengthens each thread's chain (measured: 57 -> 62 us per step on 1,000 subvolumes)
     if (a.m.R <= (uint32_t)kPropCache && g.x >= 148u)
-      launch_pdl(k_classify<Real, MAXS, true>, g, b, (size_t)a.m.R * b.x * sizeof(Real), s, a);
+      launch_pdl(k_classify<Real, MAXS, true, false>, g, b, (size_t)a.m.R * b.x * sizeof(Real), s, a);
     else
-      launch_pdl(k_classify<Real, MAXS, false>, g, b, 0, s, a);
+      launch_pdl(k_classify<Real, MAXS, false, false>, g, b, 0, s, a);
   }
 };
 
