@@ -243,6 +243,54 @@ int plis_read_event_log(plis_handle* h, plis_event_record* out, uint64_t max_rec
 #define PLIS_NOALLOC_MAX_TAUS 2147483647u
 int plis_tau_argmin_noalloc(const double* d_tau, uint64_t n, double* d_min_tau, int64_t* d_argmin, void* stream);
 
+/* z-slab decomposition of one lattice over several ranks (one process or handle per slab; no
+ * counterpart in the reference, which runs one GPU, main.cpp:25-28).  A handle created for the whole
+ * model and given plis_slab_setup computes only the subvolumes of z-layers [z0, z1); z0 and z1 must be
+ * multiples of the brick's z extent, and the slabs of the ranks 0 .. world-1 must tile the lattice in
+ * rank order.  Arrays stay full size and indices global: random streams, neighbour counts and the
+ * arg-min tie rule are those of the single domain, so the slabs together follow the single-domain
+ * trajectory bit for bit.  The caller moves the data between phases (pliscuda_b200/slabs.py does it
+ * over torch.distributed or within one process):
+ *   PLIS_SLAB_CLASSIFY  classify the slab; its summary is in buffers.summary (call first, after
+ *                       plis_set_state, for the initial state; later after PLIS_SLAB_UNPACK)
+ *     -> gather every rank's summary into buffers.summary_all (rank order)
+ *   PLIS_SLAB_CONTROL   the step decision from summary_all (identical on every rank); the face flags
+ *                       are staged in send[0] (to the slab below) and send[1] (above)
+ *     -> send[0] to the slab below's recv[1], send[1] to the slab above's recv[0]
+ *   PLIS_SLAB_FLAGS     received face flags into the ghost layers
+ *   PLIS_SLAB_PREPARE   start a run to t_end / n_steps (what plis_run / plis_step do first)
+ * and, per attempt while not done (plis_get_stats stop_reason):
+ *   PLIS_SLAB_LEAP      leap, exact events and deltas of the slab; the ghost layers (molecules sent
+ *                       across the faces) staged in send[0..1], flag writes outside the slab in remote
+ *     -> exchange send/recv as above; gather every rank's remote into remote_all
+ *   PLIS_SLAB_MERGE     received molecules added into the face layers, flags merged; faces staged
+ *     -> exchange send/recv
+ *   PLIS_SLAB_UNPACK    received face layers into the ghost layers
+ *   PLIS_SLAB_CLASSIFY, gather, PLIS_SLAB_CONTROL, exchange, PLIS_SLAB_FLAGS as above.
+ * Every phase returns once its kernels have finished.  Lattice models only; learned proposals and
+ * the event log are not available on a slab. */
+#define PLIS_SLAB_CLASSIFY 0
+#define PLIS_SLAB_CONTROL 1
+#define PLIS_SLAB_FLAGS 2
+#define PLIS_SLAB_PREPARE 3
+#define PLIS_SLAB_LEAP 4
+#define PLIS_SLAB_MERGE 5
+#define PLIS_SLAB_UNPACK 6
+typedef struct plis_slab_buffers {
+  void* send[2];          /* device int32[stage_words]: to the slab below (0) / above (1) */
+  void* recv[2];          /* device int32[stage_words]: from the slab below (0) / above (1) */
+  uint64_t stage_words;   /* (species + 1) * X * Y */
+  void* summary;          /* device, summary_bytes: this rank's summary */
+  void* summary_all;      /* device, world * summary_bytes: every rank's, in rank order */
+  uint64_t summary_bytes;
+  void* remote;           /* device, remote_bytes: this rank's flag writes outside its slab */
+  void* remote_all;       /* device, world * remote_bytes */
+  uint64_t remote_bytes;
+} plis_slab_buffers;
+int plis_slab_setup(plis_handle* h, uint32_t z0, uint32_t z1, uint32_t world, uint32_t rank);
+int plis_slab_buffers_get(plis_handle* h, plis_slab_buffers* out);
+int plis_slab_phase(plis_handle* h, int phase, double t_end, uint64_t n_steps);
+
 /* Topology helpers (host only, no device needed).
  * plis_canonical_neighbours rewrites a 6-wide table so that each row lists its distinct non-self
  * neighbours first (lattice rows in the order -x,+x,-y,+y,-z,+z) followed by self padding; this is

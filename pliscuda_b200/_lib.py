@@ -54,6 +54,11 @@ class Stats(ctypes.Structure):
                 ("device_ms", f64), ("kernel_launches", u64)]
 
 
+class SlabBuffers(ctypes.Structure):
+    _fields_ = [("send", vp * 2), ("recv", vp * 2), ("stage_words", u64), ("summary", vp), ("summary_all", vp),
+                ("summary_bytes", u64), ("remote", vp), ("remote_all", vp), ("remote_bytes", u64)]
+
+
 class BatchDesc(ctypes.Structure):
     _fields_ = [("n_replicas", u32), ("n_species", u32), ("n_reactions", u32), ("reactants", vp), ("products", vp),
                 ("lattice", vp), ("reaction_rates", vp), ("diffusion_rates", vp), ("replica_ids", vp)]
@@ -113,6 +118,9 @@ def _load() -> ctypes.CDLL:
         "plis_get_state": (i32, [vp, vp]),
         "plis_set_time": (i32, [vp, f64]),
         "plis_set_state_at": (i32, [vp, vp, f64, u64]),
+        "plis_slab_setup": (i32, [vp, u32, u32, u32, u32]),
+        "plis_slab_buffers_get": (i32, [vp, vp]),
+        "plis_slab_phase": (i32, [vp, i32, f64, u64]),
         "plis_run": (i32, [vp, f64]),
         "plis_step": (i32, [vp, u64]),
         "plis_get_stats": (i32, [vp, P(Stats)]),

@@ -146,6 +146,27 @@ int plis_set_state_at(plis_handle* h, const uint32_t* counts, double time, uint6
   PLIS_GUARD_END
 }
 
+int plis_slab_setup(plis_handle* h, uint32_t z0, uint32_t z1, uint32_t world, uint32_t rank) {
+  PLIS_GUARD_BEGIN
+  if (!h) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return fail(h, h->eng.slab_setup(z0, z1, world, rank));
+  PLIS_GUARD_END
+}
+
+int plis_slab_buffers_get(plis_handle* h, plis_slab_buffers* out) {
+  PLIS_GUARD_BEGIN
+  if (!h || !out) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return fail(h, h->eng.slab_buffers(out));
+  PLIS_GUARD_END
+}
+
+int plis_slab_phase(plis_handle* h, int phase, double t_end, uint64_t n_steps) {
+  PLIS_GUARD_BEGIN
+  if (!h) { g_err = "null argument"; return PLIS_ERR_INVALID; }
+  return fail(h, h->eng.slab_phase(phase, t_end, n_steps));
+  PLIS_GUARD_END
+}
+
 int plis_get_state(plis_handle* h, uint32_t* counts) {
   PLIS_GUARD_BEGIN
   if (!h || !counts) { g_err = "null argument"; return PLIS_ERR_INVALID; }

@@ -253,7 +253,7 @@ int Engine::create(const Model& model, const plis_options& opt) {
 }
 
 void Engine::launch_classify() {
-  const dim3 gc(args_.g.nblocks), bc(args_.g.threads);
+  const dim3 gc(slab_blocks_ ? slab_blocks_ : args_.g.nblocks), bc(args_.g.threads);
   if (use_learned_) llaunch_.classify(args_, gc, bc, stream_);
   else launch_.classify(args_, gc, bc, stream_);
 }
@@ -522,6 +522,7 @@ int Engine::read_event_log(plis_event_record* out, uint64_t max_records, uint64_
 }
 
 int Engine::advance(double t_end, uint64_t n_steps) {
+  if (slab_blocks_) { err_ = "a z-slab advances through plis_slab_phase"; return PLIS_ERR_UNSUPPORTED; }
   PLIS_CU(cudaEventRecord(ev0_, stream_));
   k_prepare<<<1, 32, 0, stream_>>>(args_, t_end, (unsigned long long)n_steps);
   launches_ += 1;
@@ -575,6 +576,130 @@ int Engine::advance(double t_end, uint64_t n_steps) {
     err_ = h_ctrl_->status == PLIS_ERR_STUCK ? "too many consecutive rollbacks in one step" : "device step failed";
     return h_ctrl_->status;
   }
+  return PLIS_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// z-slab decomposition
+// ------------------------------------------------------------------------------------------------
+int Engine::slab_setup(uint32_t z0, uint32_t z1, uint32_t world, uint32_t rank) {
+  const DevModel& dm = args_.m;
+  const Geo& g = args_.g;
+  if (!dm.lattice) { err_ = "z-slabs need a lattice topology"; return PLIS_ERR_UNSUPPORTED; }
+  if (state_set_) { err_ = "plis_slab_setup comes before plis_set_state"; return PLIS_ERR_INVALID; }
+  if (slab_blocks_) { err_ = "this handle is already a slab"; return PLIS_ERR_INVALID; }
+  if (use_learned_ || args_.b.ev.rec || opt_.profile) {
+    err_ = "learned proposals, the event log and profiling are not available on a slab";
+    return PLIS_ERR_UNSUPPORTED;
+  }
+  if (world < 1 || rank >= world) { err_ = "rank must be below world"; return PLIS_ERR_INVALID; }
+  if (!(z0 < z1 && z1 <= dm.Z) || z0 % g.tz != 0 || (z1 % g.tz != 0 && z1 != dm.Z)) {
+    err_ = "a slab is whole bricks along z: z0 < z1 <= Z, both multiples of the brick's z extent (or z1 = Z)";
+    return PLIS_ERR_INVALID;
+  }
+  SlabArgs& L = args_.sl;
+  std::memset(&L, 0, sizeof L);
+  L.layer = dm.X * dm.Y;
+  L.lo = z0 * L.layer;
+  L.hi = z1 * L.layer;
+  L.has_lo = z0 > 0 ? 1u : 0u;
+  L.has_hi = z1 < dm.Z ? 1u : 0u;
+  L.world = world;
+  L.rank = rank;
+  L.brick0 = (z0 / g.tz) * g.ntx * g.nty;
+  slab_blocks_ = ((z1 - z0 + g.tz - 1) / g.tz) * g.ntx * g.nty;
+  slab_stage_ = (size_t)(dm.S + 1) * L.layer;
+  int rc;
+  if ((rc = dmalloc((void**)&L.summary, sizeof(SlabSummary)))) return rc;
+  if ((rc = dmalloc((void**)&L.all, (size_t)world * sizeof(SlabSummary)))) return rc;
+  if ((rc = dmalloc((void**)&L.remote, sizeof(SlabRemote)))) return rc;
+  if ((rc = dmalloc((void**)&L.remote_all, (size_t)world * sizeof(SlabRemote)))) return rc;
+  for (int i = 0; i < 2; ++i) {
+    if ((rc = dmalloc((void**)&L.send[i], slab_stage_ * 4))) return rc;
+    if ((rc = dmalloc((void**)&L.recv[i], slab_stage_ * 4))) return rc;
+    PLIS_CU(cudaMemset(L.send[i], 0, slab_stage_ * 4));
+    PLIS_CU(cudaMemset((void*)L.recv[i], 0, slab_stage_ * 4));
+  }
+  PLIS_CU(cudaMemset((void*)L.all, 0, (size_t)world * sizeof(SlabSummary)));
+  PLIS_CU(cudaMemset((void*)L.remote_all, 0, (size_t)world * sizeof(SlabRemote)));
+  L.on = 1;
+  if (graph_exec_) {  // the graph holds the kernel arguments by value
+    cudaGraphExecDestroy(graph_exec_);
+    graph_exec_ = nullptr;
+  }
+  return PLIS_OK;
+}
+
+int Engine::slab_buffers(plis_slab_buffers* out) {
+  if (!slab_blocks_) { err_ = "not a slab (plis_slab_setup)"; return PLIS_ERR_INVALID; }
+  const SlabArgs& L = args_.sl;
+  for (int i = 0; i < 2; ++i) {
+    out->send[i] = L.send[i];
+    out->recv[i] = (void*)L.recv[i];
+  }
+  out->stage_words = slab_stage_;
+  out->summary = L.summary;
+  out->summary_all = (void*)L.all;
+  out->summary_bytes = sizeof(SlabSummary);
+  out->remote = L.remote;
+  out->remote_all = (void*)L.remote_all;
+  out->remote_bytes = sizeof(SlabRemote);
+  return PLIS_OK;
+}
+
+int Engine::slab_phase(int phase, double t_end, uint64_t n_steps) {
+  if (!slab_blocks_) { err_ = "not a slab (plis_slab_setup)"; return PLIS_ERR_INVALID; }
+  if (!state_set_) { err_ = "no state set"; return PLIS_ERR_INVALID; }
+  const dim3 gc(slab_blocks_), bc(args_.g.threads);
+  const dim3 gx(exact_blocks_), bx(256);
+  const uint32_t lb = (args_.sl.layer + 255u) / 256u;
+  const dim3 gl(lb < 1024u ? lb : 1024u), bl(256);
+  PLIS_CU(cudaEventRecord(ev0_, stream_));
+  switch (phase) {
+    case PLIS_SLAB_CLASSIFY:
+      launch_classify();
+      launches_ += 1;
+      break;
+    case PLIS_SLAB_CONTROL:
+      k_slab_control<<<1, 32, 0, stream_>>>(args_);
+      k_slab_pack_flags<<<gl, bl, 0, stream_>>>(args_);
+      launches_ += 2;
+      break;
+    case PLIS_SLAB_FLAGS:
+      k_slab_unpack_flags<<<gl, bl, 0, stream_>>>(args_);
+      launches_ += 1;
+      break;
+    case PLIS_SLAB_PREPARE:
+      k_prepare<<<1, 32, 0, stream_>>>(args_, t_end, (unsigned long long)n_steps);
+      launches_ += 1;
+      break;
+    case PLIS_SLAB_LEAP:
+      PLIS_CU(cudaMemsetAsync(args_.sl.remote, 0, sizeof(SlabRemote), stream_));
+      launch_.leap(args_, gc, bc, stream_);
+      launch_.exact(args_, gx, bx, stream_);
+      if (opt_.mode == PLIS_MODE_REFERENCE) k_apply<<<gx, bx, 0, stream_>>>(args_);
+      k_slab_pack_ghosts<<<gl, bl, 0, stream_>>>(args_);
+      launches_ += opt_.mode == PLIS_MODE_REFERENCE ? 4 : 3;
+      break;
+    case PLIS_SLAB_MERGE:
+      k_slab_merge<<<gl, bl, 0, stream_>>>(args_);
+      k_slab_pack_faces<<<gl, bl, 0, stream_>>>(args_);
+      launches_ += 2;
+      break;
+    case PLIS_SLAB_UNPACK:
+      k_slab_unpack_ghosts<<<gl, bl, 0, stream_>>>(args_);
+      launches_ += 1;
+      break;
+    default:
+      err_ = "unknown slab phase";
+      return PLIS_ERR_INVALID;
+  }
+  PLIS_CU(cudaGetLastError());
+  PLIS_CU(cudaEventRecord(ev1_, stream_));
+  PLIS_CU(cudaEventSynchronize(ev1_));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ev0_, ev1_);
+  device_ms_ += ms;
   return PLIS_OK;
 }
 

@@ -176,12 +176,48 @@ struct SmallModel {
   float drate_f[kSmallS];
 };
 
+// z-slab decomposition: this handle computes the subvolumes of whole z-layers [z0, z1) of a lattice
+// whose other layers belong to other ranks.  Arrays stay full size and indices global, so random
+// streams, neighbour counts and the arg-min tie rule are those of a single domain; the kernels touch
+// only the slab, and the host exchanges the layers next to its faces (the ghost layers z0-1 and z1)
+// with the neighbouring slabs and gathers every slab's summary.
+constexpr int kSlabRemote = 64;  // flag writes of one attempt that land outside the slab and its ghosts
+struct SlabSummary {             // one rank's reduction of its slab's classification
+  double tau;                    // min tau over the slab
+  long long idx;                 // its subvolume (global index; first on ties), -1 if none
+  double tau_plain;
+  unsigned long long ncr, nff;   // subvolumes flagged LEAP_CR / SSA_FF
+  uint32_t bad;                  // a negative count in the slab
+  uint32_t leap_bad;             // a draw beyond the int32 guards in the slab's leap
+  uint32_t am_flag;              // flag of idx
+  uint32_t pad_;
+};
+struct SlabRemote {              // subvolumes outside the slab and its ghosts whose SSA_FF flag must turn SSA
+  uint32_t n;                    // entries written (may exceed kSlabRemote: then the attempt fails)
+  uint32_t cell[kSlabRemote];
+};
+struct SlabArgs {
+  uint32_t on;
+  uint32_t brick0;               // first brick of the slab (bricks are numbered x fastest, z slowest)
+  uint32_t lo, hi;               // owned subvolumes [lo, hi)
+  uint32_t layer;                // subvolumes of one z-layer (X * Y)
+  uint32_t has_lo, has_hi;       // a slab below / above
+  uint32_t world, rank;
+  SlabSummary* summary;          // [1] this rank's, written by the classification's last CTA
+  const SlabSummary* all;        // [world] gathered
+  SlabRemote* remote;            // [1] this rank's flag writes outside the slab and its ghosts
+  const SlabRemote* remote_all;  // [world] gathered
+  int32_t* send[2];              // [S][layer] counts then [layer] flags (as int32): 0 = to the slab below, 1 = above
+  const int32_t* recv[2];        // the same layout from the slab below / above
+};
+
 struct KArgs {
   DevModel m;
   DevBufs b;
   DevOpts o;
   Geo g;
   SmallModel sm;
+  SlabArgs sl;
 };
 
 }  // namespace plis

@@ -47,6 +47,10 @@ class Engine {
   int set_event_log(uint64_t capacity);
   int read_event_log(plis_event_record* out, uint64_t max_records, uint64_t* n_records, uint64_t* n_dropped,
                      bool clear);
+  // z-slab decomposition (plis_slab_*): this handle computes z-layers [z0, z1) of world slabs
+  int slab_setup(uint32_t z0, uint32_t z1, uint32_t world, uint32_t rank);
+  int slab_phase(int phase, double t_end, uint64_t n_steps);
+  int slab_buffers(plis_slab_buffers* out);
   int device() const { return opt_.device; }
   const std::string& error() const { return err_; }
   const Model& model() const { return model_; }
@@ -91,6 +95,8 @@ class Engine {
   float* d_ymlp_ = nullptr;
   EvRec* d_evrec_ = nullptr;
   unsigned long long* d_evhead_ = nullptr;
+  uint32_t slab_blocks_ = 0;  // bricks of this handle's z-slab (0: not a slab)
+  size_t slab_stage_ = 0;     // int32 words of one staging buffer
 };
 
 }  // namespace plis

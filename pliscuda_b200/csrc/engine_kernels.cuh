@@ -273,7 +273,7 @@ __device__ __forceinline__ uint32_t fdiv(uint32_t n, const FastDiv& f) {
 
 __device__ __forceinline__ bool cell_of(const KArgs& A, uint32_t block, Cell& cl) {
   if (A.m.lattice) {
-    const uint32_t b = block, t = threadIdx.x;
+    const uint32_t b = block + A.sl.brick0, t = threadIdx.x;  // brick0: first brick of a z-slab (0 otherwise)
     if (t >= A.g.tx * A.g.ty * A.g.tz) return false;  // block rounded up to whole warps
     const uint32_t br = fdiv(b, A.g.dntx), bx = b - br * A.g.ntx;
     const uint32_t bz = fdiv(br, A.g.dnty), by = br - bz * A.g.nty;
@@ -1347,7 +1347,12 @@ __device__ int critical_event_ref(const KArgs& A, uint32_t c, const Counts<MAXS>
   atomicAdd(&D[(size_t)spi * m.Npad + c], -1);
   atomicAdd(&D[(size_t)spi * m.Npad + target], 1);
   const uint32_t q = flat_table_entry(m, target);  // leap.cu:192-193
-  if (flag[q] == F_SSA_FF) flag[q] = F_SSA;
+  if (!A.sl.on || (q + A.sl.has_lo * A.sl.layer >= A.sl.lo && q < A.sl.hi + A.sl.has_hi * A.sl.layer)) {
+    if (flag[q] == F_SSA_FF) flag[q] = F_SSA;
+  } else {  // z-slab: another slab owns q; its owner applies the write after the gather
+    const uint32_t i = atomicAdd(&A.sl.remote->n, 1u);
+    if (i < (uint32_t)kSlabRemote) A.sl.remote->cell[i] = q;
+  }
   if (LOG) ev_put(A.b.ev, A.b.ctrl->t, step, attempt, c, target, 1, spi, PLIS_EVENT_CRITICAL_DIFFUSION);
   return 1;
 }
@@ -1473,15 +1478,16 @@ __global__ void __launch_bounds__(256) k_exact(KArgs A) {
   const uint64_t step = K->step + 1;
   const uint32_t attempt = K->attempt;
   int fired = 0;
+  const uint32_t c_lo = A.sl.on ? A.sl.lo : 0u, c_hi = A.sl.on ? A.sl.hi : m.N;  // a z-slab: its own subvolumes
   if (ex & 1u) {  // reference: every LEAP_CR subvolume (grid-stride: the grid is a few CTAs per SM)
-    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < m.N; c += gridDim.x * blockDim.x) {
+    for (uint32_t c = c_lo + blockIdx.x * blockDim.x + threadIdx.x; c < c_hi; c += gridDim.x * blockDim.x) {
       if (flag[c] != F_LEAP_CR) continue;
       Counts<MAXS> x;
       load_counts(m, Xc, c, x);
       fired += critical_event_ref<Real, LOG>(A, c, x, Xt, step, attempt, A.b.D, flag);
     }
   }
-  if ((ex & 2u) && blockIdx.x == 0 && threadIdx.x == 0) {
+  if ((ex & 2u) && blockIdx.x == 0 && threadIdx.x == 0 && (uint32_t)K->argmin >= c_lo && (uint32_t)K->argmin < c_hi) {
     const uint32_t am = (uint32_t)K->argmin;
     const uint8_t fa = flag[am];
     Counts<MAXS> x;
@@ -1507,7 +1513,10 @@ __global__ void __launch_bounds__(256) k_apply(KArgs A) {
   if (K->done || !(K->exact & 1u)) return;
   const DevModel& m = A.m;
   int32_t* Xt = A.b.X[K->tgt];
-  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < m.N; c += gridDim.x * blockDim.x) {
+  // a z-slab: its subvolumes and the ghost layers next to its faces (deltas of events that cross a face)
+  const uint32_t c_lo = A.sl.on ? A.sl.lo - A.sl.has_lo * A.sl.layer : 0u;
+  const uint32_t c_hi = A.sl.on ? A.sl.hi + A.sl.has_hi * A.sl.layer : m.N;
+  for (uint32_t c = c_lo + blockIdx.x * blockDim.x + threadIdx.x; c < c_hi; c += gridDim.x * blockDim.x) {
     for (uint32_t s = 0; s < m.S; ++s) {
       const size_t i = (size_t)s * m.Npad + c;
       const int32_t v = A.b.D[i];
@@ -1613,6 +1622,61 @@ __device__ __forceinline__ bool classify_slot(const KArgs& A, Ctrl* K, uint32_t 
   return s_last;
 }
 
+// The step decision (driver.cu:267-334) from the grid-wide reductions: the arg-min gt / gi (gi = -1 when
+// no subvolume can fire), #LEAP_CR gcr, #SSA_FF gff, a negative count or oversized draw `bad`, the min of
+// the plain taus gp (learned proposals) and the flag of the arg-min subvolume: rollback or accept, time,
+// the next plan.  One thread.
+__device__ __forceinline__ void step_decide(const KArgs& A, Ctrl* K, uint32_t phase, uint32_t tf, double gt, long long gi,
+                                            unsigned long long gcr, unsigned long long gff, uint32_t bad, double gp,
+                                            bool learned, uint32_t am_flag) {
+  const int mode = A.o.mode;
+  K->learned = learned ? 1u : 0u;
+  if (phase == 0) {
+    K->tau_min = gt;
+    K->tau_min_plain = gp;
+    K->argmin = gi;
+    K->n_leap_cr = (uint32_t)gcr;
+    K->ff_free = gff == 0 ? 1u : 0u;
+    K->argmin_flag = am_flag;
+    K->tf = tf ^ 1u;
+    K->phase = 1;
+    K->done = 1;  // idle until a run call
+  } else if (bad) {  // check_state + revert (leap.cu:203-212, driver.cu:292-315)
+    K->attempt += 1;
+    if ((int)K->attempt > A.o.max_rollbacks) {
+      K->status = PLIS_ERR_STUCK;
+      K->stop_reason = PLIS_STOP_ERROR;
+      K->done = 1;
+    } else {
+      const uint32_t t = K->tgt;
+      K->tgt = K->spare;
+      K->spare = t;
+      set_attempt(K, mode);
+    }
+  } else {
+    // accept: swap state (driver.cu:320-323) by rotating buffer indices
+    K->t = K->t + K->dt;
+    K->step = K->step + 1;
+    K->events += K->ev_attempt;
+    K->exact_events += K->ex_attempt;
+    K->rollbacks += K->attempt;
+    K->last_tau = K->tau_min;
+    K->last_argmin = K->argmin;
+    const uint32_t oc = K->cur;
+    K->cur = K->tgt;
+    K->tgt = K->spare;
+    K->spare = oc;
+    K->tf = tf ^ 1u;
+    K->tau_min = gt;
+    K->tau_min_plain = gp;
+    K->argmin = gi;
+    K->n_leap_cr = (uint32_t)gcr;
+    K->ff_free = gff == 0 ? 1u : 0u;
+    K->argmin_flag = am_flag;
+    prepare_step(K, mode);
+  }
+}
+
 // The whole last CTA: reduce the `nslots` slots (independent L2 loads spread over the block), then
 // one thread takes the step decision (driver.cu:267-334): rollback or accept, time, the next plan.
 __device__ __forceinline__ void classify_control(const KArgs& A, Ctrl* K, uint32_t nslots) {
@@ -1663,55 +1727,18 @@ __device__ __forceinline__ void classify_control(const KArgs& A, Ctrl* K, uint32
     if (sp) gp = warp_min_d(gp);
   }
   if (threadIdx.x == 0) {
-    const int mode = A.o.mode;
     const uint32_t leap_bad = (__ldcg(&K->blocks_done) & 0x80000000u) ? 1u : 0u;
     K->blocks_done = 0;
     if (gi == 0x7FFFFFFFFFFFFFFFll) gi = -1;
-    K->learned = sp ? 1u : 0u;
-    if (phase == 0) {
-      K->tau_min = gt;
-      K->tau_min_plain = gp;
-      K->argmin = gi;
-      K->n_leap_cr = (uint32_t)gcr;
-      K->ff_free = gff == 0 ? 1u : 0u;
-      K->argmin_flag = gi >= 0 ? __ldcg(&flag_new[gi]) : F_SSA_FF;
-      K->tf = tf ^ 1u;
-      K->phase = 1;
-      K->done = 1;  // idle until a run call
-    } else if (gbad || leap_bad) {  // check_state + revert (leap.cu:203-212, driver.cu:292-315)
-      K->attempt += 1;
-      if ((int)K->attempt > A.o.max_rollbacks) {
-        K->status = PLIS_ERR_STUCK;
-        K->stop_reason = PLIS_STOP_ERROR;
-        K->done = 1;
-      } else {
-        const uint32_t t = K->tgt;
-        K->tgt = K->spare;
-        K->spare = t;
-        set_attempt(K, mode);
-      }
-    } else {
-      // accept: swap state (driver.cu:320-323) by rotating buffer indices
-      K->t = K->t + K->dt;
-      K->step = K->step + 1;
-      K->events += K->ev_attempt;
-      K->exact_events += K->ex_attempt;
-      K->rollbacks += K->attempt;
-      K->last_tau = K->tau_min;
-      K->last_argmin = K->argmin;
-      const uint32_t oc = K->cur;
-      K->cur = K->tgt;
-      K->tgt = K->spare;
-      K->spare = oc;
-      K->tf = tf ^ 1u;
-      K->tau_min = gt;
-      K->tau_min_plain = gp;
-      K->argmin = gi;
-      K->n_leap_cr = (uint32_t)gcr;
-      K->ff_free = gff == 0 ? 1u : 0u;
-      K->argmin_flag = gi >= 0 ? __ldcg(&flag_new[gi]) : F_SSA_FF;
-      prepare_step(K, mode);
+    const uint32_t am_flag = gi >= 0 ? __ldcg(&flag_new[gi]) : F_SSA_FF;
+    if (A.sl.on) {  // a z-slab: the decision waits for every slab's summary (k_slab_control)
+      SlabSummary q;
+      q.tau = gt; q.idx = gi; q.tau_plain = gp; q.ncr = gcr; q.nff = gff; q.bad = gbad; q.leap_bad = leap_bad;
+      q.am_flag = am_flag; q.pad_ = 0;
+      *A.sl.summary = q;
+      return;
     }
+    step_decide(A, K, phase, tf, gt, gi, gcr, gff, gbad | leap_bad, gp, sp != nullptr, am_flag);
   }
 }
 
@@ -1735,6 +1762,153 @@ __global__ void __launch_bounds__(256, PLIS_CLASSIFY_MIN_BLOCKS) k_classify(KArg
   if (classify_slot(A, K, blockIdx.x, gridDim.x, tn, ti, valid && fl == F_LEAP_CR, bad, valid && fl == F_SSA_FF))
     classify_control(A, K, gridDim.x);
 }
+
+#ifdef PLIS_ENGINE_HOST_TU
+// ------------------------------------------------------------------------------------------------
+// z-slab exchanges (SlabArgs): layer i of a face is subvolume (first subvolume of the layer) + i;
+// a staging buffer holds [S][layer] counts, then [layer] flags widened to int32.
+// ------------------------------------------------------------------------------------------------
+// After the leap, exact events and deltas: the ghost layers of the target (molecules this slab sent
+// across its faces, with their receivers' flags) into send[0] (below) and send[1] (above).
+__global__ void k_slab_pack_ghosts(KArgs A) {
+  const Ctrl* K = A.b.ctrl;
+  if (K->done) return;
+  const SlabArgs& L = A.sl;
+  const int32_t* Xt = A.b.X[K->tgt];
+  const uint8_t* flag = A.b.flag[K->tf];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < L.layer; i += gridDim.x * blockDim.x) {
+    for (int side = 0; side < 2; ++side) {
+      if (!(side ? L.has_hi : L.has_lo)) continue;
+      const uint32_t g = side ? L.hi + i : L.lo - L.layer + i;
+      for (uint32_t s = 0; s < A.m.S; ++s) L.send[side][(size_t)s * L.layer + i] = Xt[(size_t)s * A.m.Npad + g];
+      L.send[side][(size_t)A.m.S * L.layer + i] = flag[g];
+    }
+  }
+}
+
+// The neighbours' ghost layers added into this slab's face layers (their molecules that crossed into
+// it), their flag changes (SSA_FF -> SSA only) merged, then the gathered flag writes that land in
+// this slab applied.  An attempt with more such writes than one list holds fails (PLIS_ERR_LIMIT,
+// identically on every rank).
+__global__ void k_slab_merge(KArgs A) {
+  Ctrl* K = A.b.ctrl;
+  if (K->done) return;
+  const SlabArgs& L = A.sl;
+  int32_t* Xt = A.b.X[K->tgt];
+  uint8_t* flag = A.b.flag[K->tf];
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  for (uint32_t i = tid; i < L.layer; i += nth) {
+    for (int side = 0; side < 2; ++side) {
+      if (!(side ? L.has_hi : L.has_lo)) continue;
+      const uint32_t b = side ? L.hi - L.layer + i : L.lo + i;
+      const int32_t* r = L.recv[side];
+      for (uint32_t s = 0; s < A.m.S; ++s) {
+        const int32_t v = r[(size_t)s * L.layer + i];
+        if (v) Xt[(size_t)s * A.m.Npad + b] += v;
+      }
+      if (r[(size_t)A.m.S * L.layer + i] == F_SSA && flag[b] == F_SSA_FF) flag[b] = F_SSA;
+    }
+  }
+  for (uint32_t w = 0; w < L.world; ++w) {
+    const SlabRemote& R = L.remote_all[w];
+    const uint32_t n = R.n < (uint32_t)kSlabRemote ? R.n : (uint32_t)kSlabRemote;
+    if (R.n > (uint32_t)kSlabRemote && tid == 0) {
+      K->status = PLIS_ERR_LIMIT;
+      K->stop_reason = PLIS_STOP_ERROR;
+    }
+    for (uint32_t j = tid; j < n; j += nth) {
+      const uint32_t q = R.cell[j];
+      if (q >= L.lo && q < L.hi && flag[q] == F_SSA_FF) flag[q] = F_SSA;
+    }
+  }
+}
+
+// This slab's face layers of the target (final counts of the attempt) into send[0] / send[1].
+__global__ void k_slab_pack_faces(KArgs A) {
+  const Ctrl* K = A.b.ctrl;
+  if (K->done) return;
+  const SlabArgs& L = A.sl;
+  const int32_t* Xt = A.b.X[K->tgt];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < L.layer; i += gridDim.x * blockDim.x) {
+    for (int side = 0; side < 2; ++side) {
+      if (!(side ? L.has_hi : L.has_lo)) continue;
+      const uint32_t b = side ? L.hi - L.layer + i : L.lo + i;
+      for (uint32_t s = 0; s < A.m.S; ++s) L.send[side][(size_t)s * L.layer + i] = Xt[(size_t)s * A.m.Npad + b];
+    }
+  }
+}
+
+// The neighbours' face layers into this slab's ghost layers of the target: the neighbour counts the
+// classification of the faces reads.
+__global__ void k_slab_unpack_ghosts(KArgs A) {
+  const Ctrl* K = A.b.ctrl;
+  if (K->done) return;
+  const SlabArgs& L = A.sl;
+  int32_t* Xt = A.b.X[K->tgt];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < L.layer; i += gridDim.x * blockDim.x) {
+    for (int side = 0; side < 2; ++side) {
+      if (!(side ? L.has_hi : L.has_lo)) continue;
+      const uint32_t g = side ? L.hi + i : L.lo - L.layer + i;
+      for (uint32_t s = 0; s < A.m.S; ++s) Xt[(size_t)s * A.m.Npad + g] = L.recv[side][(size_t)s * L.layer + i];
+    }
+  }
+}
+
+// The decision from every slab's summary, reduced in rank order exactly as the single domain reduces
+// its CTA slots (min tau, then the lowest index), by one thread; identical on every rank.
+__global__ void k_slab_control(KArgs A) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  Ctrl* K = A.b.ctrl;
+  if (K->status != PLIS_OK) { K->done = 1; return; }
+  double gt = PLIS_INF_D, gp = PLIS_INF_D;
+  long long gi = 0x7FFFFFFFFFFFFFFFll;
+  unsigned long long gcr = 0, gff = 0;
+  uint32_t bad = 0, am_flag = F_SSA_FF;
+  for (uint32_t w = 0; w < A.sl.world; ++w) {
+    const SlabSummary& q = A.sl.all[w];
+    const long long qi = q.idx < 0 ? 0x7FFFFFFFFFFFFFFFll : q.idx;
+    if (q.tau < gt || (q.tau == gt && qi < gi)) { gt = q.tau; gi = qi; am_flag = q.am_flag; }
+    gp = fmin(gp, q.tau_plain);
+    gcr += q.ncr;
+    gff += q.nff;
+    bad |= q.bad | q.leap_bad;
+  }
+  if (gi == 0x7FFFFFFFFFFFFFFFll) { gi = -1; am_flag = F_SSA_FF; }
+  step_decide(A, K, K->phase, K->tf, gt, gi, gcr, gff, bad, gp, false, am_flag);
+}
+
+// After the decision: this slab's face flags (the current flags) into send[0] / send[1], and the ghost
+// layers of the next target zeroed (the classification zeroed the slab's own part).
+__global__ void k_slab_pack_flags(KArgs A) {
+  const Ctrl* K = A.b.ctrl;
+  const SlabArgs& L = A.sl;
+  const uint8_t* flag = A.b.flag[K->tf];
+  int32_t* Xn = A.b.X[K->tgt];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < L.layer; i += gridDim.x * blockDim.x) {
+    for (int side = 0; side < 2; ++side) {
+      if (!(side ? L.has_hi : L.has_lo)) continue;
+      const uint32_t b = side ? L.hi - L.layer + i : L.lo + i;
+      const uint32_t g = side ? L.hi + i : L.lo - L.layer + i;
+      L.send[side][(size_t)A.m.S * L.layer + i] = flag[b];
+      for (uint32_t s = 0; s < A.m.S; ++s) Xn[(size_t)s * A.m.Npad + g] = 0;
+    }
+  }
+}
+
+// The neighbours' face flags into this slab's ghost flags (the leap reads its receivers' flags).
+__global__ void k_slab_unpack_flags(KArgs A) {
+  const Ctrl* K = A.b.ctrl;
+  const SlabArgs& L = A.sl;
+  uint8_t* flag = A.b.flag[K->tf];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < L.layer; i += gridDim.x * blockDim.x) {
+    for (int side = 0; side < 2; ++side) {
+      if (!(side ? L.has_hi : L.has_lo)) continue;
+      const uint32_t g = side ? L.hi + i : L.lo - L.layer + i;
+      flag[g] = (uint8_t)L.recv[side][(size_t)A.m.S * L.layer + i];
+    }
+  }
+}
+#endif
 
 #ifdef PLIS_ENGINE_HOST_TU
 __global__ void k_fill_tau(double* t, uint8_t* f, uint32_t n) {
