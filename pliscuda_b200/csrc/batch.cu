@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "batch.h"
+#include "engine.h"
 #include "learned.h"
 #include "batch_kernels.cuh"
 
@@ -187,6 +188,12 @@ int BatchEngine::create(const plis_batch_desc& d, const plis_options& opt) {
   // per-replica rate tables in the working precision
   const std::vector<double> rr(d.reaction_rates, d.reaction_rates + (size_t)nrep_ * R_);
   const std::vector<double> dr(d.diffusion_rates, d.diffusion_rates + (size_t)nrep_ * S_);
+  h_rr_ = rr;
+  h_dr_ = dr;
+  {  // small networks: every replica's tables and rate constants in its argument block (SmallModel)
+    SmallModel probe;
+    small_ = fill_small_model(shared_, rr.data(), dr.data(), &probe);
+  }
   if (opt.precision == PLIS_PREC_FP32) {
     const std::vector<float> rf(rr.begin(), rr.end()), df(dr.begin(), dr.end());
     const float* p;
@@ -237,7 +244,7 @@ int BatchEngine::create(const plis_batch_desc& d, const plis_options& opt) {
   }
   PLIS_CU(cudaMemcpy(d_ctrl_, h_ctrl_.data(), nrep_ * sizeof(Ctrl), cudaMemcpyHostToDevice));
   pending_.assign(nrep_, 2);  // 2 = never given a state
-  launch_ = (opt.precision == PLIS_PREC_FP32) ? batch_pick_f32(S_, false) : batch_pick_f64(S_, false);
+  launch_ = (opt.precision == PLIS_PREC_FP32) ? batch_pick_f32(S_, false, small_) : batch_pick_f64(S_, false, small_);
   int tile[3] = {opt.tile[0], opt.tile[1], opt.tile[2]};
   if (tile[0] <= 0 || tile[1] <= 0 || tile[2] <= 0) { tile[0] = 8; tile[1] = 8; tile[2] = 4; }
   rc = layout(tile);
@@ -316,6 +323,7 @@ int BatchEngine::layout(const int tile[3]) {
     v.b.slot_cr = d_slot_cr_ + rep[r].tile_off;
     v.b.slot_bad = d_slot_bad_ + rep[r].tile_off;
     v.b.ctrl = d_ctrl_ + r;
+    if (small_) fill_small_model(shared_, &h_rr_[(size_t)r * R_], &h_dr_[(size_t)r * S_], &v.sm);
     if (learned_) {
       v.b.lp = d_lp_;
       v.b.slot_tau_plain = d_slot_plain_ + rep[r].tile_off;
@@ -400,7 +408,7 @@ int BatchEngine::set_proposer(const float* weights, double s_max) {
     PLIS_CU(cudaStreamSynchronize(stream_));
   }
   learned_ = on;
-  launch_ = (opt_.precision == PLIS_PREC_FP32) ? batch_pick_f32(S_, on) : batch_pick_f64(S_, on);
+  launch_ = (opt_.precision == PLIS_PREC_FP32) ? batch_pick_f32(S_, on, small_) : batch_pick_f64(S_, on, small_);
   const int tile[3] = {(int)tile_[0], (int)tile_[1], (int)tile_[2]};
   int rc = layout(tile);
   if (rc) return rc;

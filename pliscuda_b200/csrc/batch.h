@@ -21,8 +21,9 @@ struct BatchLaunch {
   void* kernel;        // k_batch<Real, MAXS>
   cudaError_t (*set_smem)(int bytes);
 };
-BatchLaunch batch_pick_f64(uint32_t S, bool learned);
-BatchLaunch batch_pick_f32(uint32_t S, bool learned);
+// small: the network fits the SmallModel tables (every replica's argument block carries them)
+BatchLaunch batch_pick_f64(uint32_t S, bool learned, bool small);
+BatchLaunch batch_pick_f32(uint32_t S, bool learned, bool small);
 void batch_prepare(const BatchArgs& B, double t_end, unsigned long long n_steps, cudaStream_t s);
 
 class BatchEngine {
@@ -55,6 +56,8 @@ class BatchEngine {
   std::vector<uint32_t> dims_;          // [nrep*3] squeezed lattice dims
   std::vector<uint32_t> ids_;
   std::vector<uint32_t> coff_, npad_;
+  std::vector<double> h_rr_, h_dr_;  // per-replica rate constants (host copies, for the SmallModel blocks)
+  bool small_ = false;
   uint64_t ntot_ = 0;
   uint32_t tile_[3] = {0, 0, 0};
   uint32_t total_tiles_ = 0, max_tiles_ = 0;

@@ -2,7 +2,7 @@
 #include "batch_kernels.cuh"
 
 namespace plis {
-BatchLaunch batch_pick_f64(uint32_t S, bool learned) {
-  return learned ? batch_pick_impl<double, true>(S) : batch_pick_impl<double, false>(S);
+BatchLaunch batch_pick_f64(uint32_t S, bool learned, bool small) {
+  return learned ? batch_pick_impl<double, true>(S, small) : batch_pick_impl<double, false>(S, small);
 }
 }  // namespace plis

@@ -163,6 +163,24 @@ __device__ __forceinline__ void block_prefix2(uint32_t* a, uint32_t* b, uint32_t
   __syncthreads();
 }
 
+// The argument block of replica r, copied into shared memory when the CTA's work item moves to
+// another replica (r is the CTA's work item, the same in every thread, so the branch is uniform).
+// The phases then read the replica's arrays, geometry and tables from shared memory instead of
+// global memory.  *svr names the replica held; it is written between the two barriers, so every
+// thread reads the same value at the next call.
+__device__ __forceinline__ const KArgs& replica_view(const BatchArgs& B, uint32_t r, KArgs* sv, uint32_t* svr) {
+  if (*svr != r) {
+    __syncthreads();  // every thread is done with the previous replica's block
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(B.views + r);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(sv);
+    for (uint32_t i = threadIdx.x; i < (uint32_t)(sizeof(KArgs) / 8); i += blockDim.x) dst[i] = __ldg(src + i);
+    if (threadIdx.x == 0) *svr = r;
+    __syncthreads();
+  }
+  return *sv;
+}
+static_assert(sizeof(KArgs) % 8 == 0, "replica_view copies the argument block in 8-byte words");
+
 // replica owning work index w of an inclusive-exclusive prefix array p[0..n]
 __device__ __forceinline__ uint32_t find_replica(const uint32_t* p, uint32_t n, uint32_t w) {
   uint32_t lo = 0, hi = n;  // p[lo] <= w < p[hi]
@@ -185,7 +203,8 @@ __device__ __forceinline__ uint32_t find_replica(const uint32_t* p, uint32_t n, 
 #endif
 // LEARNED: the classification phase takes learned tau proposals (learned_dev.cuh; corrected
 // semantics, every replica's view holds the proposer and its plain-min slots).
-template <typename Real, int MAXS, bool LEARNED>
+// SM: every replica's argument block carries the SmallModel tables (small networks).
+template <typename Real, int MAXS, bool LEARNED, bool SM>
 __global__ void __launch_bounds__(256, LEARNED ? PLIS_BATCH_MIN_BLOCKS_LEARNED : PLIS_BATCH_MIN_BLOCKS)
     k_batch(BatchArgs B) {
   extern __shared__ int32_t s_box[];
@@ -196,6 +215,10 @@ __global__ void __launch_bounds__(256, LEARNED ? PLIS_BATCH_MIN_BLOCKS_LEARNED :
   uint32_t* s_xp = s_cp + (nrep + 1);  // exact events: every brick (critical events) or one item (arg-min event)
   uint32_t* s_ap = s_xp + (nrep + 1);  // bricks applying critical-event deltas
   __shared__ int s_exact, s_apply;
+  __shared__ KArgs s_view;   // the argument block of the replica this CTA works on (replica_view)
+  __shared__ uint32_t s_vr;
+  if (threadIdx.x == 0) s_vr = 0xFFFFFFFFu;
+  __syncthreads();
   unsigned par = 0;  // slot parity of grab()
   Box box;
   box.acc = B.g.staged ? s_box : nullptr;
@@ -241,7 +264,7 @@ __global__ void __launch_bounds__(256, LEARNED ? PLIS_BATCH_MIN_BLOCKS_LEARNED :
         const unsigned w = grab(B.work + 0 * 3 + gen, n_leap, par);
         if (w >= n_leap) break;
         const uint32_t r = find_replica(s_lp, nrep, w);
-        const KArgs& sA = B.views[r];
+        const KArgs& sA = replica_view(B, r, &s_view, &s_vr);
         Ctrl* K = sA.b.ctrl;
         LeapCtx L;
         L.Xc = sA.b.X[K->cur];
@@ -254,7 +277,7 @@ __global__ void __launch_bounds__(256, LEARNED ? PLIS_BATCH_MIN_BLOCKS_LEARNED :
         const Real tl = (Real)K->tau_leap;
         long long ev;
         int big;
-        leap_tile<Real, MAXS, false, false>(sA, w - s_lp[r], L, tl, box, ev, big);
+        leap_tile<Real, MAXS, false, false, SM>(sA, w - s_lp[r], L, tl, box, ev, big);
         ev = warp_sum(ev);  // events by warp, straight into the replica's counter (integer: order-free)
         if ((threadIdx.x & 31) == 0 && ev) atomicAdd(&K->ev_attempt, (unsigned long long)ev);
         if (big) atomicOr(&K->blocks_done, 0x80000000u);  // rare: an oversized draw forces a rollback
@@ -271,7 +294,7 @@ __global__ void __launch_bounds__(256, LEARNED ? PLIS_BATCH_MIN_BLOCKS_LEARNED :
         if (w >= n_ex) break;
         const uint32_t r = find_replica(s_xp, nrep, w);
         const uint32_t item = w - s_xp[r];
-        const KArgs& sA = B.views[r];
+        const KArgs& sA = replica_view(B, r, &s_view, &s_vr);
         Ctrl* K = sA.b.ctrl;
         const uint32_t ex = K->exact;
         const int32_t* Xc = sA.b.X[K->cur];
@@ -314,7 +337,7 @@ __global__ void __launch_bounds__(256, LEARNED ? PLIS_BATCH_MIN_BLOCKS_LEARNED :
           const unsigned w = grab(B.work + 2 * 3 + gen, n_ap, par);
           if (w >= n_ap) break;
           const uint32_t r = find_replica(s_ap, nrep, w);
-          const KArgs& sA = B.views[r];
+          const KArgs& sA = replica_view(B, r, &s_view, &s_vr);
           const Ctrl* K = sA.b.ctrl;
           Cell cl;
           if (cell_of(sA, w - s_ap[r], cl)) {
@@ -339,7 +362,7 @@ __global__ void __launch_bounds__(256, LEARNED ? PLIS_BATCH_MIN_BLOCKS_LEARNED :
       const unsigned w = grab(B.work + 3 * 3 + gen, n_class, par);
       if (w >= n_class) break;
       const uint32_t r = find_replica(s_cp, nrep, w);
-      const KArgs& sA = B.views[r];
+      const KArgs& sA = replica_view(B, r, &s_view, &s_vr);
       Ctrl* K = sA.b.ctrl;
       const ClassifyCtx C = classify_ctx(sA, K);
       const uint32_t tile = w - s_cp[r];
@@ -350,7 +373,7 @@ __global__ void __launch_bounds__(256, LEARNED ? PLIS_BATCH_MIN_BLOCKS_LEARNED :
         long long ti;
         int fl, bad;
         bool valid;
-        classify_tile<Real, MAXS, false>(sA, tile, C, tn, ti, fl, bad, valid);
+        classify_tile<Real, MAXS, false, false, SM>(sA, tile, C, tn, ti, fl, bad, valid);
         if (classify_slot(sA, K, tile, sA.g.nblocks, tn, ti, valid && fl == F_LEAP_CR, bad, valid && fl == F_SSA_FF))
           classify_control(sA, K, sA.g.nblocks);
       }
@@ -362,24 +385,29 @@ __global__ void __launch_bounds__(256, LEARNED ? PLIS_BATCH_MIN_BLOCKS_LEARNED :
   }
 }
 
-template <typename Real, int MAXS, bool LEARNED>
+template <typename Real, int MAXS, bool LEARNED, bool SM>
 struct BatchKernelSet {
-  static void* kernel() { return (void*)&k_batch<Real, MAXS, LEARNED>; }
+  static void* kernel() { return (void*)&k_batch<Real, MAXS, LEARNED, SM>; }
   static cudaError_t set_smem(int bytes) {
-    return cudaFuncSetAttribute(k_batch<Real, MAXS, LEARNED>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return cudaFuncSetAttribute(k_batch<Real, MAXS, LEARNED, SM>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   }
 };
 
 template <typename Real, bool LEARNED>
-BatchLaunch batch_pick_impl(uint32_t S) {
-  if (S <= 1) return {BatchKernelSet<Real, 1, LEARNED>::kernel(), BatchKernelSet<Real, 1, LEARNED>::set_smem};
-  if (S <= 2) return {BatchKernelSet<Real, 2, LEARNED>::kernel(), BatchKernelSet<Real, 2, LEARNED>::set_smem};
-  if (S <= 4) return {BatchKernelSet<Real, 4, LEARNED>::kernel(), BatchKernelSet<Real, 4, LEARNED>::set_smem};
+BatchLaunch batch_pick_impl(uint32_t S, bool small) {
+  if (small) {  // the SmallModel tables hold up to kSmallS species
+    if (S <= 1) return {BatchKernelSet<Real, 1, LEARNED, true>::kernel(), BatchKernelSet<Real, 1, LEARNED, true>::set_smem};
+    if (S <= 2) return {BatchKernelSet<Real, 2, LEARNED, true>::kernel(), BatchKernelSet<Real, 2, LEARNED, true>::set_smem};
+    return {BatchKernelSet<Real, 4, LEARNED, true>::kernel(), BatchKernelSet<Real, 4, LEARNED, true>::set_smem};
+  }
+  if (S <= 1) return {BatchKernelSet<Real, 1, LEARNED, false>::kernel(), BatchKernelSet<Real, 1, LEARNED, false>::set_smem};
+  if (S <= 2) return {BatchKernelSet<Real, 2, LEARNED, false>::kernel(), BatchKernelSet<Real, 2, LEARNED, false>::set_smem};
+  if (S <= 4) return {BatchKernelSet<Real, 4, LEARNED, false>::kernel(), BatchKernelSet<Real, 4, LEARNED, false>::set_smem};
   if constexpr (LEARNED) {
     return {nullptr, nullptr};  // learned proposals: up to 4 species
   } else {
-    if (S <= 8) return {BatchKernelSet<Real, 8, false>::kernel(), BatchKernelSet<Real, 8, false>::set_smem};
-    return {BatchKernelSet<Real, 16, false>::kernel(), BatchKernelSet<Real, 16, false>::set_smem};
+    if (S <= 8) return {BatchKernelSet<Real, 8, false, false>::kernel(), BatchKernelSet<Real, 8, false, false>::set_smem};
+    return {BatchKernelSet<Real, 16, false, false>::kernel(), BatchKernelSet<Real, 16, false, false>::set_smem};
   }
 }
 

@@ -78,6 +78,43 @@ int Engine::upload(const std::vector<T>& v, const T** out) {
   return PLIS_OK;
 }
 
+// The SmallModel block of a model that fits it (at most kSmallR reactions and kSmallS species, net
+// changes within int8, one set of rate constants: rrate[R] and drate[S]; rrate null = several sets);
+// sm->on = 0 otherwise.
+bool fill_small_model(const Model& M, const double* rrate, const double* drate, SmallModel* out) {
+  SmallModel& sm = *out;
+  std::memset(&sm, 0, sizeof sm);
+  const ReactionTables& t = M.rt;
+  bool fits = rrate && M.R <= (uint32_t)kSmallR && M.S <= (uint32_t)kSmallS;
+  for (size_t r = 0; fits && r < M.R; ++r)
+    for (size_t s = 0; s < M.S; ++s) {
+      const int nu = M.products[s * M.R + r] - M.reactants[s * M.R + r];
+      if (nu < -127 || nu > 127) fits = false;
+    }
+  if (!fits) return false;
+  for (uint32_t r = 0; r < M.R; ++r) {
+    sm.nreac[r] = t.n_reac[r];
+    for (int i = 0; i < t.n_reac[r]; ++i) {
+      sm.rs[r][i] = (uint8_t)t.reac_s[r * kMaxReactantSpecies + i];
+      sm.rm[r][i] = t.reac_m[r * kMaxReactantSpecies + i];
+      sm.rnu[r][i] = (int8_t)t.reac_nu[r * kMaxReactantSpecies + i];
+      sm.rmask[sm.rs[r][i]] |= (uint8_t)(1u << r);
+    }
+    for (int i = 0; i < t.n_net[r]; ++i) sm.nu[r][t.net_s[r * kMaxNet + i]] = (int8_t)t.net_nu[r * kMaxNet + i];
+    sm.inv_denom[r] = t.inv_denom[r];
+    sm.rate_d[r] = rrate[r];
+    sm.rate_f[r] = (float)rrate[r];
+  }
+  for (uint32_t s = 0; s < M.S; ++s) {
+    sm.hor[s] = t.hor[s];
+    sm.hmult[s] = t.hmult[s];
+    sm.drate_d[s] = drate[s];
+    sm.drate_f[s] = (float)drate[s];
+  }
+  sm.on = 1;
+  return true;
+}
+
 int Engine::create(const Model& model, const plis_options& opt) {
   model_ = model;
   opt_ = opt;
@@ -144,40 +181,8 @@ int Engine::create(const Model& model, const plis_options& opt) {
     dm.dr = p;
   }
 
-  // a small model's tables in the kernel arguments (SmallModel): at most kSmallR reactions and
-  // kSmallS species, one set of rate constants for every subvolume, coefficients that fit int8
-  {
-    SmallModel& sm = args_.sm;
-    std::memset(&sm, 0, sizeof sm);
-    bool fits = M.R <= (uint32_t)kSmallR && M.S <= (uint32_t)kSmallS && M.comp.empty();
-    for (size_t r = 0; fits && r < M.R; ++r)
-      for (size_t s = 0; s < M.S; ++s) {
-        const int nu = M.products[s * M.R + r] - M.reactants[s * M.R + r];
-        if (nu < -127 || nu > 127) fits = false;
-      }
-    if (fits) {
-      for (uint32_t r = 0; r < M.R; ++r) {
-        sm.nreac[r] = t.n_reac[r];
-        for (int i = 0; i < t.n_reac[r]; ++i) {
-          sm.rs[r][i] = (uint8_t)t.reac_s[r * kMaxReactantSpecies + i];
-          sm.rm[r][i] = t.reac_m[r * kMaxReactantSpecies + i];
-          sm.rnu[r][i] = (int8_t)t.reac_nu[r * kMaxReactantSpecies + i];
-          sm.rmask[sm.rs[r][i]] |= (uint8_t)(1u << r);
-        }
-        for (int i = 0; i < t.n_net[r]; ++i) sm.nu[r][t.net_s[r * kMaxNet + i]] = (int8_t)t.net_nu[r * kMaxNet + i];
-        sm.inv_denom[r] = t.inv_denom[r];
-        sm.rate_d[r] = M.rrate[r];
-        sm.rate_f[r] = (float)M.rrate[r];
-      }
-      for (uint32_t s = 0; s < M.S; ++s) {
-        sm.hor[s] = t.hor[s];
-        sm.hmult[s] = t.hmult[s];
-        sm.drate_d[s] = M.drate[s];
-        sm.drate_f[s] = (float)M.drate[s];
-      }
-      sm.on = 1;
-    }
-  }
+  // a small model's tables in the kernel arguments (SmallModel)
+  fill_small_model(M, M.comp.empty() ? M.rrate.data() : nullptr, M.drate.data(), &args_.sm);
 
   // geometry
   Geo& g = args_.g;

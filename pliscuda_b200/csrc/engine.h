@@ -23,6 +23,9 @@ struct Launchers {
   cudaError_t (*leap_smem)(int bytes);
 };
 
+// SmallModel tables of a model (engine.cu); false, with sm->on = 0, when it does not fit.
+bool fill_small_model(const Model& M, const double* rrate, const double* drate, SmallModel* sm);
+
 class Engine {
  public:
   Engine();
