@@ -409,13 +409,14 @@ def _batch_to_checkpoints(model, state, checkpoints, *, seed, weights=None, s_ma
     return snaps, tot
 
 
-def batch_report(t0: float = 0.001, t1: float = 0.006):
+def batch_report(t0: float = 0.001, t1: float = 0.006, t_long: float = 0.05):
     """Batched form: 256 Brusselator replicas (side ~ U{8..48}, 7.77 M subvolumes, a ~ U[50,200],
     b ~ U[100,600], reference semantics, FP64) in one persistent cooperative launch, brick shape
     autotuned.  The configuration runs to t = 5, which takes ~2.7 M steps for the stiffest replica;
     the measurement is the slice t0 -> t1 after a warm-up to t0.  The unbatched alternative is the
     same 256 replicas run one after another as single handles with the same streams (identical
-    trajectories, so identical events)."""
+    trajectories, so identical events).  The batch then continues to t_long: events/s of the batch over
+    t0 -> t_long (steps per replica: the tail of stiff replicas sets the number of rounds)."""
     import numpy as np
     from pliscuda_b200 import Simulation, workloads
     from pliscuda_b200.batch import Batch
@@ -430,9 +431,14 @@ def batch_report(t0: float = 0.001, t1: float = 0.006):
         a = [b.stats(i) for i in range(n)]
         b.run(t1)
         c = [b.stats(i) for i in range(n)]
+        b.run(t_long)  # the same batch continued: a ten times longer horizon, batch only
+        e = [b.stats(i) for i in range(n)]
     steps = np.array([c[i].steps - a[i].steps for i in range(n)])
     ev = int(sum(c[i].events - a[i].events for i in range(n)))
     ms = c[0].device_ms - a[0].device_ms
+    steps_l = np.array([e[i].steps - a[i].steps for i in range(n)])
+    ev_l = int(sum(e[i].events - a[i].events for i in range(n)))
+    ms_l = e[0].device_ms - a[0].device_ms
     s_ms, s_ev = 0.0, 0
     for i, (m, st, _) in enumerate(reps):
         with Simulation(m, mode="reference", seed=1, replica=i) as sim:
@@ -455,7 +461,10 @@ def batch_report(t0: float = 0.001, t1: float = 0.006):
             "sim_time_per_s": (t1 - t0) / (ms * 1e-3), "subvolume_steps": int((steps * cells).sum()),
             "steps_per_replica_q0_50_100": [int(np.quantile(steps, q)) for q in (0, 0.5, 1)],
             "single_handles": {"device_ms": s_ms, "events": int(s_ev), "events_per_s": s_ev / (s_ms * 1e-3)},
-            "speedup_vs_single_handles": s_ms / ms}
+            "speedup_vs_single_handles": s_ms / ms,
+            "long_horizon": {"slice": f"t = {t0} -> {t_long}", "events": int(ev_l), "device_ms": ms_l,
+                             "events_per_s": ev_l / (ms_l * 1e-3), "sim_time_per_s": (t_long - t0) / (ms_l * 1e-3),
+                             "steps_per_replica_q0_50_100": [int(np.quantile(steps_l, q)) for q in (0, 0.5, 1)]}}
 
 
 def configs_report():
