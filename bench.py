@@ -254,6 +254,21 @@ def ncu_case(args):
     return 0
 
 
+def ncu_network_case(args):
+    """Fixed small case for ncu captures of the random network (10 species, 20 reactions, the precision
+    configuration's network) on a 64^3 lattice: 10 + 3 steps (capture with -k regex:"^k_leap$" -s 10 -c 1,
+    or the classification likewise).  64^3 keeps the device memory to a few tens of MB while the
+    counts (10.5 MB per buffer) still exceed what the L1s hold."""
+    from pliscuda_b200 import Simulation, workloads
+    model, state = workloads.random_network(64)
+    with Simulation(model, mode=args.mode, precision=args.precision, seed=1000) as sim:
+        sim.set_state(state)
+        sim.step(10)
+        st = sim.step(3)
+    print(json.dumps({"ncu_network_case": 64, "steps": st.steps, "events": st.events}))
+    return 0
+
+
 def ncu_learned_case(args):
     """Fixed small case for ncu captures of the learned step: a proposer trained briefly on 10 plain
     corrected steps of the workload (clamp 16), then 10 + 3 learned steps (plain launches).  Filter
@@ -652,6 +667,7 @@ def main(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--ncu-case", action="store_true", help="run only the fixed ncu capture case")
     ap.add_argument("--ncu-learned-case", action="store_true", help="run only the fixed ncu case of the learned step")
+    ap.add_argument("--ncu-network-case", action="store_true", help="run only the fixed ncu case of the random network")
     ap.add_argument("--ncu-batch-case", action="store_true", help="run only the fixed ncu case of the batched form")
     ap.add_argument("--precision-report", action="store_true", help="FP32 form vs binary64 on the precision config")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-tau comparison")
@@ -672,6 +688,8 @@ def main(argv=None):
         return ncu_case(args)
     if args.ncu_learned_case:
         return ncu_learned_case(args)
+    if args.ncu_network_case:
+        return ncu_network_case(args)
     if args.ncu_batch_case:
         return ncu_batch_case(args)
     if args.precision_report:
