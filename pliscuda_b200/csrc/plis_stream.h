@@ -146,8 +146,8 @@ enum {
 PLIS_HD uint32_t plis_ch_react(uint32_t r) { return r; }
 PLIS_HD uint32_t plis_ch_diff(uint32_t s, uint32_t slot) { return PLIS_CH_DIFF_BASE + s * 8u + slot; }
 // Grouped channels: the single uniforms of the inversion-searched draws (means below 10) of a group
-// come from shared Philox blocks, two binary64 or four binary32 uniforms per block (uniform i of a
-// group: block i / per-block, words in order).  Reactions 4g .. 4g+3 form group g; the six
+// come from shared Philox blocks, four uniforms per block (uniform i of a group: word i % 4 of block
+// i / 4).  Reactions 4g .. 4g+3 form group g; the six
 // neighbour slots of one species form its diffusion group.  Draws searched by PTRS keep their own
 // channels (plis_ch_react, plis_ch_diff).
 #define PLIS_CH_RGROUP_BASE 0x20000u  // + reaction group
@@ -211,18 +211,18 @@ PLIS_HD float plis_uniform_f(plis_stream* s) {
 
 // Uniforms 0 .. n-1 of a group (n <= 8): u[i] for every i whose bit is set in `need` (the others may
 // be left unset).  `g` is the group's stream (plis_stream_make with the group channel); its blocks
-// are computed here, only those holding a needed uniform.  binary64: uniform i from words
-// (2(i%2), 2(i%2)+1) of block i/2; binary32: word i%4 of block i/4; the conversions are
-// plis_uniform_d / plis_uniform_f's.
+// are computed here, only those holding a needed uniform.  Uniform i is word i%4 of block i/4 in both
+// precisions: binary64 takes all 32 bits of the word, (w + 1/2) 2^-32 (exact in binary64; an
+// inversion search from 0 only ever compares it with a CDF, and 2^-32 resolution leaves unreached
+// only upper tails of probability below 2^-33), binary32 the top 23 bits as plis_uniform_f does.
 PLIS_HD plis_u32x4 plis_group_block(const plis_stream* g, uint32_t b) {
   plis_u32x4 ctr = g->ctr;
   ctr.y = (ctr.y & 0xFFFFF000u) | (b & 0xFFFu);
   return plis_philox4x32_10(ctr, g->k0, g->k1);
 }
 
-PLIS_HD double plis_u64_to_uniform_d(uint32_t hi, uint32_t lo) {
-  uint64_t x = (((uint64_t)hi << 32) | (uint64_t)lo) >> 12;
-  return ((double)x + 0.5) * 2.220446049250313e-16;  // 2^-52
+PLIS_HD double plis_u32_to_uniform_d(uint32_t w) {
+  return ((double)w + 0.5) * 2.3283064365386963e-10;  // 2^-32
 }
 
 PLIS_HD float plis_u32_to_uniform_f(uint32_t w) {
@@ -234,11 +234,13 @@ PLIS_HD void plis_group_uniforms_d(const plis_stream* g, uint32_t need, double* 
 #if defined(__CUDA_ARCH__)
 #pragma unroll
 #endif
-  for (int b = 0; b < 4; ++b) {
-    if (2 * b < n && (need >> (2 * b)) & 3u) {
+  for (int b = 0; b < 2; ++b) {
+    if (4 * b < n && (need >> (4 * b)) & 15u) {
       const plis_u32x4 w = plis_group_block(g, (uint32_t)b);
-      u[2 * b] = plis_u64_to_uniform_d(w.x, w.y);
-      if (2 * b + 1 < n) u[2 * b + 1] = plis_u64_to_uniform_d(w.z, w.w);
+      u[4 * b] = plis_u32_to_uniform_d(w.x);
+      if (4 * b + 1 < n) u[4 * b + 1] = plis_u32_to_uniform_d(w.y);
+      if (4 * b + 2 < n) u[4 * b + 2] = plis_u32_to_uniform_d(w.z);
+      if (4 * b + 3 < n) u[4 * b + 3] = plis_u32_to_uniform_d(w.w);
     }
   }
 }
