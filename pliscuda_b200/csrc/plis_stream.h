@@ -458,9 +458,10 @@ PLIS_HD double plis_poisson_d(plis_stream* st, double lam) {
     // inversion by sequential search
     return plis_poisson_small_d(st, lam, plis_exp(-lam));
   }
-  // PTRS, Hormann (1993)
+  // PTRS, Hormann (1993).  ln(lambda) is needed only by the full acceptance test, which the squeeze
+  // (us >= 0.07 && V <= vr) spares about 86 % of the draws, so it is computed on first use.
   double slam = PLIS_SQRT(lam);
-  double loglam = plis_log(lam);
+  double loglam = -1.0;
   double b = 0.931 + 2.53 * slam;
   double a = -0.059 + 0.02483 * b;
   double invalpha = 1.1239 + 1.1328 / (b - 3.4);
@@ -473,6 +474,7 @@ PLIS_HD double plis_poisson_d(plis_stream* st, double lam) {
     if (us >= 0.07 && V <= vr) return k;
     if (k < 0.0 || (us < 0.013 && V > us)) continue;
     double lhs = plis_log(V) + plis_log(invalpha) - plis_log(a / (us * us) + b);
+    if (loglam < 0.0) loglam = plis_log(lam);  // lambda >= 10: ln(lambda) > 2
     double rhs = -lam + k * loglam - plis_lnfact(k);
     if (lhs <= rhs) return k;
   }
