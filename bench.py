@@ -495,6 +495,9 @@ def configs_report():
     from pliscuda_b200 import Simulation, workloads
     out = {}
     m, st = workloads.small_ab(10)
+    with Simulation(m, mode="reference", precision="fp64", seed=SEED + 1) as sim:  # untimed: first-use costs
+        sim.set_state(st)
+        sim.run(10.0)
     with Simulation(m, mode="reference", precision="fp64", seed=SEED) as sim:
         sim.set_state(st)
         for t in range(1, 11):

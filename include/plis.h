@@ -104,7 +104,9 @@ typedef struct plis_options {
   int32_t max_rollbacks;      /* per step before PLIS_ERR_STUCK, default 64 */
   int32_t steps_per_launch;   /* steps captured per CUDA-graph launch, 0 = auto */
   int32_t tile[3];            /* lattice brick per CTA (x, y, z), 0 = auto */
-  int32_t persistent;         /* 1 = one cooperative persistent launch per run call, 0 = graph of phase kernels, -1 = auto */
+  int32_t persistent;         /* reserved, ignored by plis_create: a handle's step is always the graph of phase
+                               * kernels; the persistent cooperative launch is the batched form (plis_batch_*,
+                               * one replica or many) */
   int32_t profile;            /* 1 = launch phase kernels one by one with CUDA events around each (plis_get_profile) */
   int32_t stage_halo;         /* lattice leap: 1 = stage brick + halo in shared memory, 0 = global atomics (default) */
   int32_t learned_mlp;        /* learned tau MLP: 0 = tcgen05.mma with TMEM accumulators (default), 1 = mma.sync */
@@ -112,6 +114,12 @@ typedef struct plis_options {
                                * barrier of the persistent batched kernel (>= 32 ns per poll) and the mbarrier
                                * waits of the tcgen05 MLP; 0 = defaults (2^26 and 2^22 polls).  The reference
                                * has no device waits (its host loop synchronises, driver.cu:259-376). */
+  int32_t pooled_draws;       /* leap: 1 = channels of small mean (below 1/8) drawn as one pooled Poisson total
+                               * split over them, 0 = one draw per channel, -1 = auto (default: pooled for
+                               * networks of more than 4 reactions or 4 species).  Either way every channel's
+                               * firings are Poisson with its mean, independent of the others (leap.cu:20-53
+                               * draws one per channel); the two settings give different, equally valid
+                               * trajectories. */
 } plis_options;
 
 /* Per-kernel device time accumulated while plis_options.profile is set (CUDA events recorded on the

@@ -43,7 +43,7 @@ class _Model(ctypes.Structure):
 class _Opts(ctypes.Structure):
     _fields_ = [("mode", ctypes.c_int32), ("precision", ctypes.c_int32), ("critical_threshold", ctypes.c_int32),
                 ("max_rollbacks", ctypes.c_int32), ("epsilon", ctypes.c_double), ("seed", ctypes.c_uint64),
-                ("replica", ctypes.c_uint32), ("threads", ctypes.c_int32)]
+                ("replica", ctypes.c_uint32), ("threads", ctypes.c_int32), ("pooled_draws", ctypes.c_int32)]
 
 
 class Stats(ctypes.Structure):
@@ -114,7 +114,7 @@ class Oracle:
 
     def __init__(self, n, s, r, nbr, reactants, products, reaction_rates, diffusion_rates, *,
                  n_compartments=1, compartment=None, orig=None, mode=0, precision=0, seed=1, replica=0,
-                 critical_threshold=10, epsilon=0.05, max_rollbacks=64, threads=0):
+                 critical_threshold=10, epsilon=0.05, max_rollbacks=64, threads=0, pooled_draws=-1):
         self._keep = [np.ascontiguousarray(nbr, np.uint32),
                       None if orig is None else np.ascontiguousarray(orig, np.uint32),
                       np.ascontiguousarray(reactants, np.int32), np.ascontiguousarray(products, np.int32),
@@ -122,7 +122,8 @@ class Oracle:
                       None if compartment is None else np.ascontiguousarray(compartment, np.int32)]
         k = self._keep
         self._m = _Model(n, s, r, n_compartments, _p(k[0]), _p(k[1]), _p(k[2]), _p(k[3]), _p(k[4]), _p(k[5]), _p(k[6]))
-        self._o = _Opts(mode, precision, critical_threshold, max_rollbacks, epsilon, seed, replica, threads)
+        self._o = _Opts(mode, precision, critical_threshold, max_rollbacks, epsilon, seed, replica, threads,
+                        pooled_draws)
         self.n, self.s = n, s
         self._h = lib().oracle_create(ctypes.byref(self._m), ctypes.byref(self._o))
         if not self._h:

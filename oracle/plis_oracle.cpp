@@ -59,6 +59,8 @@ template <> struct RealOps<double> {
     return plis_poisson_inv_d(u[i], lam, em);
   }
   static double uniform(plis_stream* s) { return plis_uniform_d(s); }
+  static double word_uniform(uint32_t w) { return plis_u32_to_uniform_d(w); }
+  static double inv_word(uint32_t w, double lam) { return plis_poisson_inv_d(plis_u32_to_uniform_d(w), lam, plis_exp(-lam)); }
   static double inf() { return PLIS_INF_D; }
   static double fabs_(double x) { return fabs(x); }
 };
@@ -76,6 +78,8 @@ template <> struct RealOps<float> {
     return plis_poisson_inv_f(u[i], lam, em);
   }
   static float uniform(plis_stream* s) { return plis_uniform_f(s); }
+  static float word_uniform(uint32_t w) { return plis_u32_to_uniform_f(w); }
+  static double inv_word(uint32_t w, float lam) { return plis_poisson_inv_f(plis_u32_to_uniform_f(w), lam, plis_expf(-lam)); }
   static float inf() { return PLIS_INF_F; }
   static float fabs_(float x) { return fabsf(x); }
 };
@@ -406,6 +410,7 @@ struct Sim : Base {
     const int mode = opt.mode;
     const int nc = opt.critical_threshold;
     const Real tl = (Real)tau_leap;
+    const bool pool_on = opt.pooled_draws < 0 ? (R > 4 || S > 4) : opt.pooled_draws != 0;
     std::fill(own.begin(), own.end(), 0);
     std::fill(outk.begin(), outk.end(), 0);
     std::fill(leaped.begin(), leaped.end(), 0);
@@ -419,11 +424,24 @@ struct Sim : Base {
       if (logging) cell_log[c].clear();
       if (flag[c] == SSA || flag[c] == SSA_FF) continue;  // leap.cu:9-10
       uint8_t big = 0;
+      // pooled draws (plis_stream.h): channels of mean below PLIS_POOL_CUT join the pool, in walking
+      // order (reactions, then species), while its total stays at most PLIS_POOL_MAX
+      Real pool = (Real)0;
+      auto join = [](Real& acc, Real unit, Real w) {
+        if (!(unit < (Real)PLIS_POOL_CUT) || !(acc + w <= (Real)PLIS_POOL_MAX)) return false;
+        acc = acc + w;
+        return true;
+      };
+      auto reaction_mean = [&](uint32_t r) {
+        const Real a = rr_c[(size_t)r * N + c];
+        const bool fire = (mode == 0) ? !crit_ref(x, c, r) : ((a > (Real)0) && !crit_fix(x, c, r, a));
+        return fire ? tl * a : (Real)0;
+      };
+      const int n = ncount[c];
       for (uint32_t r = 0; r < R; ++r) {
-        Real a = rr_c[(size_t)r * N + c];
-        bool fire = (mode == 0) ? !crit_ref(x, c, r) : ((a > (Real)0) && !crit_fix(x, c, r, a));
-        if (!fire) continue;
-        const Real lam = tl * a;
+        const Real lam = reaction_mean(r);
+        if (!(lam > (Real)0)) continue;  // not leaped (critical), or a zero mean (a draw of 0)
+        if (pool_on && join(pool, lam, lam)) continue;
         int64_t k;
         if (lam > (Real)0 && lam < (Real)10) {  // inversion: uniform r % 4 of reaction group r / 4
           plis_stream g = plis_stream_make(opt.seed, opt.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_rgroup(r >> 2));
@@ -440,12 +458,12 @@ struct Sim : Base {
           own[(size_t)c * S + e.first] += v;
         }
       }
-      const int n = ncount[c];
       uint8_t mark = 0;
       for (uint32_t s = 0; s < S; ++s) {
         if (cnt(x, s, c) < nc) continue;  // is_critical_diffusion, tau.cu:42-45
         if (mode == 0 && n > 0) mark = 1;  // leap.cu:54-56 marks every receiver
         Real lam = tl * dr_c[(size_t)s * N + c];
+        if (pool_on && n > 0 && lam > (Real)0 && join(pool, lam, (Real)n * lam)) continue;
         Real em = Ops::emlam(lam);
         for (int j = 0; j < n; ++j) {
           int64_t k;
@@ -462,6 +480,47 @@ struct Sim : Base {
           outk[((size_t)c * S + s) * 6 + j] = k;
           own[(size_t)c * S + s] -= k;
           ev += k;
+        }
+      }
+      if (pool > (Real)0) {  // the pool's total by inversion, then one walk per event
+        const plis_stream g = plis_stream_make(opt.seed, opt.replica, c, PLIS_PHASE_LEAP, step, attempt, PLIS_CH_POOL);
+        const int64_t K = Ops::count(Ops::inv_word(plis_group_block(&g, 0).x, pool));
+        for (int64_t e = 0; e < K; ++e) {
+          const plis_u32x4 w = plis_group_block(&g, (uint32_t)(e + 1));
+          const Real target = Ops::word_uniform(w.x) * pool;
+          Real acc = (Real)0;
+          int pick_r = -1, pick_s = -1, last_r = -1, last_s = -1;
+          for (uint32_t r = 0; r < R && pick_r < 0; ++r) {
+            const Real lr = reaction_mean(r);
+            if (lr > (Real)0 && join(acc, lr, lr)) {
+              last_r = (int)r;
+              if (target < acc) pick_r = (int)r;
+            }
+          }
+          if (pick_r < 0) {
+            for (uint32_t s = 0; s < S && pick_s < 0; ++s) {
+              if (cnt(x, s, c) < nc || n == 0) continue;
+              const Real ls = tl * dr_c[(size_t)s * N + c];
+              if (ls > (Real)0 && join(acc, ls, (Real)n * ls)) {
+                last_s = (int)s;
+                if (target < acc) pick_s = (int)s;
+              }
+            }
+            if (pick_s < 0) {  // rounding left the target at the total: the last member
+              if (last_s >= 0) pick_s = last_s;
+              else pick_r = last_r;
+            }
+          }
+          ev += 1;
+          if (pick_r >= 0) {
+            if (logging) cell_log[c].push_back(event(st.time, step, attempt, c, c, 1, (uint32_t)pick_r, 1));
+            for (auto& ne : rx[pick_r].net) own[(size_t)c * S + ne.first] += ne.second;
+          } else {
+            const uint32_t j = plis_pool_slot(w.y, (uint32_t)n);
+            if (logging) cell_log[c].push_back(event(st.time, step, attempt, c, nbr[(size_t)c * 6 + j], 1, (uint32_t)pick_s, 2));
+            outk[((size_t)c * S + pick_s) * 6 + j] += 1;
+            own[(size_t)c * S + pick_s] -= 1;
+          }
         }
       }
       for (uint32_t s = 0; s < S; ++s) {

@@ -42,6 +42,7 @@ typedef struct oracle_options {
   uint64_t seed;
   uint32_t replica;
   int32_t threads;             // OpenMP threads, 0 = default
+  int32_t pooled_draws;        // 1 = pooled draws of small-mean leap channels, 0 = off, -1 = auto (> 4 reactions or species)
 } oracle_options;
 
 typedef struct oracle_stats {

@@ -129,7 +129,7 @@ class Simulation:
                  seed: int = 1, replica: int = 0, device: int = 0, critical_threshold: int = 10,
                  epsilon: float = 0.05, max_rollbacks: int = 64, steps_per_launch: int = 0,
                  tile: Optional[Sequence[int]] = None, profile: bool = False, stage_halo: bool = False,
-                 learned_mlp: str = "tcgen05", wait_polls: int = 0):
+                 learned_mlp: str = "tcgen05", wait_polls: int = 0, pooled_draws: int = -1):
         if isinstance(mode, str):
             mode = {"reference": MODE_REFERENCE, "corrected": MODE_CORRECTED}[mode]
         if isinstance(precision, str):
@@ -139,7 +139,8 @@ class Simulation:
         kw = dict(mode=mode, precision=precision, seed=seed, replica=replica, device=device,
                   critical_threshold=critical_threshold, epsilon=epsilon, max_rollbacks=max_rollbacks,
                   steps_per_launch=steps_per_launch, profile=int(bool(profile)), stage_halo=int(bool(stage_halo)),
-                  learned_mlp={"tcgen05": 0, "mma.sync": 1}[learned_mlp], wait_polls=int(wait_polls))
+                  learned_mlp={"tcgen05": 0, "mma.sync": 1}[learned_mlp], wait_polls=int(wait_polls),
+                  pooled_draws=int(pooled_draws))
         if tile is not None:
             kw["tile"] = tile
         self.options = _lib.default_options(**kw)

@@ -38,7 +38,7 @@ class Options(ctypes.Structure):
     _fields_ = [("size", u32), ("mode", i32), ("precision", i32), ("critical_threshold", i32),
                 ("epsilon", f64), ("seed", u64), ("replica", u32), ("device", i32), ("max_rollbacks", i32),
                 ("steps_per_launch", i32), ("tile", i32 * 3), ("persistent", i32), ("profile", i32),
-                ("stage_halo", i32), ("learned_mlp", i32), ("wait_polls", u64)]
+                ("stage_halo", i32), ("learned_mlp", i32), ("wait_polls", u64), ("pooled_draws", i32)]
 
 
 class Profile(ctypes.Structure):

@@ -27,7 +27,7 @@ class Batch:
                  diffusion_rates, *, replica_ids: Optional[Sequence[int]] = None, mode: int | str = 0,
                  precision: int | str = 0, seed: int = 1, device: int = 0, critical_threshold: int = 10,
                  epsilon: float = 0.05, max_rollbacks: int = 64, tile: Optional[Sequence[int]] = None,
-                 stage_halo: bool = False, wait_polls: int = 0):
+                 stage_halo: bool = False, wait_polls: int = 0, pooled_draws: int = -1):
         if isinstance(mode, str):
             mode = {"reference": 0, "corrected": 1}[mode]
         if isinstance(precision, str):
@@ -46,7 +46,7 @@ class Batch:
                            _c(k[5]))
         kw = dict(mode=mode, precision=precision, seed=seed, device=device, critical_threshold=critical_threshold,
                   epsilon=epsilon, max_rollbacks=max_rollbacks, stage_halo=int(bool(stage_halo)),
-                  wait_polls=int(wait_polls))
+                  wait_polls=int(wait_polls), pooled_draws=int(pooled_draws))
         if tile is not None:
             kw["tile"] = tile
         self.options = _lib.default_options(**kw)

@@ -214,6 +214,8 @@ int BatchEngine::create(const plis_batch_desc& d, const plis_options& opt) {
   dopt_.eps = opt.epsilon;
   dopt_.seed = opt.seed;
   dopt_.replica = 0;
+  dopt_.pool = pooled_draws_on(opt.pooled_draws, R_, S_);
+  if (dopt_.pool) small_ = false;  // pooled draws live in the generic leap only
 
   const size_t cells = (size_t)S_ * ntot_;
   for (int i = 0; i < 3; ++i)

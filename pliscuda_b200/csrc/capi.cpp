@@ -89,6 +89,7 @@ void plis_options_init(plis_options* o) {
   o->persistent = -1;
   o->stage_halo = 0;
   o->learned_mlp = 0;
+  o->pooled_draws = -1;
 }
 
 int plis_create(const plis_model_desc* model, const plis_options* opts, plis_handle** out) {
@@ -108,6 +109,7 @@ int plis_create(const plis_model_desc* model, const plis_options* opts, plis_han
     return PLIS_ERR_INVALID;
   }
   if (o.learned_mlp != PLIS_MLP_TCGEN05 && o.learned_mlp != PLIS_MLP_MMA_SYNC) { g_err = "unknown learned_mlp"; return PLIS_ERR_INVALID; }
+  if (o.pooled_draws < -1 || o.pooled_draws > 1) { g_err = "pooled_draws must be -1, 0 or 1"; return PLIS_ERR_INVALID; }
   plis::Model m;
   std::string err;
   int rc = plis::build_model(model, &m, &err);
@@ -363,6 +365,7 @@ int plis_batch_create(const plis_batch_desc* desc, const plis_options* opts, pli
   }
   if (o.mode != PLIS_MODE_REFERENCE && o.mode != PLIS_MODE_CORRECTED) { g_err = "unknown mode"; return PLIS_ERR_INVALID; }
   if (o.precision != PLIS_PREC_FP64 && o.precision != PLIS_PREC_FP32) { g_err = "unknown precision"; return PLIS_ERR_INVALID; }
+  if (o.pooled_draws < -1 || o.pooled_draws > 1) { g_err = "pooled_draws must be -1, 0 or 1"; return PLIS_ERR_INVALID; }
   if (o.critical_threshold < 0 || !(o.epsilon > 0.0) || o.max_rollbacks < 0 || o.max_rollbacks > 4000) {
     g_err = "critical_threshold, epsilon or max_rollbacks out of range";
     return PLIS_ERR_INVALID;

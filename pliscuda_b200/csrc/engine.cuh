@@ -44,7 +44,10 @@ struct Ctrl {
   double tau_min_plain;  // min of the plain taus of the current state
   double tau_step_plain; // the same clamped onto t_end
   uint32_t learned;      // 1: tau_min is the min of proposed taus
-  uint32_t pad2_;
+  // the subvolumes whose delta rows the exact events of the attempt wrote, listed after the S x Npad
+  // deltas (D + S * Npad, N entries); past N entries the list is incomplete and k_apply scans all
+  uint32_t touched_on;   // 1: the delta buffer holds the list (single-replica handles)
+  uint32_t n_touched;
 };
 
 struct DevModel {
@@ -117,6 +120,7 @@ struct DevOpts {
   double eps;
   unsigned long long seed;
   uint32_t replica;
+  uint32_t pool;      // 1: pooled draws of small-mean channels in the generic leap (plis_stream.h)
 };
 
 // Division by a divisor fixed at set-up, as one multiply-high, two adds and two shifts: exact for
@@ -160,6 +164,11 @@ inline void geo_divisors(Geo& g) {
 // memory for every subvolume.  The values are those of the DevModel tables (same propensities, same
 // criticality, same order of summation).
 constexpr int kSmallR = 4, kSmallS = 4;
+// plis_options.pooled_draws resolved: auto (-1) pools the networks too large for the small-model tables
+inline uint32_t pooled_draws_on(int32_t setting, uint32_t R, uint32_t S) {
+  if (setting < 0) return (R > (uint32_t)kSmallR || S > (uint32_t)kSmallS) ? 1u : 0u;
+  return setting != 0 ? 1u : 0u;
+}
 struct SmallModel {
   uint32_t on;                   // 1: the model fits and the tables below are filled
   uint8_t nreac[kSmallR];        // distinct reactant species of reaction r
@@ -181,6 +190,7 @@ struct SmallModel {
 // streams, neighbour counts and the arg-min tie rule are those of a single domain; the kernels touch
 // only the slab, and the host exchanges the layers next to its faces (the ghost layers z0-1 and z1)
 // with the neighbouring slabs and gathers every slab's summary.
+constexpr uint32_t kExactChunk = 1024;  // subvolumes whose flags one k_exact CTA scans per round
 constexpr int kSlabRemote = 64;  // flag writes of one attempt that land outside the slab and its ghosts
 struct SlabSummary {             // one rank's reduction of its slab's classification
   double tau;                    // min tau over the slab

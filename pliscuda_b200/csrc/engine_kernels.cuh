@@ -95,6 +95,11 @@ template <> struct RT<double> {
   static __device__ __forceinline__ double uniform(plis_stream* s) { return plis_uniform_d(s); }
   static __device__ __forceinline__ long long count(double k) { return plis_count_d(k); }
   static __device__ __forceinline__ double inf() { return PLIS_INF_D; }
+  // a 32-bit word of a group block as a uniform, and a Poisson(lam < 10) draw by inversion from it
+  static __device__ __forceinline__ double word_uniform(uint32_t w) { return plis_u32_to_uniform_d(w); }
+  static __device__ __forceinline__ double inv_word(uint32_t w, double lam) {
+    return plis_poisson_inv_d(plis_u32_to_uniform_d(w), lam, plis_exp(-lam));
+  }
 };
 template <> struct RT<float> {
   static __device__ __forceinline__ double poisson(plis_stream* s, float lam) { return plis_poisson_f(s, lam); }
@@ -106,6 +111,10 @@ template <> struct RT<float> {
   static __device__ __forceinline__ float uniform(plis_stream* s) { return plis_uniform_f(s); }
   static __device__ __forceinline__ long long count(double k) { return plis_count_d(k); }
   static __device__ __forceinline__ float inf() { return PLIS_INF_F; }
+  static __device__ __forceinline__ float word_uniform(uint32_t w) { return plis_u32_to_uniform_f(w); }
+  static __device__ __forceinline__ double inv_word(uint32_t w, float lam) {
+    return plis_poisson_inv_f(plis_u32_to_uniform_f(w), lam, plis_expf(-lam));
+  }
 };
 
 // Per-neighbour diffusion draws of one species (leap.cu:49-53).  All n draws have the same mean, so
@@ -1033,6 +1042,15 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
     if (f == F_LEAP_CR || f == F_LEAP_NOCR) {  // leap.cu:9-10
       const int comp = SM ? 0 : comp_of(m, c);
       const int S = (int)m.S, R = (int)m.R;
+      // pooled draws (plis_stream.h): the running total of the pool and the membership rule, the
+      // same in the walk that fills the pool and in the walks that place its events
+      const bool pool_on = !SM && A.o.pool != 0;
+      Real pool = (Real)0;
+      auto pool_join = [](Real& acc, Real unit, Real w) -> bool {
+        if (!(unit < (Real)PLIS_POOL_CUT) || !(acc + w <= (Real)PLIS_POOL_MAX)) return false;
+        acc = acc + w;
+        return true;
+      };
       auto reaction_group = [&](const int r0) {
         // reactions r0..r0+3: means >= 10 go through PTRS one by one, the rest in lockstep
         Real u[4], lam[4];
@@ -1057,6 +1075,7 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
               fire = (mode == 0) ? !crit_ref(m, x, r, nc) : ((a > (Real)0) && !crit_fix(m, x, r, a, nc));
             }
             lam[i] = fire ? tl * a : (Real)0;
+            if (pool_on && lam[i] > (Real)0 && pool_join(pool, lam[i], lam[i])) lam[i] = (Real)0;  // pooled
             if (lam[i] > (Real)0) {
               if (lam[i] < (Real)10) {
                 act[i] = true;  // inversion search: its single uniform comes from the group's blocks
@@ -1126,28 +1145,31 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
       else nbr_info(m, cl, q);
       const int n = q.n;
       bool mark = false;
+      auto jump = [&](int s, long long k, uint32_t b, int dir) {
+        if (k >= kBigJump) big = 1;
+        if (k > 0) {
+          if (box.acc) atomicAdd_block(&box.acc[s * box.size + own + box_offset(box, dir)], (int)k);
+          else atomicAdd(&Xt[(size_t)s * m.Npad + b], (int)k);
+          if (mode == 1 && !L.ff_free && flag[b] == F_SSA_FF) flag[b] = F_SSA;
+          if (LOG) ev_put(A.b.ev, L.t, step, attempt, c, b, k, s, PLIS_EVENT_LEAP_DIFFUSION);
+        }
+      };
+      auto species_lam = [&](const int s) -> Real {
+        Real dr;
+        if constexpr (SM) dr = sm_drate<Real>(A.sm, s);
+        else dr = drate<Real>(m, comp, s);
+        return tl * (dr * (Real)x.get(s));
+      };
       auto species_jumps = [&](const int s) {
         const int32_t xs = x.get(s);
         if (xs < nc) return;  // is_critical_diffusion, tau.cu:42-45
         if (mode == 0 && n > 0) mark = true;
-        Real dr;
-        if constexpr (SM) dr = sm_drate<Real>(A.sm, s);
-        else dr = drate<Real>(m, comp, s);
-        const Real lam = tl * (dr * (Real)xs);
+        const Real lam = species_lam(s);
+        if (pool_on && n > 0 && lam > (Real)0 && pool_join(pool, lam, (Real)n * lam)) return;  // pooled
         const Real em = RT<Real>::emlam(lam);  // one exp for the n draws of this species
         int32_t kd[6];
         diffusion_draws<Real>(A, c, s, n, lam, em, step, attempt, kd);
         long long out = 0;
-        auto jump = [&](long long k, uint32_t b, int dir) {
-          if (k >= kBigJump) big = 1;
-          if (k > 0) {
-            if (box.acc) atomicAdd_block(&box.acc[s * box.size + own + box_offset(box, dir)], (int)k);
-            else atomicAdd(&Xt[(size_t)s * m.Npad + b], (int)k);
-            if (mode == 1 && !L.ff_free && flag[b] == F_SSA_FF) flag[b] = F_SSA;
-            if (LOG) ev_put(A.b.ev, L.t, step, attempt, c, b, k, s, PLIS_EVENT_LEAP_DIFFUSION);
-          }
-          out += k;
-        };
         if (WALK && q.lat) {  // slot j is the j-th present direction; kd is read by constant index only
           int j = 0;
 #pragma unroll
@@ -1160,16 +1182,21 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
             for (int i = 1; i < 6; ++i)
               if (j == i) k = kd[i];
             ++j;
-            jump(k, b, d);
+            jump(s, k, b, d);
+            out += k;
           }
         } else if constexpr (WALK) {
 #pragma unroll
           for (int j = 0; j < 6; ++j) {
             if (j >= n) break;
-            jump(kd[j], q.nb[j], 0);
+            jump(s, kd[j], q.nb[j], 0);
+            out += kd[j];
           }
         } else {
-          for (int j = 0; j < n; ++j) jump(kd[j], q.nb[j], q.dir[j]);
+          for (int j = 0; j < n; ++j) {
+            jump(s, kd[j], q.nb[j], q.dir[j]);
+            out += kd[j];
+          }
         }
         dl.add(s, -out);
         ev += out;
@@ -1180,6 +1207,73 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
           if (s < S) species_jumps(s);
       } else {
         for (int s = 0; s < S; ++s) species_jumps(s);
+      }
+      if constexpr (!SM) {
+        if (pool > (Real)0) {  // the pool's events: total by inversion, then one walk per event
+          const plis_stream g =
+              plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_LEAP, step, attempt, PLIS_CH_POOL);
+          const long long K = RT<Real>::count(RT<Real>::inv_word(plis_group_block(&g, 0).x, pool));
+          for (long long e = 0; e < K; ++e) {
+            const plis_u32x4 w = plis_group_block(&g, (uint32_t)(e + 1));
+            const Real target = RT<Real>::word_uniform(w.x) * pool;
+            Real acc = (Real)0;
+            int pick_r = -1, pick_s = -1, last_r = -1, last_s = -1;
+            for (int r = 0; r < R && pick_r < 0; ++r) {
+              const Real a = prop<Real>(m, x, r, comp);
+              const bool fire = (mode == 0) ? !crit_ref(m, x, r, nc) : ((a > (Real)0) && !crit_fix(m, x, r, a, nc));
+              const Real lr = fire ? tl * a : (Real)0;
+              if (lr > (Real)0 && pool_join(acc, lr, lr)) {
+                last_r = r;
+                if (target < acc) pick_r = r;
+              }
+            }
+            if (pick_r < 0) {
+              for (int s = 0; s < S; ++s) {
+                if (x.get(s) < nc || n == 0) continue;
+                const Real ls = species_lam(s);
+                if (ls > (Real)0 && pool_join(acc, ls, (Real)n * ls)) {
+                  last_s = s;
+                  if (target < acc) {
+                    pick_s = s;
+                    break;
+                  }
+                }
+              }
+              if (pick_s < 0) {  // rounding left the target at the total: the last member
+                if (last_s >= 0) pick_s = last_s;
+                else pick_r = last_r;
+              }
+            }
+            ev += 1;
+            if (pick_r >= 0) {
+              if (LOG) ev_put(A.b.ev, L.t, step, attempt, c, c, 1, pick_r, PLIS_EVENT_LEAP_REACTION);
+              const int nn = m.n_net[pick_r];
+              for (int i = 0; i < nn; ++i) dl.add(m.net_s[pick_r * 8 + i], (long long)m.net_nu[pick_r * 8 + i]);
+            } else {
+              const int j = (int)plis_pool_slot(w.y, (uint32_t)n);
+              uint32_t b = c;
+              int dir = 0;
+              if (WALK && q.lat) {
+                int jj = 0;
+                for (int d = 0; d < 6; ++d) {
+                  uint32_t bd;
+                  int nb_n;
+                  if (!nbr_dir(m, q, d, bd, nb_n)) continue;
+                  if (jj == j) {
+                    b = bd;
+                    dir = d;
+                  }
+                  ++jj;
+                }
+              } else {
+                b = q.nb[j];
+                if constexpr (!WALK) dir = q.dir[j];
+              }
+              jump(pick_s, 1, b, dir);
+              dl.add(pick_s, -1);
+            }
+          }
+        }
       }
       if (mark && !L.ff_free) {  // leap.cu:54-56: every receiver leaves fast-forward
         auto leave_ff = [&](uint32_t b, int) {
@@ -1282,6 +1376,17 @@ __global__ void __launch_bounds__(256, PLIS_LEAP_MIN_BLOCKS) k_leap(KArgs A) {
 // ------------------------------------------------------------------------------------------------
 // exact events
 // ------------------------------------------------------------------------------------------------
+// A subvolume whose delta row an exact event wrote: k_apply adds only the listed rows.
+__device__ __forceinline__ uint32_t* touched_list(const KArgs& A) {
+  return reinterpret_cast<uint32_t*>(A.b.D + (size_t)A.m.S * A.m.Npad);
+}
+__device__ __forceinline__ void touch(const KArgs& A, uint32_t c) {
+  Ctrl* K = A.b.ctrl;
+  if (!K->touched_on) return;
+  const uint32_t i = atomicAdd(&K->n_touched, 1u);
+  if (i < A.m.N) touched_list(A)[i] = c;
+}
+
 // Reference critical event of one LEAP_CR subvolume (leap.cu:86-199).
 template <typename Real, bool LOG, int MAXS>
 __device__ int critical_event_ref(const KArgs& A, uint32_t c, const Counts<MAXS>& x, const int32_t* Xt,
@@ -1321,6 +1426,7 @@ __device__ int critical_event_ref(const KArgs& A, uint32_t c, const Counts<MAXS>
     if (!fire) return 0;
     for (int i = 0; i < m.n_net[ri]; ++i)
       atomicAdd(&D[(size_t)m.net_s[ri * 8 + i] * m.Npad + c], (int)m.net_nu[ri * 8 + i]);
+    touch(A, c);
     if (LOG) ev_put(A.b.ev, A.b.ctrl->t, step, attempt, c, c, 1, ri, PLIS_EVENT_CRITICAL_REACTION);
     return 1;
   }
@@ -1346,6 +1452,8 @@ __device__ int critical_event_ref(const KArgs& A, uint32_t c, const Counts<MAXS>
   if (target == c) return 0;
   atomicAdd(&D[(size_t)spi * m.Npad + c], -1);
   atomicAdd(&D[(size_t)spi * m.Npad + target], 1);
+  touch(A, c);
+  touch(A, target);
   const uint32_t q = flat_table_entry(m, target);  // leap.cu:192-193
   if (!A.sl.on || (q + A.sl.has_lo * A.sl.layer >= A.sl.lo && q < A.sl.hi + A.sl.has_hi * A.sl.layer)) {
     if (flag[q] == F_SSA_FF) flag[q] = F_SSA;
@@ -1386,6 +1494,7 @@ __device__ int argmin_event(const KArgs& A, uint32_t mcell, const Counts<MAXS>& 
       if (ri < 0) ri = 0;
       for (int i = 0; i < m.n_net[ri]; ++i)
         atomicAdd(&dst[(size_t)m.net_s[ri * 8 + i] * m.Npad + mcell], (int)m.net_nu[ri * 8 + i]);
+      if (dst == A.b.D) touch(A, mcell);
       flag[mcell] = F_SSA;  // ssa.cu:295
       if (LOG) ev_put(A.b.ev, A.b.ctrl->t, step, attempt, mcell, mcell, 1, ri, PLIS_EVENT_SSA_REACTION);
       return 1;
@@ -1408,6 +1517,10 @@ __device__ int argmin_event(const KArgs& A, uint32_t mcell, const Counts<MAXS>& 
     if (target == mcell) return 0;
     atomicAdd(&dst[(size_t)spi * m.Npad + mcell], -1);
     atomicAdd(&dst[(size_t)spi * m.Npad + target], 1);
+    if (dst == A.b.D) {
+      touch(A, mcell);
+      touch(A, target);
+    }
     if (flag[target] == F_SSA_FF) flag[target] = F_SSA;
     if (LOG) ev_put(A.b.ev, A.b.ctrl->t, step, attempt, mcell, target, 1, spi, PLIS_EVENT_SSA_DIFFUSION);
     return 1;
@@ -1449,6 +1562,7 @@ __device__ int argmin_event(const KArgs& A, uint32_t mcell, const Counts<MAXS>& 
   if (chosen_r >= 0) {
     for (int i = 0; i < m.n_net[chosen_r]; ++i)
       atomicAdd(&dst[(size_t)m.net_s[chosen_r * 8 + i] * m.Npad + mcell], (int)m.net_nu[chosen_r * 8 + i]);
+    if (dst == A.b.D) touch(A, mcell);
     if (LOG) ev_put(A.b.ev, A.b.ctrl->t, step, attempt, mcell, mcell, 1, chosen_r, kind_r);
     return 1;
   }
@@ -1459,6 +1573,10 @@ __device__ int argmin_event(const KArgs& A, uint32_t mcell, const Counts<MAXS>& 
   const uint32_t target = nb[slot];
   atomicAdd(&dst[(size_t)chosen_s * m.Npad + mcell], -1);
   atomicAdd(&dst[(size_t)chosen_s * m.Npad + target], 1);
+  if (dst == A.b.D) {
+    touch(A, mcell);
+    touch(A, target);
+  }
   if (flag[target] == F_SSA_FF) flag[target] = F_SSA;
   if (LOG) ev_put(A.b.ev, A.b.ctrl->t, step, attempt, mcell, target, 1, chosen_s, kind_r + 1);
   return 1;
@@ -1479,12 +1597,34 @@ __global__ void __launch_bounds__(256) k_exact(KArgs A) {
   const uint32_t attempt = K->attempt;
   int fired = 0;
   const uint32_t c_lo = A.sl.on ? A.sl.lo : 0u, c_hi = A.sl.on ? A.sl.hi : m.N;  // a z-slab: its own subvolumes
-  if (ex & 1u) {  // reference: every LEAP_CR subvolume (grid-stride: the grid is a few CTAs per SM)
-    for (uint32_t c = c_lo + blockIdx.x * blockDim.x + threadIdx.x; c < c_hi; c += gridDim.x * blockDim.x) {
-      if (flag[c] != F_LEAP_CR) continue;
-      Counts<MAXS> x;
-      load_counts(m, Xc, c, x);
-      fired += critical_event_ref<Real, LOG>(A, c, x, Xt, step, attempt, A.b.D, flag);
+  if (ex & 1u) {
+    // reference: every LEAP_CR subvolume.  A CTA scans a chunk of flags, gathers the chunk's LEAP_CR
+    // subvolumes in shared memory and fires them on consecutive threads: a few per cent of the
+    // subvolumes are LEAP_CR, and a strided scan would run each event on one lane of its warp.
+    __shared__ uint32_t s_cell[kExactChunk];
+    __shared__ uint32_t s_n;
+    const unsigned lane = threadIdx.x & 31u;
+    for (uint32_t base = c_lo + blockIdx.x * kExactChunk; base < c_hi; base += gridDim.x * kExactChunk) {
+      if (threadIdx.x == 0) s_n = 0;
+      __syncthreads();
+      for (uint32_t i = threadIdx.x; i < kExactChunk; i += blockDim.x) {  // blockDim.x divides the chunk
+        const uint32_t c = base + i;
+        const bool cr = c < c_hi && flag[c] == F_LEAP_CR;
+        const unsigned mask = __ballot_sync(0xffffffffu, cr);
+        unsigned pos = 0;
+        if (lane == 0 && mask) pos = atomicAdd(&s_n, (unsigned)__popc(mask));
+        pos = __shfl_sync(0xffffffffu, pos, 0);
+        if (cr) s_cell[pos + __popc(mask & ((1u << lane) - 1u))] = c;
+      }
+      __syncthreads();
+      const uint32_t n = s_n;
+      for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
+        const uint32_t c = s_cell[j];
+        Counts<MAXS> x;
+        load_counts(m, Xc, c, x);
+        fired += critical_event_ref<Real, LOG>(A, c, x, Xt, step, attempt, A.b.D, flag);
+      }
+      __syncthreads();
     }
   }
   if ((ex & 2u) && blockIdx.x == 0 && threadIdx.x == 0 && (uint32_t)K->argmin >= c_lo && (uint32_t)K->argmin < c_hi) {
@@ -1514,6 +1654,19 @@ __global__ void __launch_bounds__(256) k_apply(KArgs A) {
   const DevModel& m = A.m;
   int32_t* Xt = A.b.X[K->tgt];
   // a z-slab: its subvolumes and the ghost layers next to its faces (deltas of events that cross a face)
+  const uint32_t nt = K->touched_on ? K->n_touched : ~0u;
+  if (nt <= m.N) {  // the listed rows (a row listed twice: the second finds zeros)
+    const uint32_t* list = touched_list(A);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += gridDim.x * blockDim.x) {
+      const uint32_t c = list[i];
+      for (uint32_t s = 0; s < m.S; ++s) {
+        const size_t j = (size_t)s * m.Npad + c;
+        const int32_t v = atomicExch(&A.b.D[j], 0);
+        if (v) atomicAdd(&Xt[j], v);
+      }
+    }
+    return;
+  }
   const uint32_t c_lo = A.sl.on ? A.sl.lo - A.sl.has_lo * A.sl.layer : 0u;
   const uint32_t c_hi = A.sl.on ? A.sl.hi + A.sl.has_hi * A.sl.layer : m.N;
   for (uint32_t c = c_lo + blockIdx.x * blockDim.x + threadIdx.x; c < c_hi; c += gridDim.x * blockDim.x) {
@@ -1751,6 +1904,7 @@ template <typename Real, int MAXS, bool CACHE, bool SM>
 __global__ void __launch_bounds__(256, PLIS_CLASSIFY_MIN_BLOCKS) k_classify(KArgs A) {
   extern __shared__ __align__(16) unsigned char s_prop[];  // CACHE: R x blockDim propensities
   pdl_entry();
+  if (blockIdx.x == 0 && threadIdx.x == 0) A.b.ctrl->n_touched = 0;  // k_apply has consumed the list
   Ctrl* K = A.b.ctrl;
   if (K->done) return;
   const ClassifyCtx C = classify_ctx(A, K);

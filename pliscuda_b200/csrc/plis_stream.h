@@ -155,6 +155,21 @@ PLIS_HD uint32_t plis_ch_diff(uint32_t s, uint32_t slot) { return PLIS_CH_DIFF_B
 PLIS_HD uint32_t plis_ch_rgroup(uint32_t g) { return PLIS_CH_RGROUP_BASE + g; }
 PLIS_HD uint32_t plis_ch_dgroup(uint32_t s) { return PLIS_CH_DGROUP_BASE + s; }
 
+// Pooled draws.  A leap of a network with many channels, most of them with tiny means, draws the
+// channels of small mean together: walking the reactions (in order) and then the diffusing species
+// (in order), a channel whose mean is below PLIS_POOL_CUT joins the pool while the pool's total mean
+// stays at most PLIS_POOL_MAX (a species joins with its n neighbour slots, weight n * mean).  The
+// pool's total K ~ Poisson(total) comes by inversion from word x of block 0 of the pool channel;
+// event e (0-based) takes block e + 1: word x picks the channel with probability weight / total
+// (cumulative weights in walking order), word y the neighbour slot of a diffusion event,
+// slot = (y * n) >> 32.  Given K the channel counts are multinomial, so every pooled channel's count
+// is Poisson(mean) and independent of the others, as a draw per channel would be (Poisson splitting;
+// up to the 2^-32 resolution of the choices).  The other channels draw as before.
+#define PLIS_CH_POOL 0x7FFFFu
+#define PLIS_POOL_CUT 0.125
+#define PLIS_POOL_MAX 1.0
+PLIS_HD uint32_t plis_pool_slot(uint32_t y, uint32_t n) { return (uint32_t)(((uint64_t)y * (uint64_t)n) >> 32); }
+
 typedef struct plis_stream {
   plis_u32x4 ctr;
   uint32_t k0, k1;

@@ -76,6 +76,20 @@ def random_graph_model(n=200, seed=0, S=3):
     return m, state
 
 
+def birth_death_model(side=16, seed=1):
+    """5 species at counts ~ Poisson(20): births (k=20), deaths (k=1), two slow bimolecular reactions,
+    jump rates 0.02 .. 0.4.  Cao's tau puts every leap channel's mean below the pool cut, so the
+    leaps go through the pooled draws (12 reactions: pooled by default)."""
+    from pliscuda_b200 import workloads
+    S = 5
+    reactions = ([({}, {i: 1}) for i in range(S)] + [({i: 1}, {}) for i in range(S)]
+                 + [({0: 1, 1: 1}, {2: 1}), ({3: 1, 4: 1}, {})])
+    model = workloads._model((side,) * 3, S, reactions, [20.0] * S + [1.0] * S + [0.001, 0.002],
+                             [0.02, 0.05, 0.1, 0.2, 0.4])
+    state = np.random.default_rng(seed).poisson(20, S * model.n_subvolumes).astype(np.uint32)
+    return model, state
+
+
 def bits(a: np.ndarray) -> np.ndarray:
     return np.ascontiguousarray(a, np.float64).view(np.int64)
 

@@ -22,9 +22,9 @@ def _replicas(n=6, seed=3):
     return out
 
 
-def _oracle(model, state, r, mode, precision, seed):
+def _oracle(model, state, r, mode, precision, seed, pooled_draws=-1):
     from oracle.oracle import Oracle
-    o = Oracle.from_model(model, mode=mode, precision=precision, seed=seed, replica=r)
+    o = Oracle.from_model(model, mode=mode, precision=precision, seed=seed, replica=r, pooled_draws=pooled_draws)
     o.set_state(state)
     return o
 
@@ -152,3 +152,25 @@ def test_batch_proposer_with_unit_clamp_is_the_plain_batch():
             out.append([(b.get_state(r).copy(), b.stats(r).steps, b.stats(r).events) for r in range(len(reps))])
     for (x0, s0, e0), (x1, s1, e1) in zip(*out):
         assert np.array_equal(x0, x1) and s0 == s1 and e0 == e1
+
+
+@pytest.mark.parametrize("mode", [0, 1], ids=["ref", "corr"])
+def test_batch_pooled_draws_match_oracle(mode):
+    """Pooled leap draws forced on (the generic batched kernel): every replica bit-exact."""
+    from pliscuda_b200.batch import Batch
+    reps = _replicas()
+    with Batch.from_models([m for m, _ in reps], mode=mode, seed=4, pooled_draws=1) as b:
+        for r, (m, st) in enumerate(reps):
+            b.set_state(r, st)
+        orcs = [_oracle(m, st, r, mode, 0, 4, pooled_draws=1) for r, (m, st) in enumerate(reps)]
+        for k in range(3):
+            b.step(2)
+            for r, o in enumerate(orcs):
+                o.step(2)
+                _same(b, r, o, f"step {2 * (k + 1)}")
+        b.run(0.5)
+        for r, o in enumerate(orcs):
+            o.run(0.5)
+            _same(b, r, o, "t = 0.5")
+        for o in orcs:
+            o.close()

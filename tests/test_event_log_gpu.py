@@ -5,7 +5,7 @@ in no particular order).  The reference prints these events under LOG (PLISCuda/
 import numpy as np
 import pytest
 
-from helpers import assert_same, random_graph_model, ref_fixture
+from helpers import assert_same, birth_death_model, random_graph_model, ref_fixture
 
 pytestmark = pytest.mark.gpu
 
@@ -18,6 +18,7 @@ def _cases():
     yield "diff64", lambda: ref_fixture("test_diff-64")[:2], 0.2, {}
     yield "randgraph", lambda: random_graph_model(), 0.5, {}        # explicit neighbour table
     yield "schlogl8_eps1", lambda: workloads.schlogl(8), 0.3, {"epsilon": 1.0}  # rollbacks
+    yield "birthdeath8", lambda: birth_death_model(8), 0.05, {}        # pooled reaction and diffusion draws
 
 
 CASES = list(_cases())

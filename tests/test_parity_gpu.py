@@ -4,7 +4,7 @@ and over whole runs (the latter through the CUDA-graph batches)."""
 import numpy as np
 import pytest
 
-from helpers import assert_same, chain_model, random_graph_model, ref_fixture
+from helpers import assert_same, birth_death_model, chain_model, random_graph_model, ref_fixture
 
 pytestmark = pytest.mark.gpu
 
@@ -13,7 +13,8 @@ def _pair(model, state, mode, precision, seed=11, epsilon=0.05, **kw):
     from oracle.oracle import Oracle
     from pliscuda_b200 import Simulation
     sim = Simulation(model, mode=mode, precision=precision, seed=seed, epsilon=epsilon, **kw)
-    orc = Oracle.from_model(model, mode=mode, precision=precision, seed=seed, epsilon=epsilon)
+    orc = Oracle.from_model(model, mode=mode, precision=precision, seed=seed, epsilon=epsilon,
+                            pooled_draws=kw.get("pooled_draws", -1))
     sim.set_state(state)
     orc.set_state(state)
     return sim, orc
@@ -33,6 +34,12 @@ def _cases():
     yield "network10", lambda: workloads.random_network(5), None, 300, {}            # S=10, stiff: step-bounded
     yield "schlogl8_eps1", lambda: workloads.schlogl(8), 0.3, 10**6, {"epsilon": 1.0}      # rollbacks
     yield "react9_eps3", lambda: ref_fixture("test_react-9")[:2], 8.0, 10**6, {"epsilon": 3.0}
+    # pooled leap draws: the default for networks of more than 4 reactions or species, forced on
+    # small networks (generic kernels) and off on a large one (one draw per channel)
+    yield "birthdeath12", lambda: birth_death_model(12), 0.05, 10**6, {}
+    yield "network10_perchannel", lambda: workloads.random_network(5), None, 300, {"pooled_draws": 0}
+    yield "schlogl8_pooled", lambda: workloads.schlogl(8), 0.5, 10**6, {"pooled_draws": 1}
+    yield "small_ab6_pooled", lambda: workloads.small_ab(6, seed=4), 1.0, 10**6, {"pooled_draws": 1}
 
 
 CASES = list(_cases())
