@@ -65,15 +65,15 @@ def _peaks():
 
 # dram__bytes_read.sum + dram__bytes_write.sum per launch of the dominant kernel, from the committed
 # ncu capture of the same kernel on the same workload (profiles/k_leap_schlogl64.md: 2.44 MB read,
-# 0.01 MB written per launch under ncu's cache flush).  Keyed by (workload, semantics, precision, kernel); absent
+# 0.02 MB written per launch under ncu's cache flush).  Keyed by (workload, semantics, precision, kernel); absent
 # keys report null.
-NCU_TRAFFIC = {("schlogl64", "reference", "fp64", "leap"): (2.437632e6 + 0.010752e6, "profiles/k_leap_schlogl64.md")}
+NCU_TRAFFIC = {("schlogl64", "reference", "fp64", "leap"): (2.439936e6 + 0.021504e6, "profiles/k_leap_schlogl64.md")}
 # smsp__inst_executed.sum per launch (warp instructions) of the same capture.  The kernel is bound by
 # instruction issue and dependent latency, not by DRAM, so the line also reports the achieved warp-
 # instruction rate against the issue peak (148 SMs x 4 schedulers x the SM clock sampled during the
-# timed region).  The count is that of steps 41-43 from the initial state; later steps of the bench
+# timed region).  The count is that of step 41 from the initial state; later steps of the bench
 # trajectory draw from similar Poisson means, so the rate is an estimate.
-NCU_WARP_INSTR = {("schlogl64", "reference", "fp64", "leap"): (23.54e6, "profiles/k_leap_schlogl64.md")}
+NCU_WARP_INSTR = {("schlogl64", "reference", "fp64", "leap"): (22.557566e6, "profiles/k_leap_schlogl64.md")}
 SM_COUNT, SCHEDULERS_PER_SM = 148, 4
 
 def issue_roofline(instr, ms_launch, clocks):
@@ -364,8 +364,7 @@ def learned_report():
     rollbacks among all attempts.  The batched form (the persistent kernel) runs the same comparison
     with the chosen proposer: plain batch against learned batch, KS against the plain run."""
     from pliscuda_b200 import workloads
-    from pliscuda_b200.learned import (_ks_per_checkpoint, _moment_z_per_checkpoint, _run_to_checkpoints, calibrate,
-                                       train_proposer)
+    from pliscuda_b200.learned import _ks_per_checkpoint, _moments_per_checkpoint, _run_to_checkpoints, calibrate, train_proposer
     m64, s64 = workloads.schlogl(64)
     cands, training = [], []
     for eps_l in (0.4, 0.8, 1.6):
@@ -387,12 +386,22 @@ def learned_report():
     w, s_max, tag = cands[best]
     ls, lt = _run_to_checkpoints(m128, s128, cps, seed=12, precision="fp64", device=0, weights=w, s_max=s_max)
     ks = _ks_per_checkpoint(ps, ls)
-    zs = _moment_z_per_checkpoint(ps, ls)
     lt.update(tag)
     out.update({"learned": lt, "ks": [round(k, 5) for k in ks], "ks_max": max(ks), "ks_bound": 0.02,
-                "z_mean": [round(z[0], 3) for z in zs], "z_var": [round(z[1], 3) for z in zs],
+                **_moment_lists(_moments_per_checkpoint(ps, ls)),
                 "speedup_events_per_s": lt["events_per_s"] / pt["events_per_s"],
                 "speedup_sim_time_per_s": lt["sim_time_per_s"] / pt["sim_time_per_s"]})
+    # the most conservative admissible candidate (smallest clamp, then smallest label tolerance) on the
+    # same workload: the other end of the speed / fidelity trade-off
+    adm = [i for i, r in enumerate(cal["candidates"]) if r["admissible"]]
+    ic = min(adm, key=lambda i: (cands[i][1], cands[i][2]["label_epsilon"]))
+    if ic != best:
+        wc, s_c, tag_c = cands[ic]
+        cs, ct = _run_to_checkpoints(m128, s128, cps, seed=15, precision="fp64", device=0, weights=wc, s_max=s_c)
+        ksc = _ks_per_checkpoint(ps, cs)
+        ct.update(tag_c)
+        out["learned_conservative"] = {"learned": ct, "ks_max": max(ksc), **_moment_lists(_moments_per_checkpoint(ps, cs)),
+                                       "speedup_events_per_s": ct["events_per_s"] / pt["events_per_s"]}
     # the batched form (the persistent kernel, MLP by mma.sync) on the same workload: plain and learned
     pbs, pb = _batch_to_checkpoints(m128, s128, cps, seed=13)
     lbs, lb = _batch_to_checkpoints(m128, s128, cps, seed=14, weights=w, s_max=s_max)
@@ -400,7 +409,20 @@ def learned_report():
     out["batched_form"] = {"plain": pb, "learned": lb, "ks_max_vs_plain": max(ksb),
                            "speedup_events_per_s": lb["events_per_s"] / pb["events_per_s"],
                            "learned_vs_plain_multi_kernel": lb["events_per_s"] / pt["events_per_s"]}
+    # the same statistics between two plain runs (seeds 11 and 13; the batched plain run is the plain
+    # method bit for bit): the scale of KS and z that independent plain trajectories show on this
+    # lattice, against which the learned run's figures above are read
+    ks0 = _ks_per_checkpoint(ps, pbs)
+    out["plain_vs_plain"] = {"seeds": [11, 13], "ks": [round(k, 5) for k in ks0], "ks_max": max(ks0),
+                             **_moment_lists(_moments_per_checkpoint(ps, pbs))}
     return out
+
+
+def _moment_lists(ms):
+    """Per-checkpoint moment comparison as lists: z of the mean and of the variance, relative
+    differences of the mean and of the variance."""
+    return {"z_mean": [round(z[0], 3) for z in ms], "z_var": [round(z[1], 3) for z in ms],
+            "rel_mean": [float(f"{z[2]:.3g}") for z in ms], "rel_var": [float(f"{z[3]:.3g}") for z in ms]}
 
 
 def _batch_to_checkpoints(model, state, checkpoints, *, seed, weights=None, s_max=0.0):

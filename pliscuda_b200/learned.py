@@ -159,9 +159,16 @@ def _moment_z_per_checkpoint(a, b) -> list:
     with the largest |z| each, standard errors as for independent samples (var/n for the mean,
     (m4 - var^2)/n for the variance).  Neighbouring subvolumes are correlated, so these are
     descriptive: the replica-based test (tests/test_learned_stats_gpu.py) is the statistical check."""
+    return [z[:2] for z in _moments_per_checkpoint(a, b)]
+
+
+def _moments_per_checkpoint(a, b) -> list:
+    """Per checkpoint (z of the mean, z of the variance, relative difference of the mean, relative
+    difference of the variance) of b against a, each the species with the largest |value|: the z
+    values as in _moment_z_per_checkpoint, the relative differences (b - a) / a."""
     out = []
     for x, y in zip(a, b):
-        zm = zv = 0.0
+        zm = zv = rm = rv = 0.0
         for s in range(x.shape[0]):
             u, v = x[s].astype(np.float64), y[s].astype(np.float64)
             se = np.sqrt(u.var() / u.size + v.var() / v.size)
@@ -169,9 +176,13 @@ def _moment_z_per_checkpoint(a, b) -> list:
             m4u, m4v = np.mean((u - u.mean()) ** 4), np.mean((v - v.mean()) ** 4)
             sev = np.sqrt(max(m4u - u.var() ** 2, 0) / u.size + max(m4v - v.var() ** 2, 0) / v.size)
             z2 = (v.var() - u.var()) / sev if sev > 0 else 0.0
+            r1 = (v.mean() - u.mean()) / u.mean() if u.mean() != 0 else 0.0
+            r2 = (v.var() - u.var()) / u.var() if u.var() != 0 else 0.0
             zm = z1 if abs(z1) > abs(zm) else zm
             zv = z2 if abs(z2) > abs(zv) else zv
-        out.append((float(zm), float(zv)))
+            rm = r1 if abs(r1) > abs(rm) else rm
+            rv = r2 if abs(r2) > abs(rv) else rv
+        out.append((float(zm), float(zv), float(rm), float(rv)))
     return out
 
 
