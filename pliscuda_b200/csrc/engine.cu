@@ -187,9 +187,29 @@ int Engine::create(const Model& model, const plis_options& opt) {
   // geometry
   Geo& g = args_.g;
   if (dm.lattice) {
-    uint32_t tx = opt.tile[0] > 0 ? (uint32_t)opt.tile[0] : std::min<uint32_t>(32, pow2_at_least(dm.X));
-    uint32_t ty = opt.tile[1] > 0 ? (uint32_t)opt.tile[1] : std::min<uint32_t>(std::max<uint32_t>(1, 256 / tx), pow2_at_least(dm.Y));
-    uint32_t tz = opt.tile[2] > 0 ? (uint32_t)opt.tile[2] : std::min<uint32_t>(std::max<uint32_t>(1, 256 / (tx * ty)), pow2_at_least(dm.Z));
+    // default brick: 8 x 8 in x and y and deep enough in z for 256 subvolumes (8 x 8 x 4 on a cube),
+    // then wider in x and y where the lattice is too thin in z.  Measured on one B200 against the
+    // earlier 32 x 8 x 1 rows: Schlogl 64^3 -1.6 % time, the random network 128^3 -1.1 %, the small
+    // A/B 10^3 -0.9 % (the six neighbours of a compact brick are more often in the brick's own lines)
+    uint32_t tx, ty, tz;
+    if (opt.tile[0] > 0) {
+      tx = (uint32_t)opt.tile[0];
+      ty = opt.tile[1] > 0 ? (uint32_t)opt.tile[1] : std::min<uint32_t>(std::max<uint32_t>(1, 256 / tx), pow2_at_least(dm.Y));
+      tz = opt.tile[2] > 0 ? (uint32_t)opt.tile[2] : std::min<uint32_t>(std::max<uint32_t>(1, 256 / (tx * ty)), pow2_at_least(dm.Z));
+    } else if (opt.tile[1] > 0 || opt.tile[2] > 0) {  // y and/or z given: x fills up to 256
+      ty = opt.tile[1] > 0 ? (uint32_t)opt.tile[1] : 1u;
+      tz = opt.tile[2] > 0 ? (uint32_t)opt.tile[2] : 1u;
+      tx = std::min<uint32_t>(std::max<uint32_t>(1, 256 / std::max<uint32_t>(1, ty * tz)), pow2_at_least(dm.X));
+    } else {
+      const uint32_t px = pow2_at_least(dm.X), py = pow2_at_least(dm.Y), pz = pow2_at_least(dm.Z);
+      tx = std::min<uint32_t>(8, px);
+      ty = std::min<uint32_t>(8, py);
+      tz = std::min<uint32_t>(256 / (tx * ty), pz);
+      while (tx * ty * tz < 256 && (tx < px || ty < py)) {
+        if (tx < px && (tx <= ty || ty >= py)) tx *= 2;
+        else ty *= 2;
+      }
+    }
     if (tx * ty * tz > 256 || tx * ty * tz == 0) { err_ = "tile must hold 1..256 subvolumes"; return PLIS_ERR_INVALID; }
     g.tx = tx; g.ty = ty; g.tz = tz;
     g.ntx = (dm.X + tx - 1) / tx; g.nty = (dm.Y + ty - 1) / ty; g.ntz = (dm.Z + tz - 1) / tz;
