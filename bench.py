@@ -519,9 +519,36 @@ def configs_report():
       80 MB of counts per buffer), reference semantics, FP64 and FP32: 200 steps after 20 warm-up
       steps (Cao tau ~1e-10 at these counts: t = 2 is out of reach of any tau-leaping step), with the
       HBM roofline of its dominant kernel from an event-instrumented replay of 40 more steps:
-      8 S N bytes per leap launch (counts read and written), 4 S N + 9 N + 4 S N per classification."""
+      8 S N bytes per leap launch (counts read and written), 4 S N + 9 N + 4 S N per classification;
+    * the headline workload (Schlogl 64^3, reference semantics) in the FP32 form, the reference's own
+      propensity precision: the same 5 warm-up and 20 timed intervals as the headline, L2 flushed
+      between intervals."""
+    import torch
+
     from pliscuda_b200 import Simulation, workloads
     out = {}
+    m, st = workloads.schlogl(64)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    with Simulation(m, mode="reference", precision="fp32", seed=SEED) as sim:
+        sim.set_state(st)
+        t = 0.0
+        for _ in range(5):
+            t += INTERVAL
+            sim.run(t)
+        a0 = sim.stats()
+        ms = 0.0
+        for _ in range(20):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            a = sim.stats()
+            t += INTERVAL
+            b = sim.run(t)
+            ms += b.device_ms - a.device_ms
+        out["schlogl64_fp32"] = {"workload": "schlogl64 in the FP32 form, reference semantics, t = 5 -> 25 (the headline's slice)",
+                                 "events": int(b.events - a0.events), "steps": int(b.steps - a0.steps), "device_ms": ms,
+                                 "events_per_s": (b.events - a0.events) / (ms * 1e-3),
+                                 "sim_time_per_s": (b.time - a0.time) / (ms * 1e-3)}
+    del flush
     m, st = workloads.small_ab(10)
     with Simulation(m, mode="reference", precision="fp64", seed=SEED + 1) as sim:  # untimed: first-use costs
         sim.set_state(st)
