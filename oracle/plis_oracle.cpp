@@ -46,10 +46,10 @@ enum Flag : uint8_t { LEAP_CR = 0, LEAP_NOCR = 1, SSA = 2, SSA_FF = 3 };  // enu
 template <typename Real> struct RealOps;
 template <> struct RealOps<double> {
   static double poisson(plis_stream* s, double lam) { return plis_poisson_d(s, lam); }
-  static double emlam(double lam) { return lam < 10.0 ? plis_exp(-lam) : 0.0; }
+  static double emlam(double lam) { return lam < PLIS_LEAP_INV_MAX ? plis_exp(-lam) : 0.0; }
   static double poisson_shared(plis_stream* s, double lam, double em) {
     if (!(lam > 0.0)) return 0.0;
-    return lam < 10.0 ? plis_poisson_small_d(s, lam, em) : plis_poisson_d(s, lam);
+    return lam < PLIS_LEAP_INV_MAX ? plis_poisson_small_d(s, lam, em) : plis_poisson_d(s, lam);
   }
   static int64_t count(double k) { return (int64_t)plis_count_d(k); }
   // inversion draw i of a group of n from the group's shared Philox blocks (plis_group_uniforms_d)
@@ -66,10 +66,10 @@ template <> struct RealOps<double> {
 };
 template <> struct RealOps<float> {
   static double poisson(plis_stream* s, float lam) { return plis_poisson_f(s, lam); }
-  static float emlam(float lam) { return lam < 10.0f ? plis_expf(-lam) : 0.0f; }
+  static float emlam(float lam) { return lam < (float)PLIS_LEAP_INV_MAX ? plis_expf(-lam) : 0.0f; }
   static double poisson_shared(plis_stream* s, float lam, float em) {
     if (!(lam > 0.0f)) return 0.0;
-    return lam < 10.0f ? plis_poisson_small_f(s, lam, em) : plis_poisson_d(s, (double)lam);
+    return lam < (float)PLIS_LEAP_INV_MAX ? plis_poisson_small_f(s, lam, em) : plis_poisson_d(s, (double)lam);
   }
   static int64_t count(double k) { return (int64_t)plis_count_d(k); }
   static double inv_group(const plis_stream* g, uint32_t i, int n, float lam, float em) {
@@ -443,7 +443,7 @@ struct Sim : Base {
         if (!(lam > (Real)0)) continue;  // not leaped (critical), or a zero mean (a draw of 0)
         if (pool_on && join(pool, lam, lam)) continue;
         int64_t k;
-        if (lam > (Real)0 && lam < (Real)10) {  // inversion: uniform r % 4 of reaction group r / 4
+        if (lam > (Real)0 && lam < (Real)PLIS_LEAP_INV_MAX) {  // inversion: uniform r % 4 of reaction group r / 4
           plis_stream g = plis_stream_make(opt.seed, opt.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_rgroup(r >> 2));
           k = Ops::count(Ops::inv_group(&g, r & 3u, 4, lam, Ops::emlam(lam)));
         } else {
@@ -467,7 +467,7 @@ struct Sim : Base {
         Real em = Ops::emlam(lam);
         for (int j = 0; j < n; ++j) {
           int64_t k;
-          if (lam > (Real)0 && lam < (Real)10) {  // inversion: uniform j of the species' diffusion group
+          if (lam > (Real)0 && lam < (Real)PLIS_LEAP_INV_MAX) {  // inversion: uniform j of the species' diffusion group
             plis_stream g = plis_stream_make(opt.seed, opt.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_dgroup(s));
             k = Ops::count(Ops::inv_group(&g, (uint32_t)j, 6, lam, em));
           } else {

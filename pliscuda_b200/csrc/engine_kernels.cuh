@@ -87,15 +87,15 @@ inline void launch_pdl(Kern kern, dim3 g, dim3 b, size_t smem, cudaStream_t s, A
 template <typename Real> struct RT;
 template <> struct RT<double> {
   static __device__ __forceinline__ double poisson(plis_stream* s, double lam) { return plis_poisson_d(s, lam); }
-  static __device__ __forceinline__ double emlam(double lam) { return lam < 10.0 ? plis_exp(-lam) : 0.0; }
+  static __device__ __forceinline__ double emlam(double lam) { return lam < PLIS_LEAP_INV_MAX ? plis_exp(-lam) : 0.0; }
   static __device__ __forceinline__ double poisson_shared(plis_stream* s, double lam, double em) {
     if (!(lam > 0.0)) return 0.0;
-    return lam < 10.0 ? plis_poisson_small_d(s, lam, em) : plis_poisson_d(s, lam);
+    return lam < PLIS_LEAP_INV_MAX ? plis_poisson_small_d(s, lam, em) : plis_poisson_d(s, lam);
   }
   static __device__ __forceinline__ double uniform(plis_stream* s) { return plis_uniform_d(s); }
   static __device__ __forceinline__ long long count(double k) { return plis_count_d(k); }
   static __device__ __forceinline__ double inf() { return PLIS_INF_D; }
-  // a 32-bit word of a group block as a uniform, and a Poisson(lam < 10) draw by inversion from it
+  // a 32-bit word of a group block as a uniform, and a Poisson draw by inversion from it
   static __device__ __forceinline__ double word_uniform(uint32_t w) { return plis_u32_to_uniform_d(w); }
   static __device__ __forceinline__ double inv_word(uint32_t w, double lam) {
     return plis_poisson_inv_d(plis_u32_to_uniform_d(w), lam, plis_exp(-lam));
@@ -103,10 +103,10 @@ template <> struct RT<double> {
 };
 template <> struct RT<float> {
   static __device__ __forceinline__ double poisson(plis_stream* s, float lam) { return plis_poisson_f(s, lam); }
-  static __device__ __forceinline__ float emlam(float lam) { return lam < 10.0f ? plis_expf(-lam) : 0.0f; }
+  static __device__ __forceinline__ float emlam(float lam) { return lam < (float)PLIS_LEAP_INV_MAX ? plis_expf(-lam) : 0.0f; }
   static __device__ __forceinline__ double poisson_shared(plis_stream* s, float lam, float em) {
     if (!(lam > 0.0f)) return 0.0;
-    return lam < 10.0f ? plis_poisson_small_f(s, lam, em) : plis_poisson_d(s, (double)lam);
+    return lam < (float)PLIS_LEAP_INV_MAX ? plis_poisson_small_f(s, lam, em) : plis_poisson_d(s, (double)lam);
   }
   static __device__ __forceinline__ float uniform(plis_stream* s) { return plis_uniform_f(s); }
   static __device__ __forceinline__ long long count(double k) { return plis_count_d(k); }
@@ -118,7 +118,7 @@ template <> struct RT<float> {
 };
 
 // Per-neighbour diffusion draws of one species (leap.cu:49-53).  All n draws have the same mean, so
-// for lam < 10 the inversion CDF is built once, up to the largest of the n uniforms, and each draw
+// for lam < PLIS_LEAP_INV_MAX the inversion CDF is built once, up to the largest of the n uniforms, and each draw
 // reads its result off it: identical results to n separate sequential searches
 // (plis_poisson_small_d / _f), max_j k_j iterations instead of sum_j k_j.
 template <typename Real> struct DiffTraits;
@@ -147,7 +147,7 @@ __device__ __forceinline__ void diffusion_draws(const KArgs& A, uint32_t c, int 
     for (int j = 0; j < 6; ++j) k[j] = 0;
     return;
   }
-  if (!(lam < (Real)10)) {
+  if (!(lam < (Real)PLIS_LEAP_INV_MAX)) {
 #pragma unroll
     for (int j = 0; j < 6; ++j) k[j] = 0;
 #pragma unroll 1
@@ -1052,7 +1052,7 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
         return true;
       };
       auto reaction_group = [&](const int r0) {
-        // reactions r0..r0+3: means >= 10 go through PTRS one by one, the rest in lockstep
+        // reactions r0..r0+3: means >= PLIS_LEAP_INV_MAX go through PTRS one by one, the rest in lockstep
         Real u[4], lam[4];
         bool act[4];
         long long kk[4];
@@ -1077,7 +1077,7 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
             lam[i] = fire ? tl * a : (Real)0;
             if (pool_on && lam[i] > (Real)0 && pool_join(pool, lam[i], lam[i])) lam[i] = (Real)0;  // pooled
             if (lam[i] > (Real)0) {
-              if (lam[i] < (Real)10) {
+              if (lam[i] < (Real)PLIS_LEAP_INV_MAX) {
                 act[i] = true;  // inversion search: its single uniform comes from the group's blocks
                 need |= 1u << i;
               } else {
@@ -1086,7 +1086,7 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
             }
           }
         }
-        while (big_mean) {  // draws with means >= 10, one at a time through a single inlined PTRS
+        while (big_mean) {  // draws with means >= PLIS_LEAP_INV_MAX, one at a time through a single inlined PTRS
           const int i = __ffs(big_mean) - 1;
           big_mean &= big_mean - 1u;
           Real li = lam[0];

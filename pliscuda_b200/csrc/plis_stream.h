@@ -145,11 +145,16 @@ enum {
 #define PLIS_CH_DIFF_BASE 0x40000u  // diffusion channels: base + species * 8 + slot
 PLIS_HD uint32_t plis_ch_react(uint32_t r) { return r; }
 PLIS_HD uint32_t plis_ch_diff(uint32_t s, uint32_t slot) { return PLIS_CH_DIFF_BASE + s * 8u + slot; }
-// Grouped channels: the single uniforms of the inversion-searched draws (means below 10) of a group
-// come from shared Philox blocks, four uniforms per block (uniform i of a group: word i % 4 of block
-// i / 4).  Reactions 4g .. 4g+3 form group g; the six
+// Grouped channels: the single uniforms of the inversion-searched draws (means below
+// PLIS_LEAP_INV_MAX) of a group come from shared Philox blocks, four uniforms per block (uniform i of
+// a group: word i % 4 of block i / 4).  Reactions 4g .. 4g+3 form group g; the six
 // neighbour slots of one species form its diffusion group.  Draws searched by PTRS keep their own
 // channels (plis_ch_react, plis_ch_diff).
+// The leap's draws search by inversion up to a mean of 20 (the stand-alone samplers below switch to
+// PTRS at 10): a search from 0 costs about lambda + 3 sqrt(lambda) iterations of a few operations for
+// the slowest lane of a warp, where PTRS costs a few hundred divergent instructions per draw, and
+// the two cross near 20.  Both searches are exact samplers, so the mean only picks the algorithm.
+#define PLIS_LEAP_INV_MAX 20.0
 #define PLIS_CH_RGROUP_BASE 0x20000u  // + reaction group
 #define PLIS_CH_DGROUP_BASE 0x60000u  // + species
 PLIS_HD uint32_t plis_ch_rgroup(uint32_t g) { return PLIS_CH_RGROUP_BASE + g; }
