@@ -129,6 +129,13 @@ template <> struct DiffTraits<double> {
   }
   static constexpr double tail = 8.673617379884035e-19;
   static constexpr int kmax = 200;
+  // The searches below read binary64 group uniforms, u <= 1 - 2^-33, with means below 20.  Their tail
+  // test p <= F 2^-60 cannot change a result there, so it is left out (the k >= kmax bound stays):
+  // p_k > e^-20 / 16 > 2^-60 for k <= 2 lambda, so the test could only fire at some k > 2 lambda, where
+  // p_{j+1} / p_j < 1/2 and the mass beyond k is below p_k <= 2^-60; the computed F_k is within
+  // 4 k 2^-53 < 2^-44 of the exact CDF (k < 100), so F_k > 1 - 2^-43 > u: the search has already
+  // stopped on u <= F.
+  static constexpr bool tail_test = false;
 };
 template <> struct DiffTraits<float> {
   static __device__ __forceinline__ float uni(plis_stream* s) { return plis_uniform_f(s); }
@@ -137,6 +144,8 @@ template <> struct DiffTraits<float> {
   }
   static constexpr float tail = 2.9802322e-08f;
   static constexpr int kmax = 100;
+  // binary32: the rounding of F can leave it below a uniform near 1, so the stop test is needed
+  static constexpr bool tail_test = true;
 };
 
 template <typename Real>
@@ -185,7 +194,7 @@ __device__ __forceinline__ void diffusion_draws(const KArgs& A, uint32_t c, int 
     ki += 1;
     p = (p * lam) * (Real)plis_inv_k_tab[ki];
     F += p;
-    const bool brk = (p <= F * DiffTraits<Real>::tail) || ki >= DiffTraits<Real>::kmax;
+    const bool brk = (DiffTraits<Real>::tail_test && p <= F * DiffTraits<Real>::tail) || ki >= DiffTraits<Real>::kmax;
     pending = false;
 #pragma unroll
     for (int j = 0; j < 6; ++j) {
@@ -228,7 +237,8 @@ __device__ __forceinline__ void batched_small_draws(const Real u[4], const Real 
       if (open_[i]) {
         p[i] = (p[i] * lam[i]) * ik;
         F[i] += p[i];
-        const bool brk = (p[i] <= F[i] * DiffTraits<Real>::tail) || ki >= DiffTraits<Real>::kmax;
+        const bool brk =
+            (DiffTraits<Real>::tail_test && p[i] <= F[i] * DiffTraits<Real>::tail) || ki >= DiffTraits<Real>::kmax;
         if (!(u[i] > F[i]) || brk) {
           open_[i] = false;
           k[i] = ki;
