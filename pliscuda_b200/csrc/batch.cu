@@ -214,6 +214,7 @@ int BatchEngine::create(const plis_batch_desc& d, const plis_options& opt) {
   dopt_.eps = opt.epsilon;
   dopt_.seed = opt.seed;
   dopt_.replica = 0;
+  devopts_keys(dopt_);
   dopt_.pool = pooled_draws_on(opt.pooled_draws, R_, S_);
   if (dopt_.pool) small_ = false;  // pooled draws live in the generic leap only
 
@@ -310,6 +311,7 @@ int BatchEngine::layout(const int tile[3]) {
     v.m.dr = (const char*)d_dr_ + (size_t)r * S_ * rsz;
     v.o = dopt_;
     v.o.replica = ids_[r];
+    devopts_keys(v.o);
     v.g = geo_;
     v.g.ntx = rep[r].ntx; v.g.nty = rep[r].nty; v.g.ntz = rep[r].ntz;
     geo_divisors(v.g);

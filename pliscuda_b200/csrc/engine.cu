@@ -260,6 +260,7 @@ int Engine::create(const Model& model, const plis_options& opt) {
   o.eps = opt.epsilon;
   o.seed = opt.seed;
   o.replica = opt.replica;
+  devopts_keys(o);
   o.pool = pooled_draws_on(opt.pooled_draws, M.R, M.S);
   if (o.pool) args_.sm.on = 0;  // pooled draws live in the generic leap only
 

@@ -4,6 +4,8 @@
 
 #include <stdint.h>
 
+#include "plis_stream.h"
+
 namespace plis {
 
 enum : uint8_t { F_LEAP_CR = 0, F_LEAP_NOCR = 1, F_SSA = 2, F_SSA_FF = 3 };  // constants.cuh:53-58
@@ -121,7 +123,11 @@ struct DevOpts {
   unsigned long long seed;
   uint32_t replica;
   uint32_t pool;      // 1: pooled draws of small-mean channels in the generic leap (plis_stream.h)
+  uint32_t rk0[10], rk1[10];  // Philox round keys of (seed, replica): plis_round_keys, set with devopts_keys
 };
+
+// Fill the round keys of o.seed / o.replica; call after either changes.
+inline void devopts_keys(DevOpts& o) { plis_round_keys(o.seed, o.replica, o.rk0, o.rk1); }
 
 // Division by a divisor fixed at set-up, as one multiply-high, two adds and two shifts: exact for
 // every 32-bit numerator (Granlund and Montgomery, "Division by invariant integers using

@@ -127,6 +127,9 @@ template <> struct DiffTraits<double> {
   static __device__ __forceinline__ void group(const plis_stream* g, uint32_t need, double* u, int n) {
     plis_group_uniforms_d(g, need, u, n);
   }
+  static __device__ __forceinline__ void group_rk(const plis_stream* g, uint32_t need, double* u, int n, const DevOpts& o) {
+    plis_group_uniforms_rk_d(g, need, u, n, o.rk0, o.rk1);
+  }
   static constexpr double tail = 8.673617379884035e-19;
   static constexpr int kmax = 200;
   // The searches below read binary64 group uniforms, u <= 1 - 2^-33, with means below 20.  Their tail
@@ -142,13 +145,16 @@ template <> struct DiffTraits<float> {
   static __device__ __forceinline__ void group(const plis_stream* g, uint32_t need, float* u, int n) {
     plis_group_uniforms_f(g, need, u, n);
   }
+  static __device__ __forceinline__ void group_rk(const plis_stream* g, uint32_t need, float* u, int n, const DevOpts& o) {
+    plis_group_uniforms_rk_f(g, need, u, n, o.rk0, o.rk1);
+  }
   static constexpr float tail = 2.9802322e-08f;
   static constexpr int kmax = 100;
   // binary32: the rounding of F can leave it below a uniform near 1, so the stop test is needed
   static constexpr bool tail_test = true;
 };
 
-template <typename Real>
+template <typename Real, bool RK = false>
 __device__ __forceinline__ void diffusion_draws(const KArgs& A, uint32_t c, int s, int n, Real lam, Real em,
                                                 uint64_t step, uint32_t attempt, int32_t k[6]) {
   if (!(lam > (Real)0)) {
@@ -178,7 +184,8 @@ __device__ __forceinline__ void diffusion_draws(const KArgs& A, uint32_t c, int 
   for (int j = 0; j < 6; ++j) u[j] = (Real)0;
   {  // the slots' uniforms from the species' grouped blocks
     const plis_stream g = plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_dgroup(s));
-    DiffTraits<Real>::group(&g, (1u << n) - 1u, u, 6);
+    if constexpr (RK) DiffTraits<Real>::group_rk(&g, (1u << n) - 1u, u, 6, A.o);
+    else DiffTraits<Real>::group(&g, (1u << n) - 1u, u, 6);
   }
 #pragma unroll
   for (int j = 0; j < 6; ++j) {
@@ -1018,7 +1025,9 @@ struct LeapCtx {
 // events and guard flag.  leap_step, leap.cu:3-65.
 // SM: a small model whose tables are in A.sm (SmallModel): the reaction and species loops run to
 // the tables' compile-time sizes, so every table read is a constant-bank operand.
-template <typename Real, int MAXS, bool LOG, bool WALK = true, bool SM = false>
+// RK: the group blocks use the round keys in A.o (kernel arguments: constant-bank operands); the
+// batched kernel, whose per-replica arguments sit in shared memory, recomputes them instead.
+template <typename Real, int MAXS, bool LOG, bool WALK = true, bool SM = false, bool RK = false>
 __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const LeapCtx& L, Real tl, const Box& box,
                                           long long& ev, int& big) {
   static_assert(!SM || MAXS <= kSmallS, "small-model tables hold kSmallS species");
@@ -1112,7 +1121,8 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
         if (need) {
           const plis_stream g =
               plis_stream_make(A.o.seed, A.o.replica, c, PLIS_PHASE_LEAP, step, attempt, plis_ch_rgroup((uint32_t)r0 >> 2));
-          DiffTraits<Real>::group(&g, need, u, 4);
+          if constexpr (RK) DiffTraits<Real>::group_rk(&g, need, u, 4, A.o);
+          else DiffTraits<Real>::group(&g, need, u, 4);
         }
         long long ks[4];
         batched_small_draws<Real>(u, lam, act, ks);
@@ -1178,7 +1188,7 @@ __device__ __forceinline__ void leap_tile(const KArgs& A, uint32_t tile, const L
         if (pool_on && n > 0 && lam > (Real)0 && pool_join(pool, lam, (Real)n * lam)) return;  // pooled
         const Real em = RT<Real>::emlam(lam);  // one exp for the n draws of this species
         int32_t kd[6];
-        diffusion_draws<Real>(A, c, s, n, lam, em, step, attempt, kd);
+        diffusion_draws<Real, RK>(A, c, s, n, lam, em, step, attempt, kd);
         long long out = 0;
         if (WALK && q.lat) {  // slot j is the j-th present direction; kd is read by constant index only
           int j = 0;
@@ -1365,7 +1375,7 @@ __global__ void __launch_bounds__(256, PLIS_LEAP_MIN_BLOCKS) k_leap(KArgs A) {
   __syncthreads();
   long long ev;
   int big;
-  leap_tile<Real, MAXS, LOG, true, SM>(A, blockIdx.x, L, tl, box, ev, big);
+  leap_tile<Real, MAXS, LOG, true, SM, true>(A, blockIdx.x, L, tl, box, ev, big);
   // events and guard flags of the CTA
   ev = warp_sum(ev);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;

@@ -250,6 +250,74 @@ PLIS_HD float plis_u32_to_uniform_f(uint32_t w) {
   return ((float)x + 0.5f) * 1.1920928955078125e-07f;  // 2^-23
 }
 
+// Precomputed round keys.  The ten round keys of plis_philox4x32_10 under the key plis_stream_make
+// derives from (seed, replica) are rk0[i] = k0 + i W0, rk1[i] = k1 + i W1; a caller that holds them
+// (the step kernels keep them in their arguments) computes a block without the key schedule, with
+// the same result as plis_philox4x32_10 / plis_group_block.
+PLIS_HD void plis_round_keys(uint64_t seed, uint32_t replica, uint32_t rk0[10], uint32_t rk1[10]) {
+  const plis_stream s = plis_stream_make(seed, replica, 0u, 0u, 0u, 0u, 0u);
+  for (int i = 0; i < 10; ++i) {
+    rk0[i] = s.k0 + (uint32_t)i * PLIS_PHILOX_W0;
+    rk1[i] = s.k1 + (uint32_t)i * PLIS_PHILOX_W1;
+  }
+}
+
+PLIS_HD plis_u32x4 plis_philox4x32_10_rk(plis_u32x4 c, const uint32_t rk0[10], const uint32_t rk1[10]) {
+#if defined(__CUDA_ARCH__)
+#pragma unroll
+#endif
+  for (int i = 0; i < 10; ++i) {
+    uint64_t p0 = (uint64_t)PLIS_PHILOX_M0 * (uint64_t)c.x;
+    uint64_t p1 = (uint64_t)PLIS_PHILOX_M1 * (uint64_t)c.z;
+    plis_u32x4 n;
+    n.x = (uint32_t)(p1 >> 32) ^ c.y ^ rk0[i];
+    n.y = (uint32_t)p1;
+    n.z = (uint32_t)(p0 >> 32) ^ c.w ^ rk1[i];
+    n.w = (uint32_t)p0;
+    c = n;
+  }
+  return c;
+}
+
+PLIS_HD plis_u32x4 plis_group_block_rk(const plis_stream* g, uint32_t b, const uint32_t rk0[10], const uint32_t rk1[10]) {
+  plis_u32x4 ctr = g->ctr;
+  ctr.y = (ctr.y & 0xFFFFF000u) | (b & 0xFFFu);
+  return plis_philox4x32_10_rk(ctr, rk0, rk1);
+}
+
+// plis_group_uniforms_d / _f with precomputed round keys (same uniforms)
+PLIS_HD void plis_group_uniforms_rk_d(const plis_stream* g, uint32_t need, double* u, int n, const uint32_t rk0[10],
+                                      const uint32_t rk1[10]) {
+#if defined(__CUDA_ARCH__)
+#pragma unroll
+#endif
+  for (int b = 0; b < 2; ++b) {
+    if (4 * b < n && (need >> (4 * b)) & 15u) {
+      const plis_u32x4 w = plis_group_block_rk(g, (uint32_t)b, rk0, rk1);
+      u[4 * b] = plis_u32_to_uniform_d(w.x);
+      if (4 * b + 1 < n) u[4 * b + 1] = plis_u32_to_uniform_d(w.y);
+      if (4 * b + 2 < n) u[4 * b + 2] = plis_u32_to_uniform_d(w.z);
+      if (4 * b + 3 < n) u[4 * b + 3] = plis_u32_to_uniform_d(w.w);
+    }
+  }
+}
+
+PLIS_HD void plis_group_uniforms_rk_f(const plis_stream* g, uint32_t need, float* u, int n, const uint32_t rk0[10],
+                                      const uint32_t rk1[10]) {
+#if defined(__CUDA_ARCH__)
+#pragma unroll
+#endif
+  for (int b = 0; b < 2; ++b) {
+    if (4 * b < n && (need >> (4 * b)) & 15u) {
+      const plis_u32x4 w = plis_group_block_rk(g, (uint32_t)b, rk0, rk1);
+      u[4 * b] = plis_u32_to_uniform_f(w.x);
+      if (4 * b + 1 < n) u[4 * b + 1] = plis_u32_to_uniform_f(w.y);
+      if (4 * b + 2 < n) u[4 * b + 2] = plis_u32_to_uniform_f(w.z);
+      if (4 * b + 3 < n) u[4 * b + 3] = plis_u32_to_uniform_f(w.w);
+    }
+  }
+}
+
 PLIS_HD void plis_group_uniforms_d(const plis_stream* g, uint32_t need, double* u, int n) {
 #if defined(__CUDA_ARCH__)
 #pragma unroll
