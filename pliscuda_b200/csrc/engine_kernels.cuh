@@ -234,25 +234,38 @@ __device__ __forceinline__ void batched_small_draws(const Real u[4], const Real 
       pending |= open_[i];
     }
   }
+  // two terms per pass (k = ki + 1, ki + 2): the same arithmetic, half the loop overhead; kmax is even,
+  // so ki + 2 <= kmax and the table index stays in range
+  static_assert(DiffTraits<Real>::kmax % 2 == 0, "two terms per pass need an even kmax");
   int ki = 0;
   while (pending) {
-    ki += 1;
-    const Real ik = (Real)plis_inv_k_tab[ki];
+    const Real ik1 = (Real)plis_inv_k_tab[ki + 1];
+    const Real ik2 = (Real)plis_inv_k_tab[ki + 2];
     pending = false;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       if (open_[i]) {
-        p[i] = (p[i] * lam[i]) * ik;
+        p[i] = (p[i] * lam[i]) * ik1;
         F[i] += p[i];
-        const bool brk =
-            (DiffTraits<Real>::tail_test && p[i] <= F[i] * DiffTraits<Real>::tail) || ki >= DiffTraits<Real>::kmax;
-        if (!(u[i] > F[i]) || brk) {
+        const bool brk1 = (DiffTraits<Real>::tail_test && p[i] <= F[i] * DiffTraits<Real>::tail) ||
+                          ki + 1 >= DiffTraits<Real>::kmax;
+        if (!(u[i] > F[i]) || brk1) {
           open_[i] = false;
-          k[i] = ki;
+          k[i] = ki + 1;
+        } else {
+          p[i] = (p[i] * lam[i]) * ik2;
+          F[i] += p[i];
+          const bool brk2 = (DiffTraits<Real>::tail_test && p[i] <= F[i] * DiffTraits<Real>::tail) ||
+                            ki + 2 >= DiffTraits<Real>::kmax;
+          if (!(u[i] > F[i]) || brk2) {
+            open_[i] = false;
+            k[i] = ki + 2;
+          }
         }
         pending |= open_[i];
       }
     }
+    ki += 2;
   }
 }
 
