@@ -87,7 +87,8 @@ inline void launch_pdl(Kern kern, dim3 g, dim3 b, size_t smem, cudaStream_t s, A
 template <typename Real> struct RT;
 template <> struct RT<double> {
   static __device__ __forceinline__ double poisson(plis_stream* s, double lam) { return plis_poisson_d(s, lam); }
-  static __device__ __forceinline__ double emlam(double lam) { return lam < PLIS_LEAP_INV_MAX ? plis_exp(-lam) : 0.0; }
+  // lam >= 0 (a rate times a count times tau): below the inversion limit e^-lam is a normal number
+  static __device__ __forceinline__ double emlam(double lam) { return lam < PLIS_LEAP_INV_MAX ? plis_exp_normal(-lam) : 0.0; }
   static __device__ __forceinline__ double poisson_shared(plis_stream* s, double lam, double em) {
     if (!(lam > 0.0)) return 0.0;
     return lam < PLIS_LEAP_INV_MAX ? plis_poisson_small_d(s, lam, em) : plis_poisson_d(s, lam);
@@ -103,7 +104,9 @@ template <> struct RT<double> {
 };
 template <> struct RT<float> {
   static __device__ __forceinline__ double poisson(plis_stream* s, float lam) { return plis_poisson_f(s, lam); }
-  static __device__ __forceinline__ float emlam(float lam) { return lam < (float)PLIS_LEAP_INV_MAX ? plis_expf(-lam) : 0.0f; }
+  static __device__ __forceinline__ float emlam(float lam) {
+    return lam < (float)PLIS_LEAP_INV_MAX ? plis_expf_normal(-lam) : 0.0f;
+  }
   static __device__ __forceinline__ double poisson_shared(plis_stream* s, float lam, float em) {
     if (!(lam > 0.0f)) return 0.0;
     return lam < (float)PLIS_LEAP_INV_MAX ? plis_poisson_small_f(s, lam, em) : plis_poisson_d(s, (double)lam);

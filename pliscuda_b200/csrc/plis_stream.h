@@ -389,6 +389,29 @@ PLIS_HD double plis_exp(double x) {
   return (p * plis_pow2i(k + 60)) * 8.673617379884035e-19;  // 2^-60; rounds once into the subnormals
 }
 
+// e^x for -708 < x < 709 (normal results): plis_exp without its NaN and range tests, the same operations
+// and therefore the same bits on that domain.  The leap's e^-lambda (0 <= lambda < PLIS_LEAP_INV_MAX).
+PLIS_HD double plis_exp_normal(double x) {
+  double kd = PLIS_FLOOR(x * PLIS_INV_LN2 + 0.5);
+  int k = (int)kd;
+  double r = (x - kd * PLIS_LN2_HI) - kd * PLIS_LN2_LO;
+  double p = 1.6059043836821613e-10;
+  p = PLIS_FMA(p, r, 2.08767569878681e-09);
+  p = PLIS_FMA(p, r, 2.505210838544172e-08);
+  p = PLIS_FMA(p, r, 2.755731922398589e-07);
+  p = PLIS_FMA(p, r, 2.7557319223985893e-06);
+  p = PLIS_FMA(p, r, 2.48015873015873e-05);
+  p = PLIS_FMA(p, r, 0.0001984126984126984);
+  p = PLIS_FMA(p, r, 0.001388888888888889);
+  p = PLIS_FMA(p, r, 0.008333333333333333);
+  p = PLIS_FMA(p, r, 0.041666666666666664);
+  p = PLIS_FMA(p, r, 0.16666666666666666);
+  p = PLIS_FMA(p, r, 0.5);
+  p = PLIS_FMA(p, r, 1.0);
+  p = PLIS_FMA(p, r, 1.0);
+  return p * plis_pow2i(k);
+}
+
 PLIS_HD double plis_log(double x) {
   if (!(x > 0.0)) return (x == 0.0) ? -PLIS_INF_D : PLIS_NAN_D;
   if (plis_isinf_d(x)) return x;
@@ -609,6 +632,23 @@ PLIS_HD float plis_expf(float x) {
     return p * plis_pow2i_f(k);
   }
   return (p * plis_pow2i_f(k + 30)) * 9.3132257e-10f;  // 2^-30
+}
+
+// e^x for -87 < x < 88 (normal results): plis_expf without its NaN and range tests, the same bits there.
+PLIS_HD float plis_expf_normal(float x) {
+  float kf = PLIS_FLOORF(x * PLIS_INV_LN2_F + 0.5f);
+  int k = (int)kf;
+  float r = (x - kf * PLIS_LN2_HI_F) - kf * PLIS_LN2_LO_F;
+  float p = 2.4801588e-05f;
+  p = PLIS_FMAF(p, r, 0.0001984127f);
+  p = PLIS_FMAF(p, r, 0.0013888889f);
+  p = PLIS_FMAF(p, r, 0.008333334f);
+  p = PLIS_FMAF(p, r, 0.041666668f);
+  p = PLIS_FMAF(p, r, 0.16666667f);
+  p = PLIS_FMAF(p, r, 0.5f);
+  p = PLIS_FMAF(p, r, 1.0f);
+  p = PLIS_FMAF(p, r, 1.0f);
+  return p * plis_pow2i_f(k);
 }
 
 PLIS_HD float plis_logf(float x) {
